@@ -1,0 +1,145 @@
+/*
+ * kielflow_b200.h -- C ABI of the B200 (sm_100a) time-step hot path of kielflow.
+ *
+ * One context = one cubic periodic grid resident on one GPU: the spectral
+ * state (u'_x, u'_y, u'_z, s = ln n as half spectra), the potential phi, the
+ * dust charge n_d and the penalization mask, plus all work buffers.  Host
+ * arrays use the reference's layouts:
+ *   real field      field_real::val, double[n*n*n], index k + n*(j + n*i)
+ *                   (field_base.hpp:23-24)
+ *   spectral field  field_imag::val, fftw_complex[n*n*(n/2+1)] = interleaved
+ *                   (re, im) doubles (field_imag.cpp:16,23), FFTW r2c layout,
+ *                   forward unnormalised, inverse scaled by 1/N
+ *                   (OP_FFT.cpp:49-63, OP_iFFT.cpp:49-64).
+ * Every call returns KF_OK (0) or a negative KF_ERR_* code; kf_last_error()
+ * gives the message.  A context is not thread-safe; distinct contexts are
+ * independent.  No call copies device data to the host unless it says so.
+ */
+#ifndef KIELFLOW_B200_H_
+#define KIELFLOW_B200_H_
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KF_OK 0
+#define KF_ERR_ARG (-1)           /* invalid argument or unsupported grid        */
+#define KF_ERR_CUDA (-2)          /* CUDA runtime error (message has the name)   */
+#define KF_ERR_NAN (-3)           /* NaN/Inf detected in phi (cf. reference      */
+                                  /* solver_poisson_jacobi_nlin.cpp:78-82,95-99) */
+#define KF_ERR_NOT_CONVERGED (-4) /* Poisson solve hit its iteration cap         */
+#define KF_ERR_NO_DEVICE (-5)     /* no CUDA device / wrong architecture         */
+
+/* right-hand-side terms (runtime form of rhs_standard.hpp:22-30) */
+#define KF_T_POISSON (1 << 0)      /* nonlinear Poisson solve for phi            */
+#define KF_T_DISSIPATION (1 << 1)  /* ion-neutral friction tau u                 */
+#define KF_T_SVISCOSITY (1 << 2)   /* spectral viscosity field_SV                */
+#define KF_T_E_INT (1 << 3)        /* -grad phi (filtered)                       */
+#define KF_T_PRESSURE (1 << 4)     /* -grad s / theta  (the reference's          */
+                                   /*  _RHS_DIFFUSION switch)                    */
+#define KF_T_E_EXT (1 << 5)        /* mean flow  -M d/dx                          */
+#define KF_T_CONTINUITY (1 << 6)   /* -div u - u.grad s                          */
+#define KF_T_ADVECTION (1 << 7)    /* -(u.grad) u                                */
+#define KF_T_PENALIZATION (1 << 8) /* masking penalization of the dust grain     */
+#define KF_T_DIFFUSION (1 << 9)    /* Laplacian diffusion D lap(u), D lap(s)     */
+#define KF_T_SHIPPED 0xFF          /* the set the reference's build enables       */
+
+/* Poisson solver */
+#define KF_PS_JACOBI_REF 0 /* nonlinear Jacobi, relative-update stop (reference)  */
+#define KF_PS_JACOBI_RES 1 /* nonlinear Jacobi, max-norm residual stop            */
+#define KF_PS_CASCADIC 2   /* the reference's cascadic multigrid plan             */
+#define KF_PS_FAS 3        /* FAS V-cycles, red-black point-Newton smoother       */
+
+/* bulk precision */
+#define KF_FP64 0
+#define KF_FP32_BULK 1 /* FFTs, products, RK4 in FP32; Poisson in FP64 */
+
+typedef struct {
+    int n;             /* cubic grid n^3: 16, 32, 64, 96, 128 or 256                 */
+    double L;          /* box side; axes axis_CoEqSt(-L/2, L, n)                      */
+    double M;          /* Mach number (parameters::M)                                */
+    double tau;        /* friction (parameters::tau)                                 */
+    double theta;      /* Te/Ti (parameters::theta)                                  */
+    double diff_D;     /* Laplacian diffusion coefficient                            */
+    double sv_eps;     /* spectral-viscosity amplitude (0.5 in rhs_standard.cpp:57)  */
+    double sv_cut;     /* SV only where |k~| > sv_cut (0: everywhere)                */
+    double pen_eta;    /* penalization damping eta_d (<= 0)                          */
+    int terms;         /* KF_T_* bitmask                                             */
+    int poisson_mode;  /* KF_PS_*                                                    */
+    int nlj_max_it;    /* Jacobi sweep cap (negative: 1000, as the reference)        */
+    double nlj_limit;  /* relative-update limit (KF_PS_JACOBI_REF)                   */
+    double res_tol;    /* max-norm residual target (KF_PS_JACOBI_RES, KF_PS_FAS)     */
+    int mg_levels;     /* FAS levels, finest n ... coarsest n >> (levels-1)          */
+    int mg_pre;        /* FAS pre-smoothing sweeps                                   */
+    int mg_post;       /* FAS post-smoothing sweeps                                  */
+    double coarse_tol; /* FAS coarsest-level residual target                         */
+    int max_cycles;    /* FAS V-cycle cap per solve                                  */
+    int precision;     /* KF_FP64 or KF_FP32_BULK                                    */
+} kf_config;
+
+typedef struct kf_ctx kf_ctx;
+
+typedef struct {
+    int solves;             /* Poisson solves since creation                    */
+    int last_iterations;    /* sweeps (Jacobi) or V-cycles (FAS) of the last one */
+    long long total_iterations;
+    double last_residual;   /* max-norm residual at exit of the last solve      */
+    int not_converged;      /* solves that hit their cap                        */
+    double charge;          /* sum(e^s - e^phi + n_d) h^3 (FP64)                */
+    double kinetic;         /* sum 0.5 e^s |u|^2 h^3, u = u' + M e_x (FP64)     */
+} kf_diag_out;
+
+/* Context lifetime.  Replaces constructing the reference's rhs_standard
+ * (rhs_standard.cpp:7-85), solver_poisson_jacobi_nlin / solver_poisson_multigrid
+ * (kielflow.cpp:197-217) and Runge_kutta_O4 (RKO4.cpp:41-47). */
+int kf_ctx_create(const kf_config *cfg, kf_ctx **out);
+int kf_ctx_destroy(kf_ctx *ctx);
+const char *kf_last_error(const kf_ctx *ctx);
+/* Make the context issue its work on an existing cudaStream_t (NULL: own stream). */
+int kf_set_stream(kf_ctx *ctx, void *cuda_stream);
+int kf_synchronize(kf_ctx *ctx);
+
+/* State transfer (host, reference layout).  set = H2D, get = D2H. */
+int kf_set_state(kf_ctx *ctx, const double *FUx, const double *FUy, const double *FUz,
+                 const double *Fni);
+int kf_get_state(kf_ctx *ctx, double *FUx, double *FUy, double *FUz, double *Fni);
+/* dust charge n_d and penalization mask H, real fields (NULL: leave as is) */
+int kf_set_sources(kf_ctx *ctx, const double *nd, const double *mask);
+int kf_set_phi(kf_ctx *ctx, const double *phi);
+int kf_get_phi(kf_ctx *ctx, double *phi);
+
+/* interface_rhs::solve (interface_rhs.hpp:11-12; rhs_standard.cpp:89-566):
+ * replaces the context's state by its time derivative, in place.  t is
+ * accepted for interface parity; the right-hand side is autonomous. */
+int kf_rhs_eval(kf_ctx *ctx, double t);
+
+/* interface_ode_solver::solve (interface_ODE_solver.hpp:11-12; RKO4.cpp:50-241):
+ * nsteps classic RK4 steps of size dt on the device-resident state. */
+int kf_rk4_steps(kf_ctx *ctx, int nsteps, double dt);
+
+/* interface_poisson_solver::solve (interface_poisson_solver.hpp:18): phi_io is
+ * the initial guess and the result, rho is read only; host arrays, n^3 doubles. */
+int kf_poisson_solve(kf_ctx *ctx, double *phi_io, const double *rho);
+
+/* diagnostics: Poisson statistics and FP64 conserved-quantity reductions */
+int kf_diag(kf_ctx *ctx, kf_diag_out *out);
+
+/* The standalone spectral operators on host arrays (OP_FFT.cpp:49-63,
+ * OP_iFFT.cpp:49-64): r2c unnormalised, c2r scaled by 1/N. */
+int kf_fft_r2c(kf_ctx *ctx, const double *in_real, double *out_complex);
+int kf_fft_c2r(kf_ctx *ctx, const double *in_complex, double *out_real);
+
+/* Device pointers of the resident state (4 half spectra, interleaved complex
+ * in the context's bulk precision) for zero-copy consumers; NULL entries skip. */
+int kf_state_device_ptrs(kf_ctx *ctx, void **FUx, void **FUy, void **FUz, void **Fni);
+
+/* Kernel launches issued by this context since creation (measurement aid). */
+long long kf_launch_count(const kf_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,230 @@
+"""ctypes binding of libkf.so (include/kielflow_b200.h)."""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+
+KF_OK = 0
+KF_ERRORS = {-1: "KF_ERR_ARG", -2: "KF_ERR_CUDA", -3: "KF_ERR_NAN", -4: "KF_ERR_NOT_CONVERGED",
+             -5: "KF_ERR_NO_DEVICE"}
+
+KF_T_POISSON = 1 << 0
+KF_T_DISSIPATION = 1 << 1
+KF_T_SVISCOSITY = 1 << 2
+KF_T_E_INT = 1 << 3
+KF_T_PRESSURE = 1 << 4
+KF_T_E_EXT = 1 << 5
+KF_T_CONTINUITY = 1 << 6
+KF_T_ADVECTION = 1 << 7
+KF_T_PENALIZATION = 1 << 8
+KF_T_DIFFUSION = 1 << 9
+KF_T_SHIPPED = 0xFF
+KF_T_ALL = 0x3FF
+
+KF_PS_JACOBI_REF, KF_PS_JACOBI_RES, KF_PS_CASCADIC, KF_PS_FAS = 0, 1, 2, 3
+KF_FP64, KF_FP32_BULK = 0, 1
+
+_D = ctypes.POINTER(ctypes.c_double)
+
+
+class KfError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{KF_ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Config(ctypes.Structure):
+    """kf_config (include/kielflow_b200.h)."""
+    _fields_ = [
+        ("n", ctypes.c_int), ("L", ctypes.c_double), ("M", ctypes.c_double), ("tau", ctypes.c_double),
+        ("theta", ctypes.c_double), ("diff_D", ctypes.c_double), ("sv_eps", ctypes.c_double),
+        ("sv_cut", ctypes.c_double), ("pen_eta", ctypes.c_double), ("terms", ctypes.c_int),
+        ("poisson_mode", ctypes.c_int), ("nlj_max_it", ctypes.c_int), ("nlj_limit", ctypes.c_double),
+        ("res_tol", ctypes.c_double), ("mg_levels", ctypes.c_int), ("mg_pre", ctypes.c_int),
+        ("mg_post", ctypes.c_int), ("coarse_tol", ctypes.c_double), ("max_cycles", ctypes.c_int),
+        ("precision", ctypes.c_int),
+    ]
+
+    @classmethod
+    def make(cls, n, L, M, tau=0.1, theta=30.0, diff_D=0.0, sv_eps=0.5, sv_cut=0.0, pen_eta=0.0,
+             terms=KF_T_SHIPPED, poisson_mode=KF_PS_JACOBI_REF, nlj_max_it=80, nlj_limit=0.5e-5,
+             res_tol=1e-10, mg_levels=4, mg_pre=2, mg_post=2, coarse_tol=1e-13, max_cycles=50,
+             precision=KF_FP64):
+        return cls(n, L, M, tau, theta, diff_D, sv_eps, sv_cut, pen_eta, terms, poisson_mode, nlj_max_it,
+                   nlj_limit, res_tol, mg_levels, mg_pre, mg_post, coarse_tol, max_cycles, precision)
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class DiagOut(ctypes.Structure):
+    _fields_ = [("solves", ctypes.c_int), ("last_iterations", ctypes.c_int),
+                ("total_iterations", ctypes.c_longlong), ("last_residual", ctypes.c_double),
+                ("not_converged", ctypes.c_int), ("charge", ctypes.c_double), ("kinetic", ctypes.c_double)]
+
+
+def library_path() -> str:
+    return os.environ.get("KIELFLOW_B200_LIB", os.path.join(PKG, "libkf.so"))
+
+
+EXPORTS = [
+    "kf_ctx_create", "kf_ctx_destroy", "kf_last_error", "kf_set_stream", "kf_synchronize", "kf_set_state",
+    "kf_get_state", "kf_set_sources", "kf_set_phi", "kf_get_phi", "kf_rhs_eval", "kf_rk4_steps",
+    "kf_poisson_solve", "kf_diag", "kf_fft_r2c", "kf_fft_c2r", "kf_state_device_ptrs", "kf_launch_count",
+]
+
+_lib = None
+
+
+def load_library():
+    """Load libkf.so; raises if it is missing (there is no CPU fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = library_path()
+    if not os.path.exists(path):
+        raise KfError(-5, f"CUDA library not built: {path} (run python -m kielflow_b200.build)")
+    L = ctypes.CDLL(path)
+    vp = ctypes.c_void_p
+    L.kf_ctx_create.argtypes = [ctypes.POINTER(Config), ctypes.POINTER(vp)]
+    L.kf_ctx_destroy.argtypes = [vp]
+    L.kf_last_error.argtypes = [vp]
+    L.kf_last_error.restype = ctypes.c_char_p
+    L.kf_set_stream.argtypes = [vp, vp]
+    L.kf_synchronize.argtypes = [vp]
+    L.kf_set_state.argtypes = [vp, _D, _D, _D, _D]
+    L.kf_get_state.argtypes = [vp, _D, _D, _D, _D]
+    L.kf_set_sources.argtypes = [vp, _D, _D]
+    L.kf_set_phi.argtypes = [vp, _D]
+    L.kf_get_phi.argtypes = [vp, _D]
+    L.kf_rhs_eval.argtypes = [vp, ctypes.c_double]
+    L.kf_rk4_steps.argtypes = [vp, ctypes.c_int, ctypes.c_double]
+    L.kf_poisson_solve.argtypes = [vp, _D, _D]
+    L.kf_diag.argtypes = [vp, ctypes.POINTER(DiagOut)]
+    L.kf_fft_r2c.argtypes = [vp, _D, _D]
+    L.kf_fft_c2r.argtypes = [vp, _D, _D]
+    L.kf_state_device_ptrs.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                       ctypes.POINTER(vp)]
+    L.kf_launch_count.argtypes = [vp]
+    L.kf_launch_count.restype = ctypes.c_longlong
+    _lib = L
+    return L
+
+
+def _ptr(a: np.ndarray):
+    if not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("array must be C-contiguous")
+    return a.ctypes.data_as(_D)
+
+
+class Context:
+    """One grid resident on the GPU (kf_ctx)."""
+
+    def __init__(self, cfg: Config):
+        self.L = load_library()
+        self.cfg = cfg
+        h = ctypes.c_void_p()
+        rc = self.L.kf_ctx_create(ctypes.byref(cfg), ctypes.byref(h))
+        if rc:
+            raise KfError(rc, self.L.kf_last_error(None).decode())
+        self.h = h
+        n = cfg.n
+        self.shape_c = (n, n, n // 2 + 1)
+        self.shape_r = (n, n, n)
+
+    def _check(self, rc):
+        if rc:
+            raise KfError(rc, self.L.kf_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.kf_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- data movement -------------------------------------------------
+    def set_state(self, FUx, FUy, FUz, Fni):
+        arrs = [np.ascontiguousarray(a, np.complex128) for a in (FUx, FUy, FUz, Fni)]
+        for a in arrs:
+            if a.shape != self.shape_c:
+                raise ValueError(f"spectral field must have shape {self.shape_c}")
+        self._check(self.L.kf_set_state(self.h, *[a.ctypes.data_as(_D) for a in arrs]))
+
+    def get_state(self, out=None):
+        out = out or [np.empty(self.shape_c, np.complex128) for _ in range(4)]
+        self._check(self.L.kf_get_state(self.h, *[a.ctypes.data_as(_D) for a in out]))
+        return out
+
+    def set_sources(self, nd=None, mask=None):
+        nd = None if nd is None else np.ascontiguousarray(nd, np.float64)
+        mask = None if mask is None else np.ascontiguousarray(mask, np.float64)
+        self._check(self.L.kf_set_sources(self.h, None if nd is None else _ptr(nd),
+                                          None if mask is None else _ptr(mask)))
+
+    def set_phi(self, phi):
+        phi = np.ascontiguousarray(phi, np.float64)
+        self._check(self.L.kf_set_phi(self.h, _ptr(phi)))
+
+    def get_phi(self):
+        out = np.empty(self.shape_r, np.float64)
+        self._check(self.L.kf_get_phi(self.h, _ptr(out)))
+        return out
+
+    # ---- the hot path --------------------------------------------------
+    def rhs(self, t: float = 0.0):
+        self._check(self.L.kf_rhs_eval(self.h, t))
+
+    def rk4(self, dt: float, nsteps: int = 1):
+        self._check(self.L.kf_rk4_steps(self.h, nsteps, dt))
+
+    def poisson(self, phi, rho):
+        phi = np.array(phi, dtype=np.float64, order="C", copy=True)
+        rho = np.ascontiguousarray(rho, np.float64)
+        self._check(self.L.kf_poisson_solve(self.h, _ptr(phi), _ptr(rho)))
+        return phi
+
+    def diag(self) -> DiagOut:
+        d = DiagOut()
+        self._check(self.L.kf_diag(self.h, ctypes.byref(d)))
+        return d
+
+    def r2c(self, x):
+        x = np.ascontiguousarray(x, np.float64)
+        out = np.empty(self.shape_c, np.complex128)
+        self._check(self.L.kf_fft_r2c(self.h, _ptr(x), out.ctypes.data_as(_D)))
+        return out
+
+    def c2r(self, F):
+        F = np.ascontiguousarray(F, np.complex128)
+        out = np.empty(self.shape_r, np.float64)
+        self._check(self.L.kf_fft_c2r(self.h, F.ctypes.data_as(_D), _ptr(out)))
+        return out
+
+    def synchronize(self):
+        self._check(self.L.kf_synchronize(self.h))
+
+    def set_stream(self, stream_handle):
+        self._check(self.L.kf_set_stream(self.h, ctypes.c_void_p(stream_handle)))
+
+    def device_state_ptrs(self):
+        p = [ctypes.c_void_p() for _ in range(4)]
+        self._check(self.L.kf_state_device_ptrs(self.h, *[ctypes.byref(x) for x in p]))
+        return [x.value for x in p]
+
+    def launch_count(self) -> int:
+        return int(self.L.kf_launch_count(self.h))

@@ -1,0 +1,65 @@
+"""The standard workloads of the kielflow time step, with their sizes.
+
+Physics shared by all workloads: box side L = 2*pi*4 Debye lengths, theta =
+Te/Ti = 30 (the reference frontend's default, frontend.cpp:70), Laplacian
+diffusion D = 1e-3 on s and u', dust grain = Gaussian charge at the box
+centre, penalization sphere of radius 0.5 with eta_d = -1e-3 (masking form of
+effect_penalization.cpp:35; targets u'_x = -M, u'_y = u'_z = 0, s = -10 as in
+rhs_standard.cpp:486-526), the phi filter and the grad(s)/theta pressure term
+of rhs_standard.cpp:218-248, 2/3 dealiasing, initial noise amplitude 1e-3 on
+|m| <= 4, dt = 0.2 h / max|u| from the initial state.
+"""
+from __future__ import annotations
+
+import math
+
+from ._lib import (KF_FP32_BULK, KF_FP64, KF_PS_FAS, KF_PS_JACOBI_RES, KF_T_ALL, KF_T_SVISCOSITY, Config)
+
+L_BOX = 2.0 * math.pi * 4.0
+THETA = 30.0
+DIFF_D = 1e-3
+PEN_ETA = -1e-3
+MASK_RADIUS = 0.5
+CFL = 0.2
+
+WORKLOADS = {
+    # plain FP64, nonlinear Jacobi to residual 1e-10, no spectral viscosity
+    "jacobi32": dict(n=32, M=0.8, tau=0.1, Q=-10.0, sigma=0.5, steps=100, sv=False,
+                     poisson_mode=KF_PS_JACOBI_RES, precision=KF_FP64),
+    # plain FP64, FAS V-cycles (4 levels, 2+2), spectral viscosity beyond 0.6 k_max
+    "fas128": dict(n=128, M=1.2, tau=0.1, Q=-10.0, sigma=0.5, steps=1000, sv=True,
+                   poisson_mode=KF_PS_FAS, precision=KF_FP64),
+    # FP32 bulk (FFTs, products, RK4) with the FP64 Poisson solve, 256^3
+    "fp32bulk256": dict(n=256, M=1.0, tau=0.05, Q=-50.0, sigma=0.3, steps=2000, sv=True,
+                        poisson_mode=KF_PS_FAS, precision=KF_FP32_BULK),
+    # the same 256^3 problem in plain FP64 (the comparison arm)
+    "fp64_256": dict(n=256, M=1.0, tau=0.05, Q=-50.0, sigma=0.3, steps=2000, sv=True,
+                     poisson_mode=KF_PS_FAS, precision=KF_FP64),
+    # adjoint workload geometry (forward part)
+    "adj128": dict(n=128, M=0.9, tau=0.1, Q=-20.0, sigma=0.5, steps=200, sv=True,
+                   poisson_mode=KF_PS_FAS, precision=KF_FP64),
+}
+
+
+def config_for(w: dict, n: int | None = None, precision: int | None = None, **over) -> Config:
+    """kf_config of a workload dict (optionally on another grid size)."""
+    n = n or w["n"]
+    terms = KF_T_ALL if w["sv"] else (KF_T_ALL & ~KF_T_SVISCOSITY)
+    levels = max(1, min(4, int(math.log2(n)) - 3))
+    kw = dict(tau=w["tau"], theta=THETA, diff_D=DIFF_D, sv_eps=0.5, sv_cut=0.6 if w["sv"] else 0.0,
+              pen_eta=PEN_ETA, terms=terms, poisson_mode=w["poisson_mode"], nlj_max_it=100000,
+              nlj_limit=0.5e-5, res_tol=1e-10, mg_levels=levels, mg_pre=2, mg_post=2, coarse_tol=1e-13,
+              max_cycles=100, precision=w["precision"] if precision is None else precision)
+    kw.update(over)
+    return Config.make(n, L_BOX, w["M"], **kw)
+
+
+def make_inputs(w: dict, n: int | None = None, seed: int = 0):
+    """(state, n_d, mask, dt) of a workload, from the seeded generator."""
+    from . import inputs as I
+    n = n or w["n"]
+    st = I.initial_state(n, seed=seed)
+    nd = I.gauss_charge(n, L_BOX, w["Q"], w["sigma"])
+    mask = I.sphere_mask(n, L_BOX, MASK_RADIUS)
+    dt = I.cfl_dt(st, n, L_BOX, w["M"], CFL)
+    return st, nd, mask, dt

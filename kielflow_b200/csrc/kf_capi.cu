@@ -1,0 +1,981 @@
+// kf_capi.cu -- host driver and C ABI (include/kielflow_b200.h).
+//
+// The right-hand side of rhs_standard::solve (rhs_standard.cpp:89-566) is run as
+// six rounds of kernels on device-resident buffers:
+//   A  inverse x/y passes of s^ (P s^, i k_x P s^, i k_y P s^) and the z pass of
+//      P s^  ->  s_d;  rho = exp(s_d) + n_d;  Poisson solve -> phi
+//   B  phi^ = r2c(phi)                                    (E-force, :218-226)
+//   C  (penalization) rl_q = -lin_q in k-space
+//   D  inverse passes generating U_c, d_d U_c, d_d s (and c2r(rl_q))
+//   E  physical-space products (advection, u.grad s) [+ penalization]
+//   F  forward z/y passes, then the forward x pass fused with the assembly
+//      K_q = -(lin_q + F_q)   (or P F_q with penalization)
+// RK4 (RKO4.cpp:50-241) combines four such evaluations with k_rk.
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/kielflow_b200.h"
+#include "kf_passes.cuh"
+#include "kf_pointwise.cuh"
+#include "kf_poisson.cuh"
+
+using namespace kf;
+
+namespace {
+
+struct KfError {
+    int code;
+    std::string msg;
+};
+
+#define CK(x)                                                                                  \
+    do {                                                                                       \
+        cudaError_t e_ = (x);                                                                  \
+        if (e_ != cudaSuccess) throw KfError{KF_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)}; \
+    } while (0)
+
+struct LevelBuf {
+    int n = 0;
+    double *dd = nullptr, *dp = nullptr, *dm = nullptr, *gam = nullptr;
+    double *phi = nullptr, *rho = nullptr, *r = nullptr, *phi0 = nullptr;
+    Lev lev() const { return Lev{n, dd, dp, dm}; }
+};
+
+constexpr int RBS = 256;  // reduction block size
+
+}  // namespace
+
+struct kf_ctx {
+    kf_config cfg;
+    int n = 0, nzc = 0;
+    long N = 0, Nc = 0;
+    bool fp32 = false;
+    size_t es = 8, cs = 16;
+    cudaStream_t st = nullptr;
+    bool own_stream = false;
+    std::string err;
+    long long launches = 0;
+    std::vector<void *> allocs;
+
+    void *Y[4] = {}, *Ys[4] = {}, *ACC[4] = {}, *K[4] = {};
+    void *CX[12] = {}, *CY[16] = {}, *R[24] = {}, *phihat = nullptr, *LIN[4] = {};
+    double *phi = nullptr, *rho = nullptr, *nd = nullptr;
+    void *H = nullptr, *phiT = nullptr;
+    void *kv = nullptr, *SV = nullptr, *PF = nullptr, *tw = nullptr;
+    double *q2 = nullptr;
+    double *stage64 = nullptr;
+    std::vector<LevelBuf> lv;
+    double *partial = nullptr;
+    int npartial = 0;
+    double *red = nullptr;
+    double *h_red = nullptr;
+    int *d_sweeps = nullptr;
+    AxisJob *dj = nullptr;
+    ZJob *dz = nullptr;
+    // job-list offsets (into dj / dz) and counts
+    int jA_x = 0, jA_y = 0, zA = 0, zB = 0, jB_y = 0, jB_x = 0, jD_x = 0, nD_x = 0, jD_y = 0, nD_y = 0;
+    int zD = 0, nzD = 0, zF = 0, jF_y = 0, jF_x = 0, jT_x = 0, jT_y = 0, zT = 0, jTf_y = 0, jTf_x = 0;
+    int jG_x = 0, jG_y = 0, zG = 0;
+    // Jacobi state carried between sweeps and solves (solver_poisson_jacobi_nlin.hpp:66-95)
+    double norm_max = 0., norm_sum = 0., norm_max_old = -1., norm_sum_old = -1.;
+    double sup = 0., inf = 0., omega = 1.;
+    kf_diag_out diag{};
+    // per-(precision, n) entry points
+    void (*rhs_fn)(kf_ctx *) = nullptr;
+    void (*r2c_fn)(kf_ctx *) = nullptr;
+    void (*c2r_fn)(kf_ctx *) = nullptr;
+    void (*inv_state_fn)(kf_ctx *) = nullptr;
+};
+
+namespace {
+
+template <typename P> P *dalloc(kf_ctx *c, size_t bytes) {
+    void *p = nullptr;
+    CK(cudaMalloc(&p, bytes ? bytes : 16));
+    c->allocs.push_back(p);
+    return static_cast<P *>(p);
+}
+
+inline int nblk(long work, int bs) { return (int)((work + bs - 1) / bs); }
+
+// ------------------------------------------------------------------ host tables
+double k_val_at(int i, int n, double L) {  // axis_EqSt.cpp:57-61
+    double pi = acos(-1.);
+    return ((i <= n / 2) ? (2. * pi * i / L) : (2. * pi * (i - n) / L));
+}
+double val_at(int i, int n, double L) { return -0.5 * L + i * (L / n); }  // axis_EqSt.cpp:52-55
+
+// ------------------------------------------------------------------ Poisson driver
+void reduce_read(kf_ctx *c, int nb) {
+    k_reduce_final<RBS><<<1, RBS, 0, c->st>>>(c->partial, nb, c->red);
+    c->launches++;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(c->h_red, c->red, sizeof(double) * KF_RED, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+}
+
+int red_blocks(long N) {
+    long nb = (N + RBS - 1) / RBS;
+    return (int)(nb < 1184 ? nb : 1184);
+}
+
+double max_residual(kf_ctx *c, const LevelBuf &L, const double *phi, const double *rho, double *r = nullptr) {
+    const long N = (long)L.n * L.n * L.n;
+    const int nb = red_blocks(N);
+    k_residual<RBS><<<nb, RBS, 0, c->st>>>(phi, rho, L.lev(), r, c->partial);
+    c->launches++;
+    reduce_read(c, nb);
+    return c->h_red[4];
+}
+
+// solver_poisson_jacobi_nlin::solve (:50-108) on one level; phi, tmp: level-sized.
+int jacobi_solve(kf_ctx *c, const LevelBuf &L, double *phi, double *tmp, const double *rho, int max_it,
+                 double limit_max, bool resstop, double tol) {
+    const long N = (long)L.n * L.n * L.n;
+    const int nb = red_blocks(N);
+    c->sup = 0.;
+    c->inf = 0.;
+    int iteration = 0;
+    c->omega = 1.;
+    bool converged = false;
+    c->norm_sum_old = -1.;
+    if (max_it < 0) max_it = 1000;
+    double *cur = phi, *oth = tmp;
+    double rlast = 0.;
+    while (!converged && iteration < max_it) {
+        iteration++;
+        c->norm_sum_old = c->norm_sum;
+        c->norm_max_old = c->norm_max;
+        k_jacobi<RBS><<<nb, RBS, 0, c->st>>>(cur, oth, rho, L.lev(), c->omega, c->partial);
+        c->launches++;
+        reduce_read(c, nb);
+        std::swap(cur, oth);
+        c->norm_max = c->h_red[0];
+        c->norm_sum = c->h_red[1];
+        c->sup = c->h_red[2];
+        c->inf = c->h_red[3];
+        rlast = c->h_red[4];
+        if (rlast != rlast || c->norm_max != c->norm_max) throw KfError{KF_ERR_NAN, "NaN in the Jacobi sweep"};
+        // Carre's over-relaxation factor (:237-252)
+        c->norm_sum = c->norm_sum / ((double)N);
+        if ((c->norm_max < c->norm_max_old) && (iteration > 1)) {
+            double lambda = c->norm_sum / c->norm_sum_old;
+            c->omega = 2. / (1. + sqrt(1. - pow(lambda + c->omega - 1., 2.) / (lambda * pow(c->omega, 2.))));
+        } else {
+            c->omega = .5;
+        }
+        if (c->omega != c->omega) c->omega = .5;
+        bool conv_rel = c->norm_max < limit_max * (c->sup - c->inf);
+        converged = resstop ? (rlast <= tol) : conv_rel;
+    }
+    if (cur != phi) CK(cudaMemcpyAsync(phi, cur, sizeof(double) * N, cudaMemcpyDeviceToDevice, c->st));
+    c->diag.last_iterations = iteration;
+    c->diag.total_iterations += iteration;
+    c->diag.last_residual = rlast;
+    if (!converged) c->diag.not_converged++;
+    return converged ? 0 : 1;
+}
+
+void vcycle(kf_ctx *c, int l) {
+    LevelBuf &L = c->lv[l];
+    const kf_config &cf = c->cfg;
+    const int n = L.n;
+    const long N = (long)n * n * n;
+    if (l == (int)c->lv.size() - 1) {
+        k_coarse_solve<<<1, 1024, 0, c->st>>>(L.phi, L.rho, L.lev(), cf.coarse_tol, 1000, c->d_sweeps);
+        c->launches++;
+        return;
+    }
+    const long Mh = N / 2;
+    for (int s = 0; s < cf.mg_pre; ++s)
+        for (int color = 0; color < 2; ++color) {
+            k_rbgs<<<nblk(Mh, 256), 256, 0, c->st>>>(L.phi, L.rho, L.lev(), color);
+            c->launches++;
+        }
+    k_residual<RBS><<<red_blocks(N), RBS, 0, c->st>>>(L.phi, L.rho, L.lev(), L.r, c->partial);
+    LevelBuf &Lc = c->lv[l + 1];
+    const long Nc3 = (long)Lc.n * Lc.n * Lc.n;
+    k_restrict<<<nblk(Nc3, 256), 256, 0, c->st>>>(L.r, L.phi, n, Lc.r, Lc.phi, Lc.phi0);
+    k_fas_rhs<<<nblk(Nc3, 256), 256, 0, c->st>>>(Lc.phi, Lc.r, Lc.lev(), Lc.rho);
+    c->launches += 3;
+    vcycle(c, l + 1);
+    k_prolong_add<<<nblk(N, 256), 256, 0, c->st>>>(L.phi, Lc.phi, Lc.phi0, L.gam, n);
+    c->launches++;
+    for (int s = 0; s < cf.mg_post; ++s)
+        for (int color = 0; color < 2; ++color) {
+            k_rbgs<<<nblk(Mh, 256), 256, 0, c->st>>>(L.phi, L.rho, L.lev(), color);
+            c->launches++;
+        }
+    CK(cudaGetLastError());
+}
+
+// Poisson solve on c->phi with source c->rho.  Returns KF_OK or KF_ERR_NOT_CONVERGED.
+int poisson(kf_ctx *c) {
+    const kf_config &cf = c->cfg;
+    c->diag.solves++;
+    LevelBuf &L0 = c->lv[0];
+    int rc = 0;
+    if (cf.poisson_mode == KF_PS_JACOBI_REF || cf.poisson_mode == KF_PS_JACOBI_RES) {
+        rc = jacobi_solve(c, L0, c->phi, L0.r, c->rho, cf.nlj_max_it, cf.nlj_limit,
+                          cf.poisson_mode == KF_PS_JACOBI_RES, cf.res_tol);
+        if (cf.poisson_mode == KF_PS_JACOBI_REF) {
+            c->diag.last_residual = max_residual(c, L0, c->phi, c->rho);
+            rc = 0;  // the reference's plan has no failure on a sweep cap
+        }
+    } else if (cf.poisson_mode == KF_PS_CASCADIC) {
+        // kielflow.cpp:207-217 through solver_poisson_multigrid.cpp:246-418
+        const int steps[4] = {0, -1, -1, -1};
+        const double tol[4] = {0.01, 0.0005, 0.0001, 0.0001};
+        const int n = c->n;
+        LevelBuf &L3 = c->lv[3];
+        k_inject<<<nblk((long)L3.n * L3.n * L3.n, 256), 256, 0, c->st>>>(c->phi, n, 8, L3.phi);
+        c->launches++;
+        for (int cas = 0; cas < 4; ++cas) {
+            const int l = 3 - cas;
+            LevelBuf &L = c->lv[l];
+            const long Nl = (long)L.n * L.n * L.n;
+            if (cas > 0) {
+                double *dst = l == 0 ? c->phi : L.phi;
+                k_prolong_set<<<nblk(Nl, 256), 256, 0, c->st>>>(dst, c->lv[l + 1].phi, L.gam, L.n);
+                c->launches++;
+            }
+            const double *rho_l = c->rho;
+            if (l > 0) {
+                k_inject<<<nblk(Nl, 256), 256, 0, c->st>>>(c->rho, n, n / L.n, L.rho);
+                c->launches++;
+                rho_l = L.rho;
+            }
+            double *phi_l = l == 0 ? c->phi : L.phi;
+            jacobi_solve(c, L, phi_l, L.r, rho_l, steps[cas], tol[cas], false, 0.);
+        }
+        c->diag.last_residual = max_residual(c, L0, c->phi, c->rho);
+        rc = 0;
+    } else {
+        double r = max_residual(c, L0, c->phi, c->rho);
+        int cyc = 0;
+        while (r > cf.res_tol && cyc < cf.max_cycles) {
+            vcycle(c, 0);
+            ++cyc;
+            r = max_residual(c, L0, c->phi, c->rho);
+        }
+        c->diag.last_iterations = cyc;
+        c->diag.total_iterations += cyc;
+        c->diag.last_residual = r;
+        if (r != r) throw KfError{KF_ERR_NAN, "NaN in the multigrid solve"};
+        if (r > cf.res_tol) {
+            c->diag.not_converged++;
+            rc = 1;
+        }
+    }
+    if (c->diag.last_residual != c->diag.last_residual) throw KfError{KF_ERR_NAN, "NaN in phi"};
+    return rc;
+}
+
+// ------------------------------------------------------------------ per-(T, N) implementation
+template <typename T, int N> struct Impl {
+    typedef typename C2<T>::type T2;
+    static constexpr int TC = Tile<T>::TC, P = Plan<N>::P, LZ = ZTile<T>::LZ, NZC = N / 2 + 1;
+
+    static Geo<T> geo(kf_ctx *c) { return Geo<T>{c->n, c->nzc, (const T *)c->kv, c->q2}; }
+
+    static void set_attrs() {
+        static bool done = false;
+        if (done) return;
+        const int big = 200 * 1024;
+        CK(cudaFuncSetAttribute(k_axis_pass<T, N, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+        CK(cudaFuncSetAttribute(k_axis_pass<T, N, +1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+        CK(cudaFuncSetAttribute(k_z_c2r<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+        CK(cudaFuncSetAttribute(k_z_r2c<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+        CK(cudaFuncSetAttribute(k_xfwd_assemble<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+        done = true;
+    }
+
+    static void axis(kf_ctx *c, int off, int njobs, int ax, int sign) {
+        const int ntiles = ax == 0 ? (N * NZC + TC - 1) / TC : N * ((NZC + TC - 1) / TC);
+        const size_t smem = (size_t)N * TC * sizeof(T2);
+        if (sign < 0)
+            k_axis_pass<T, N, -1><<<njobs * ntiles, TC * P, smem, c->st>>>(c->dj + off, njobs, ax, geo(c), (const T2 *)c->tw);
+        else
+            k_axis_pass<T, N, +1><<<njobs * ntiles, TC * P, smem, c->st>>>(c->dj + off, njobs, ax, geo(c), (const T2 *)c->tw);
+        c->launches++;
+    }
+    static void zc2r(kf_ctx *c, int off, int njobs) {
+        const int nrows = N * N;
+        const int ntiles = (nrows + LZ - 1) / LZ;
+        const size_t smem = (size_t)(2 * LZ * NZC + LZ * (N + 1)) * sizeof(T2);
+        k_z_c2r<T, N><<<njobs * ntiles, LZ * P, smem, c->st>>>(c->dz + off, njobs, nrows, geo(c), (const T2 *)c->tw,
+                                                             (T)(1. / ((double)N * N * N)));
+        c->launches++;
+    }
+    static void zr2c(kf_ctx *c, int off, int njobs) {
+        const int nrows = N * N;
+        const int ntiles = (nrows + LZ - 1) / LZ;
+        const size_t smem = (size_t)(LZ * (N + 1)) * sizeof(T2);
+        k_z_r2c<T, N><<<njobs * ntiles, LZ * P, smem, c->st>>>(c->dz + off, njobs, nrows, (const T2 *)c->tw);
+        c->launches++;
+    }
+    static RhsArgs<T> rargs(kf_ctx *c) {
+        RhsArgs<T> a;
+        for (int q = 0; q < 4; ++q) a.Y[q] = (const T2 *)c->Ys[q];
+        a.phihat = (const T2 *)c->phihat;
+        a.SV = (const T *)c->SV;
+        a.PF = (const T *)c->PF;
+        a.tau = (T)c->cfg.tau;
+        a.theta = (T)c->cfg.theta;
+        a.M = (T)c->cfg.M;
+        a.D = (T)c->cfg.diff_D;
+        a.terms = c->cfg.terms;
+        return a;
+    }
+
+    // one right-hand-side evaluation: Ys -> K
+    static void rhs(kf_ctx *c) {
+        const int Tm = c->cfg.terms;
+        const bool pen = Tm & T_PENALIZATION;
+        const bool pois = (Tm & T_POISSON) && (Tm & T_E_INT);
+        // A
+        axis(c, c->jA_x, 2, 0, +1);
+        axis(c, c->jA_y, 3, 1, +1);
+        if (pois || pen) zc2r(c, c->zA, 1);
+        if (pois) {
+            k_rho<T><<<nblk(c->N, 256), 256, 0, c->st>>>((const T *)c->R[0], c->nd, c->rho, c->N);
+            c->launches++;
+            CK(cudaGetLastError());
+            int rc = poisson(c);
+            if (rc) throw KfError{KF_ERR_NOT_CONVERGED, "Poisson solve did not reach its tolerance"};
+        }
+        // B
+        if (Tm & T_E_INT) {
+            if (c->fp32) {
+                k_from_f64<T><<<nblk(c->N, 256), 256, 0, c->st>>>((T *)c->phiT, c->phi, c->N);
+                c->launches++;
+            }
+            zr2c(c, c->zB, 1);
+            axis(c, c->jB_y, 1, 1, -1);
+            axis(c, c->jB_x, 1, 0, -1);
+        }
+        // C
+        if (pen) {
+            k_lin<T><<<nblk(c->Nc, 256), 256, 0, c->st>>>(rargs(c), geo(c), (T2 *)c->LIN[0], (T2 *)c->LIN[1],
+                                                         (T2 *)c->LIN[2], (T2 *)c->LIN[3]);
+            c->launches++;
+        }
+        // D
+        axis(c, c->jD_x, pen ? 10 : 6, 0, +1);
+        axis(c, c->jD_y, pen ? 13 : 9, 1, +1);
+        zc2r(c, c->zD, pen ? 10 : 8);
+        // E
+        ProdArgs<T> pa;
+        for (int q = 0; q < 3; ++q) {
+            pa.U[q] = (const T *)c->R[1 + q];
+            pa.ds[q] = (const T *)c->R[13 + q];
+            for (int d = 0; d < 3; ++d) pa.dU[q][d] = (const T *)c->R[4 + 3 * q + d];
+        }
+        for (int q = 0; q < 4; ++q) {
+            pa.rl[q] = (const T *)c->R[16 + q];
+            pa.out[q] = (T *)c->R[20 + q];
+        }
+        pa.sd = (const T *)c->R[0];
+        pa.H = (const T *)c->H;
+        pa.M = (T)c->cfg.M;
+        pa.eta = (T)c->cfg.pen_eta;
+        pa.terms = Tm;
+        pa.N = c->N;
+        k_products<T><<<nblk(c->N, 256), 256, 0, c->st>>>(pa);
+        c->launches++;
+        // F
+        zr2c(c, c->zF, 2);
+        axis(c, c->jF_y, 4, 1, -1);
+        const int ntiles = (N * NZC + TC - 1) / TC;
+        k_xfwd_assemble<T, N><<<ntiles, TC * P, (size_t)N * TC * sizeof(T2), c->st>>>(c->dj + c->jF_x, geo(c), rargs(c),
+                                                                                     (const T2 *)c->tw);
+        c->launches++;
+        CK(cudaGetLastError());
+    }
+
+    // standalone transforms on R[0] <-> CX[0] (through CY[0])
+    static void r2c(kf_ctx *c) {
+        zr2c(c, c->zT, 1);
+        axis(c, c->jTf_y, 1, 1, -1);
+        axis(c, c->jTf_x, 1, 0, -1);
+        CK(cudaGetLastError());
+    }
+    static void c2r(kf_ctx *c) {
+        axis(c, c->jT_x, 1, 0, +1);
+        axis(c, c->jT_y, 1, 1, +1);
+        zc2r(c, c->zT + 1, 1);
+        CK(cudaGetLastError());
+    }
+    // inverse transforms of the (undealiased) state into R[20..23] for diagnostics
+    static void inv_state(kf_ctx *c) {
+        axis(c, c->jG_x, 4, 0, +1);
+        axis(c, c->jG_y, 4, 1, +1);
+        zc2r(c, c->zG, 2);
+        CK(cudaGetLastError());
+    }
+};
+
+template <typename T> struct Dispatch {
+    static bool pick(kf_ctx *c) {
+        switch (c->n) {
+#define KF_CASE(NN)                                    \
+    case NN:                                           \
+        Impl<T, NN>::set_attrs();                      \
+        c->rhs_fn = &Impl<T, NN>::rhs;                 \
+        c->r2c_fn = &Impl<T, NN>::r2c;                 \
+        c->c2r_fn = &Impl<T, NN>::c2r;                 \
+        c->inv_state_fn = &Impl<T, NN>::inv_state;     \
+        return true;
+            KF_CASE(16)
+            KF_CASE(32)
+            KF_CASE(64)
+            KF_CASE(96)
+            KF_CASE(128)
+            KF_CASE(256)
+#undef KF_CASE
+            default:
+                return false;
+        }
+    }
+};
+
+// FP64 sums of the charge density e^s - e^phi + n_d and the kinetic energy
+// density 0.5 e^s |M e_x + u'|^2 (block partials in slots 0 and 1).
+template <typename T>
+__global__ void __launch_bounds__(RBS) k_diag_sums(const T *__restrict__ s, const T *__restrict__ ux,
+                                                   const T *__restrict__ uy, const T *__restrict__ uz,
+                                                   const double *__restrict__ phi, const double *__restrict__ nd,
+                                                   double M, long N, double *__restrict__ partial) {
+    __shared__ double sh[2 * RBS];
+    double ch = 0., kin = 0.;
+    for (long i = (long)blockIdx.x * RBS + threadIdx.x; i < N; i += (long)gridDim.x * RBS) {
+        const double n_i = exp((double)s[i]);
+        ch += n_i - exp(phi[i]) + nd[i];
+        const double vx = M + (double)ux[i], vy = (double)uy[i], vz = (double)uz[i];
+        kin += 0.5 * n_i * (vx * vx + vy * vy + vz * vz);
+    }
+    sh[threadIdx.x] = kin;
+    sh[RBS + threadIdx.x] = ch;
+    __syncthreads();
+    for (int w = RBS / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) {
+            sh[threadIdx.x] += sh[threadIdx.x + w];
+            sh[RBS + threadIdx.x] += sh[RBS + threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        partial[(long)blockIdx.x * KF_RED + 0] = sh[0];
+        partial[(long)blockIdx.x * KF_RED + 1] = sh[RBS];
+    }
+}
+
+__global__ void k_diag_final(const double *__restrict__ partial, int nb, double *__restrict__ out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double a = 0., b = 0.;
+        for (int i = 0; i < nb; ++i) {
+            a += partial[(long)i * KF_RED + 0];
+            b += partial[(long)i * KF_RED + 1];
+        }
+        out[0] = a;
+        out[1] = b;
+    }
+}
+
+void build_tables(kf_ctx *c) {
+    const int n = c->n, nzc = c->nzc;
+    const double L = c->cfg.L;
+    std::vector<double> kv(n), q2(n);
+    const double kmax = k_val_at(n / 2, n, L);
+    const double kzq = k_val_at(nzc / 2, n, L);  // operations.hpp:25 quirk: field_imag::Nz = n/2+1
+    for (int i = 0; i < n; ++i) {
+        kv[i] = k_val_at(i, n, L);
+        q2[i] = pow(kv[i] / kmax, 2.);
+    }
+    std::vector<double> SV(c->Nc), PF(c->Nc);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j)
+            for (int k = 0; k < nzc; ++k) {
+                const size_t ijk = (size_t)k + nzc * ((size_t)j + (size_t)i * n);
+                const double kx = kv[i], ky = kv[j], kz = kv[k];
+                // rhs_standard.cpp:64-71 (field_SV), optional cut at sv_cut
+                const double knorm = sqrt(pow(kx / kmax, 2.) + pow(ky / kmax, 2.) + pow(kz / kmax, 2.));
+                const double filter = 1. - exp(-8. * pow(sqrt(knorm), 8.));
+                double svv = c->cfg.sv_eps * filter;
+                if (c->cfg.sv_cut > 0. && !(knorm > c->cfg.sv_cut)) svv = 0.;
+                SV[ijk] = svv;
+                // operations.hpp:35-40 with the filter of rhs_standard.cpp:220
+                const double kq = sqrt(pow(kx / kmax, 2.) + pow(ky / kmax, 2.) + pow(kz / kzq, 2.));
+                PF[ijk] = exp(-2000. * pow(kq, 15.));
+            }
+    // twiddles W_N^m = exp(-2 pi i m / N), long double
+    std::vector<double> tw(2 * n);
+    const long double twopi = 6.283185307179586476925286766559005768L;
+    for (int m = 0; m < n; ++m) {
+        long double a = twopi * (long double)m / (long double)n;
+        tw[2 * m] = (double)cosl(a);
+        tw[2 * m + 1] = (double)(-sinl(a));
+    }
+    c->q2 = dalloc<double>(c, sizeof(double) * n);
+    CK(cudaMemcpy(c->q2, q2.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    if (c->fp32) {
+        std::vector<float> kvf(n), SVf(c->Nc), PFf(c->Nc), twf(2 * n);
+        for (int i = 0; i < n; ++i) kvf[i] = (float)kv[i];
+        for (long i = 0; i < c->Nc; ++i) { SVf[i] = (float)SV[i]; PFf[i] = (float)PF[i]; }
+        for (int i = 0; i < 2 * n; ++i) twf[i] = (float)tw[i];
+        c->kv = dalloc<void>(c, 4 * n);
+        c->SV = dalloc<void>(c, 4 * c->Nc);
+        c->PF = dalloc<void>(c, 4 * c->Nc);
+        c->tw = dalloc<void>(c, 8 * n);
+        CK(cudaMemcpy(c->kv, kvf.data(), 4 * n, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(c->SV, SVf.data(), 4 * c->Nc, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(c->PF, PFf.data(), 4 * c->Nc, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(c->tw, twf.data(), 8 * n, cudaMemcpyHostToDevice));
+    } else {
+        c->kv = dalloc<void>(c, 8 * n);
+        c->SV = dalloc<void>(c, 8 * c->Nc);
+        c->PF = dalloc<void>(c, 8 * c->Nc);
+        c->tw = dalloc<void>(c, 16 * n);
+        CK(cudaMemcpy(c->kv, kv.data(), 8 * n, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(c->SV, SV.data(), 8 * c->Nc, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(c->PF, PF.data(), 8 * c->Nc, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(c->tw, tw.data(), 16 * n, cudaMemcpyHostToDevice));
+    }
+}
+
+void build_levels(kf_ctx *c) {
+    const kf_config &cf = c->cfg;
+    int nl = 1;
+    if (cf.poisson_mode == KF_PS_FAS) nl = cf.mg_levels > 1 ? cf.mg_levels : 1;
+    if (cf.poisson_mode == KF_PS_CASCADIC) nl = 4;
+    for (int l = 1; l < nl; ++l)
+        if ((c->n >> l) < 2 || ((c->n >> (l - 1)) % 2))
+            throw KfError{KF_ERR_ARG, "too many multigrid levels for this grid"};
+    if (cf.poisson_mode == KF_PS_CASCADIC && c->n % 8) throw KfError{KF_ERR_ARG, "cascadic plan needs n % 8 == 0"};
+    if (cf.poisson_mode == KF_PS_FAS && ((long)(c->n >> (nl - 1)) * (c->n >> (nl - 1)) * (c->n >> (nl - 1)) > 64 * 1024))
+        throw KfError{KF_ERR_ARG, "coarsest FAS level above 40^3 points; add levels"};
+    c->lv.resize(nl);
+    for (int l = 0; l < nl; ++l) {
+        LevelBuf &L = c->lv[l];
+        const int n = c->n >> l;
+        L.n = n;
+        const double Lb = cf.L;
+        std::vector<double> H(n + 1), dd(n), dp(n), dm(n), gam(n, 0.);
+        for (int i = 0; i < n + 1; ++i) H[i] = val_at(i, n, Lb) - val_at(i - 1, n, Lb);  // H_create (:112-126)
+        for (int i = 0; i < n; ++i) {
+            dd[i] = 2. / (H[i + 1] * H[i]);
+            dp[i] = H[i + 1] * (H[i + 1] + H[i]);
+            dm[i] = H[i] * (H[i + 1] + H[i]);
+        }
+        for (int m = 1; m < n; m += 2) {  // OP_hto2h gamma on this (fine) axis
+            const double x1 = val_at(m - 1, n, Lb), x2 = val_at(m + 1, n, Lb), x = val_at(m, n, Lb);
+            gam[m] = (x - x1) / (x2 - x1);
+        }
+        L.dd = dalloc<double>(c, 8 * n);
+        L.dp = dalloc<double>(c, 8 * n);
+        L.dm = dalloc<double>(c, 8 * n);
+        L.gam = dalloc<double>(c, 8 * n);
+        CK(cudaMemcpy(L.dd, dd.data(), 8 * n, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(L.dp, dp.data(), 8 * n, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(L.dm, dm.data(), 8 * n, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(L.gam, gam.data(), 8 * n, cudaMemcpyHostToDevice));
+        const size_t bytes = sizeof(double) * (size_t)n * n * n;
+        L.r = dalloc<double>(c, bytes);
+        if (l == 0) {
+            L.phi = c->phi;
+            L.rho = c->rho;
+        } else {
+            L.phi = dalloc<double>(c, bytes);
+            L.rho = dalloc<double>(c, bytes);
+            L.phi0 = dalloc<double>(c, bytes);
+        }
+    }
+}
+
+void build_jobs(kf_ctx *c) {
+    std::vector<AxisJob> J;
+    std::vector<ZJob> Z;
+    auto aj = [&](const void *in, void *out, int mul) { J.push_back(AxisJob{in, out, mul, 0}); };
+    auto zj = [&](const void *ia, int ma, const void *ib, int mb, void *oa, void *ob) {
+        Z.push_back(ZJob{ia, ib, oa, ob, ma, mb});
+    };
+    void **CX = c->CX, **CY = c->CY, **R = c->R;
+    // A
+    c->jA_x = (int)J.size();
+    aj(c->Ys[3], CX[0], MUL_P);
+    aj(c->Ys[3], CX[1], MUL_P_IK);
+    c->jA_y = (int)J.size();
+    aj(CX[0], CY[0], MUL_NONE);
+    aj(CX[0], CY[1], MUL_IK);
+    aj(CX[1], CY[2], MUL_NONE);
+    c->zA = (int)Z.size();
+    zj(CY[0], MUL_NONE, nullptr, 0, R[0], nullptr);
+    // B
+    c->zB = (int)Z.size();
+    zj(c->phiT, 0, nullptr, 0, CX[2], nullptr);
+    c->jB_y = (int)J.size();
+    aj(CX[2], CY[3], MUL_NONE);
+    c->jB_x = (int)J.size();
+    aj(CY[3], c->phihat, MUL_NONE);
+    // D
+    c->jD_x = (int)J.size();
+    for (int q = 0; q < 3; ++q) {
+        aj(c->Ys[q], CX[2 + 2 * q], MUL_P);
+        aj(c->Ys[q], CX[3 + 2 * q], MUL_P_IK);
+    }
+    for (int q = 0; q < 4; ++q) aj(c->LIN[q], CX[8 + q], MUL_NONE);
+    c->jD_y = (int)J.size();
+    for (int q = 0; q < 3; ++q) {
+        aj(CX[2 + 2 * q], CY[3 + 3 * q], MUL_NONE);
+        aj(CX[2 + 2 * q], CY[4 + 3 * q], MUL_IK);
+        aj(CX[3 + 2 * q], CY[5 + 3 * q], MUL_NONE);
+    }
+    for (int q = 0; q < 4; ++q) aj(CX[8 + q], CY[12 + q], MUL_NONE);
+    c->zD = (int)Z.size();
+    for (int q = 0; q < 3; ++q) {
+        zj(CY[3 + 3 * q], MUL_NONE, CY[3 + 3 * q], MUL_IK, R[1 + q], R[4 + 3 * q + 2]);  // U_c, d_z U_c
+        zj(CY[4 + 3 * q], MUL_NONE, CY[5 + 3 * q], MUL_NONE, R[4 + 3 * q + 1], R[4 + 3 * q + 0]);  // d_y, d_x
+    }
+    zj(CY[1], MUL_NONE, CY[2], MUL_NONE, R[14], R[13]);  // d_y s, d_x s
+    zj(CY[0], MUL_IK, nullptr, 0, R[15], nullptr);       // d_z s
+    zj(CY[12], MUL_NONE, CY[13], MUL_NONE, R[16], R[17]);
+    zj(CY[14], MUL_NONE, CY[15], MUL_NONE, R[18], R[19]);
+    // F
+    c->zF = (int)Z.size();
+    zj(R[20], 0, R[21], 0, CX[0], CX[1]);
+    zj(R[22], 0, R[23], 0, CX[2], CX[3]);
+    c->jF_y = (int)J.size();
+    for (int q = 0; q < 4; ++q) aj(CX[q], CY[q], MUL_NONE);
+    c->jF_x = (int)J.size();
+    for (int q = 0; q < 4; ++q) aj(CY[q], c->K[q], MUL_NONE);
+    // standalone transforms: r2c R[0] -> CX[0] ; c2r CX[0] -> R[0]
+    c->zT = (int)Z.size();
+    zj(R[0], 0, nullptr, 0, CX[1], nullptr);
+    zj(CY[0], MUL_NONE, nullptr, 0, R[0], nullptr);
+    c->jTf_y = (int)J.size();
+    aj(CX[1], CY[1], MUL_NONE);
+    c->jTf_x = (int)J.size();
+    aj(CY[1], CX[0], MUL_NONE);
+    c->jT_x = (int)J.size();
+    aj(CX[0], CX[1], MUL_NONE);
+    c->jT_y = (int)J.size();
+    aj(CX[1], CY[0], MUL_NONE);
+    // diagnostics: c2r of the state (Y) -> R[20..23]
+    c->jG_x = (int)J.size();
+    for (int q = 0; q < 4; ++q) aj(c->Y[q], CX[q], MUL_NONE);
+    c->jG_y = (int)J.size();
+    for (int q = 0; q < 4; ++q) aj(CX[q], CY[q], MUL_NONE);
+    c->zG = (int)Z.size();
+    zj(CY[0], MUL_NONE, CY[1], MUL_NONE, R[20], R[21]);
+    zj(CY[2], MUL_NONE, CY[3], MUL_NONE, R[22], R[23]);
+    c->dj = dalloc<AxisJob>(c, sizeof(AxisJob) * J.size());
+    c->dz = dalloc<ZJob>(c, sizeof(ZJob) * Z.size());
+    CK(cudaMemcpy(c->dj, J.data(), sizeof(AxisJob) * J.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->dz, Z.data(), sizeof(ZJob) * Z.size(), cudaMemcpyHostToDevice));
+}
+
+void create(kf_ctx *c) {
+    const kf_config &cf = c->cfg;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) throw KfError{KF_ERR_NO_DEVICE, "no CUDA device"};
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, dev));
+    if (prop.major != 10) throw KfError{KF_ERR_NO_DEVICE, "this build targets sm_100a (B200)"};
+    if (cf.precision != KF_FP64 && cf.precision != KF_FP32_BULK) throw KfError{KF_ERR_ARG, "precision"};
+    if (cf.pen_eta > 0.) throw KfError{KF_ERR_ARG, "penalization damping must be <= 0 (effect_penalization.cpp:7-12)"};
+    if (!(cf.L > 0.) || !(cf.theta != 0.)) throw KfError{KF_ERR_ARG, "L > 0 and theta != 0 required"};
+    c->fp32 = cf.precision == KF_FP32_BULK;
+    c->es = c->fp32 ? 4 : 8;
+    c->cs = 2 * c->es;
+    c->n = cf.n;
+    c->nzc = cf.n / 2 + 1;
+    c->N = (long)cf.n * cf.n * cf.n;
+    c->Nc = (long)cf.n * cf.n * c->nzc;
+    bool ok = c->fp32 ? Dispatch<float>::pick(c) : Dispatch<double>::pick(c);
+    if (!ok) throw KfError{KF_ERR_ARG, "grid size must be one of 16, 32, 64, 96, 128, 256"};
+    CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+    c->own_stream = true;
+    const size_t cb = c->cs * c->Nc, rb = c->es * c->N;
+    for (int q = 0; q < 4; ++q) {
+        c->Y[q] = dalloc<void>(c, cb);
+        c->Ys[q] = dalloc<void>(c, cb);
+        c->ACC[q] = dalloc<void>(c, cb);
+        c->K[q] = dalloc<void>(c, cb);
+        c->LIN[q] = dalloc<void>(c, cb);
+    }
+    for (int i = 0; i < 12; ++i) c->CX[i] = dalloc<void>(c, cb);
+    for (int i = 0; i < 16; ++i) c->CY[i] = dalloc<void>(c, cb);
+    for (int i = 0; i < 24; ++i) c->R[i] = dalloc<void>(c, rb);
+    c->phihat = dalloc<void>(c, cb);
+    c->phi = dalloc<double>(c, 8 * c->N);
+    c->rho = dalloc<double>(c, 8 * c->N);
+    c->nd = dalloc<double>(c, 8 * c->N);
+    c->H = dalloc<void>(c, rb);
+    c->phiT = c->fp32 ? dalloc<void>(c, rb) : (void *)c->phi;
+    c->stage64 = dalloc<double>(c, (size_t)16 * (c->Nc > c->N ? c->Nc : c->N));
+    CK(cudaMemset(c->phi, 0, 8 * c->N));
+    CK(cudaMemset(c->nd, 0, 8 * c->N));
+    CK(cudaMemset(c->H, 0, rb));
+    for (int q = 0; q < 4; ++q) {
+        CK(cudaMemset(c->Y[q], 0, cb));
+        CK(cudaMemset(c->Ys[q], 0, cb));
+    }
+    c->npartial = 1184;
+    c->partial = dalloc<double>(c, sizeof(double) * KF_RED * c->npartial);
+    c->red = dalloc<double>(c, sizeof(double) * 8);
+    c->d_sweeps = dalloc<int>(c, sizeof(int) * 4);
+    CK(cudaMallocHost(&c->h_red, sizeof(double) * 8));
+    build_tables(c);
+    build_levels(c);
+    build_jobs(c);
+    CK(cudaDeviceSynchronize());
+}
+
+// H2D of a host FP64 array of `count` doubles into a bulk-precision device array
+void put_bulk(kf_ctx *c, void *dst, const double *src, long count) {
+    if (!c->fp32) {
+        CK(cudaMemcpyAsync(dst, src, 8 * count, cudaMemcpyHostToDevice, c->st));
+    } else {
+        CK(cudaMemcpyAsync(c->stage64, src, 8 * count, cudaMemcpyHostToDevice, c->st));
+        k_from_f64<float><<<nblk(count, 256), 256, 0, c->st>>>((float *)dst, c->stage64, count);
+        c->launches++;
+    }
+}
+
+void get_bulk(kf_ctx *c, double *dst, const void *src, long count) {
+    if (!c->fp32) {
+        CK(cudaMemcpyAsync(dst, src, 8 * count, cudaMemcpyDeviceToHost, c->st));
+    } else {
+        k_to_f64<float><<<nblk(count, 256), 256, 0, c->st>>>(c->stage64, (const float *)src, count);
+        c->launches++;
+        CK(cudaMemcpyAsync(dst, c->stage64, 8 * count, cudaMemcpyDeviceToHost, c->st));
+    }
+}
+
+void copy_state(kf_ctx *c, void *const *dst, void *const *src) {
+    for (int q = 0; q < 4; ++q)
+        CK(cudaMemcpyAsync(dst[q], src[q], c->cs * c->Nc, cudaMemcpyDeviceToDevice, c->st));
+}
+
+void rk_launch(kf_ctx *c, double cdt, int mode) {
+    const long M = c->Nc;
+    for (int q = 0; q < 4; ++q) {
+        if (c->fp32)
+            k_rk<float><<<nblk(M, 256), 256, 0, c->st>>>((float2 *)c->Y[q], (float2 *)c->ACC[q], (float2 *)c->Ys[q],
+                                                        (const float2 *)c->K[q], (float)cdt, mode, M);
+        else
+            k_rk<double><<<nblk(M, 256), 256, 0, c->st>>>((double2 *)c->Y[q], (double2 *)c->ACC[q], (double2 *)c->Ys[q],
+                                                         (const double2 *)c->K[q], cdt, mode, M);
+        c->launches++;
+    }
+    CK(cudaGetLastError());
+}
+
+template <typename F> int guarded(kf_ctx *c, F f) {
+    if (!c) return KF_ERR_ARG;
+    try {
+        f();
+        return KF_OK;
+    } catch (const KfError &e) {
+        c->err = e.msg;
+        return e.code;
+    } catch (const std::exception &e) {
+        c->err = e.what();
+        return KF_ERR_ARG;
+    }
+}
+
+}  // namespace
+
+// k_rk mode 2 writes the new state to y0; keep the stage input equal to it.
+extern "C" {
+
+static thread_local std::string g_create_err;
+
+int kf_ctx_create(const kf_config *cfg, kf_ctx **out) {
+    if (!cfg || !out) return KF_ERR_ARG;
+    kf_ctx *c = new kf_ctx;
+    c->cfg = *cfg;
+    int rc = guarded(c, [&] { create(c); });
+    if (rc) {
+        g_create_err = c->err;
+        kf_ctx_destroy(c);
+        *out = nullptr;
+        return rc;
+    }
+    *out = c;
+    return KF_OK;
+}
+
+int kf_ctx_destroy(kf_ctx *c) {
+    if (!c) return KF_ERR_ARG;
+    if (c->st) cudaStreamSynchronize(c->st);
+    for (void *p : c->allocs) cudaFree(p);
+    if (c->h_red) cudaFreeHost(c->h_red);
+    if (c->st && c->own_stream) cudaStreamDestroy(c->st);
+    delete c;
+    return KF_OK;
+}
+
+const char *kf_last_error(const kf_ctx *c) { return c ? c->err.c_str() : g_create_err.c_str(); }
+
+int kf_set_stream(kf_ctx *c, void *stream) {
+    return guarded(c, [&] {
+        CK(cudaStreamSynchronize(c->st));
+        if (c->own_stream) CK(cudaStreamDestroy(c->st));
+        if (stream) {
+            c->st = (cudaStream_t)stream;
+            c->own_stream = false;
+        } else {
+            CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+            c->own_stream = true;
+        }
+    });
+}
+
+int kf_synchronize(kf_ctx *c) {
+    return guarded(c, [&] { CK(cudaStreamSynchronize(c->st)); CK(cudaGetLastError()); });
+}
+
+int kf_set_state(kf_ctx *c, const double *ux, const double *uy, const double *uz, const double *s) {
+    return guarded(c, [&] {
+        if (!ux || !uy || !uz || !s) throw KfError{KF_ERR_ARG, "null state array"};
+        const double *src[4] = {ux, uy, uz, s};
+        for (int q = 0; q < 4; ++q) put_bulk(c, c->Y[q], src[q], 2 * c->Nc);
+        copy_state(c, c->Ys, c->Y);
+        CK(cudaStreamSynchronize(c->st));
+    });
+}
+
+int kf_get_state(kf_ctx *c, double *ux, double *uy, double *uz, double *s) {
+    return guarded(c, [&] {
+        double *dst[4] = {ux, uy, uz, s};
+        for (int q = 0; q < 4; ++q)
+            if (dst[q]) get_bulk(c, dst[q], c->Y[q], 2 * c->Nc);
+        CK(cudaStreamSynchronize(c->st));
+    });
+}
+
+int kf_set_sources(kf_ctx *c, const double *nd, const double *mask) {
+    return guarded(c, [&] {
+        if (nd) CK(cudaMemcpyAsync(c->nd, nd, 8 * c->N, cudaMemcpyHostToDevice, c->st));
+        if (mask) put_bulk(c, c->H, mask, c->N);
+        CK(cudaStreamSynchronize(c->st));
+    });
+}
+
+int kf_set_phi(kf_ctx *c, const double *phi) {
+    return guarded(c, [&] {
+        CK(cudaMemcpyAsync(c->phi, phi, 8 * c->N, cudaMemcpyHostToDevice, c->st));
+        CK(cudaStreamSynchronize(c->st));
+    });
+}
+
+int kf_get_phi(kf_ctx *c, double *phi) {
+    return guarded(c, [&] {
+        CK(cudaMemcpyAsync(phi, c->phi, 8 * c->N, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+    });
+}
+
+int kf_rhs_eval(kf_ctx *c, double t) {
+    (void)t;
+    return guarded(c, [&] {
+        copy_state(c, c->Ys, c->Y);
+        c->rhs_fn(c);
+        copy_state(c, c->Y, c->K);
+        copy_state(c, c->Ys, c->K);
+        CK(cudaStreamSynchronize(c->st));
+    });
+}
+
+int kf_rk4_steps(kf_ctx *c, int nsteps, double dt) {
+    return guarded(c, [&] {
+        if (nsteps < 0) throw KfError{KF_ERR_ARG, "nsteps < 0"};
+        for (int s = 0; s < nsteps; ++s) {
+            // Ys == Y on entry
+            c->rhs_fn(c);
+            rk_launch(c, 0.5 * dt, 0);
+            c->rhs_fn(c);
+            rk_launch(c, 0.5 * dt, 1);
+            c->rhs_fn(c);
+            rk_launch(c, 1.0 * dt, 1);
+            c->rhs_fn(c);
+            rk_launch(c, dt / 6., 2);
+            copy_state(c, c->Ys, c->Y);
+        }
+        CK(cudaGetLastError());
+    });
+}
+
+int kf_poisson_solve(kf_ctx *c, double *phi_io, const double *rho) {
+    int rc = guarded(c, [&] {
+        if (!phi_io || !rho) throw KfError{KF_ERR_ARG, "null array"};
+        CK(cudaMemcpyAsync(c->phi, phi_io, 8 * c->N, cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(c->rho, rho, 8 * c->N, cudaMemcpyHostToDevice, c->st));
+        int r = poisson(c);
+        CK(cudaMemcpyAsync(phi_io, c->phi, 8 * c->N, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        if (r) throw KfError{KF_ERR_NOT_CONVERGED, "Poisson solve did not reach its tolerance"};
+    });
+    return rc;
+}
+
+int kf_diag(kf_ctx *c, kf_diag_out *out) {
+    return guarded(c, [&] {
+        if (!out) throw KfError{KF_ERR_ARG, "null output"};
+        c->inv_state_fn(c);
+        const int nb = red_blocks(c->N);
+        if (c->fp32)
+            k_diag_sums<float><<<nb, RBS, 0, c->st>>>((const float *)c->R[23], (const float *)c->R[20],
+                                                     (const float *)c->R[21], (const float *)c->R[22], c->phi, c->nd,
+                                                     c->cfg.M, c->N, c->partial);
+        else
+            k_diag_sums<double><<<nb, RBS, 0, c->st>>>((const double *)c->R[23], (const double *)c->R[20],
+                                                      (const double *)c->R[21], (const double *)c->R[22], c->phi,
+                                                      c->nd, c->cfg.M, c->N, c->partial);
+        k_diag_final<<<1, 32, 0, c->st>>>(c->partial, nb, c->red);
+        c->launches += 2;
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(c->h_red, c->red, sizeof(double) * 2, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        const double h = c->cfg.L / c->n, h3 = h * h * h;
+        *out = c->diag;
+        out->kinetic = c->h_red[0] * h3;
+        out->charge = c->h_red[1] * h3;
+    });
+}
+
+int kf_fft_r2c(kf_ctx *c, const double *in, double *out) {
+    return guarded(c, [&] {
+        put_bulk(c, c->R[0], in, c->N);
+        c->r2c_fn(c);
+        get_bulk(c, out, c->CX[0], 2 * c->Nc);
+        CK(cudaStreamSynchronize(c->st));
+    });
+}
+
+int kf_fft_c2r(kf_ctx *c, const double *in, double *out) {
+    return guarded(c, [&] {
+        put_bulk(c, c->CX[0], in, 2 * c->Nc);
+        c->c2r_fn(c);
+        get_bulk(c, out, c->R[0], c->N);
+        CK(cudaStreamSynchronize(c->st));
+    });
+}
+
+int kf_state_device_ptrs(kf_ctx *c, void **ux, void **uy, void **uz, void **s) {
+    return guarded(c, [&] {
+        void **o[4] = {ux, uy, uz, s};
+        for (int q = 0; q < 4; ++q)
+            if (o[q]) *o[q] = c->Y[q];
+    });
+}
+
+long long kf_launch_count(const kf_ctx *c) { return c ? c->launches : -1; }
+
+}  // extern "C"

@@ -1,0 +1,336 @@
+// kf_passes.cuh -- the transform passes of the spectral right-hand side.
+//
+// A 3-D real transform of the reference's layout (real n^3, half spectrum
+// n x n x (n/2+1), z fastest; field_base.hpp:23-24, field_imag.cpp:16) is done
+// in three passes, each one read and one write of HBM:
+//   inverse : x pass (complex) -> y pass (complex) -> z pass (c2r, x 1/N)
+//   forward : z pass (r2c)     -> y pass (complex) -> x pass (complex)
+// The x and y passes load a tile of TC contiguous columns by the whole line
+// (coalesced 128-byte row segments), transform it with the Stockham engine and
+// store it back in place of the same tile of another buffer.  The z passes
+// pack two real rows into one complex line (z = a + i b).  Loads apply the
+// spectral multipliers of the right-hand side (2/3 mask, i k) so derivative
+// fields are generated on the fly instead of being written out.
+#pragma once
+
+#include "kf_fft.cuh"
+#include "kf_types.cuh"
+
+namespace kf {
+
+template <typename T> struct Tile { static constexpr int TC = sizeof(T) == 8 ? 8 : 16; };
+
+template <typename T2>
+__device__ __forceinline__ T2 mul_ik(T2 a, decltype(T2::x) k) {  // i k a
+    return mk<T2>(-k * a.y, k * a.x);
+}
+
+// --------------------------------------------------------------- x / y pass
+// axis 0: columns are the flattened (j, kz) plane, line index i, stride n*nzc.
+// axis 1: columns are kz within an x-plane, line index j, stride nzc.
+// gridDim.x = njobs * ntiles (job fastest so that jobs sharing an input run
+// together and hit L2).
+template <typename T, int N, int SIGN>
+__global__ void __launch_bounds__(Tile<T>::TC * Plan<N>::P)
+k_axis_pass(const AxisJob *__restrict__ jobs, int njobs, int axis, Geo<T> g,
+            const typename C2<T>::type *__restrict__ tw) {
+    typedef typename C2<T>::type T2;
+    constexpr int TC = Tile<T>::TC, P = Plan<N>::P, E = N / P;
+    extern __shared__ __align__(16) unsigned char kf_smem[];
+    T2 *sm = reinterpret_cast<T2 *>(kf_smem);
+    const int job = blockIdx.x % njobs, tile = blockIdx.x / njobs;
+    const AxisJob J = jobs[job];
+    const T2 *__restrict__ in = static_cast<const T2 *>(J.in);
+    T2 *__restrict__ out = static_cast<T2 *>(J.out);
+    const int c = threadIdx.x % TC, p = threadIdx.x / TC;
+    const int n = g.n, nzc = g.nzc;
+    long base;
+    long rstride;
+    int jj = 0, kk = 0;
+    bool valid;
+    if (axis == 0) {
+        const int col = tile * TC + c;
+        valid = col < n * nzc;
+        base = col;
+        rstride = (long)n * nzc;
+        jj = col / nzc;
+        kk = col - jj * nzc;
+    } else {
+        const int tpp = (nzc + TC - 1) / TC;
+        const int plane = tile / tpp;
+        kk = (tile - plane * tpp) * TC + c;
+        valid = kk < nzc;
+        base = (long)plane * n * nzc + kk;
+        rstride = nzc;
+    }
+    T2 v[E];
+#pragma unroll
+    for (int q = 0; q < E; ++q) {
+        const int row = reg_row<N, P, Plan<N>::R1>(p, q);
+        T2 x = valid ? in[base + row * rstride] : mk<T2>((T)0, (T)0);
+        if (J.mul == MUL_P || J.mul == MUL_P_IK) {
+            if (!dealias_keep(g.q2, row, jj, kk)) x = mk<T2>((T)0, (T)0);
+        }
+        if (J.mul == MUL_P_IK || J.mul == MUL_IK) x = mul_ik(x, g.kv[row]);
+        v[q] = x;
+    }
+    Plan<N>::template fft<T2, SIGN>(v, sm + c, TC, p, tw);
+    if (valid) {
+#pragma unroll
+        for (int q = 0; q < E; ++q) {
+            const int row = reg_row<N, P, Plan<N>::RL>(p, q);
+            out[base + row * rstride] = v[q];
+        }
+    }
+}
+
+// --------------------------------------------------------------- z c2r pass
+// LZ line pairs per block; thread = p + P*l.  Half rows are staged in shared
+// memory, multiplied, extended by Hermitian symmetry (the imaginary parts of
+// the kz = 0 and kz = n/2 bins are dropped, as a c2r transform does), packed
+// as A + iB, transformed backwards and written as two real rows scaled by
+// `scale` (the 1/N of OP_iFFT.cpp:59-61).
+template <typename T> struct ZTile { static constexpr int LZ = 8; };
+
+template <typename T, int N>
+__global__ void __launch_bounds__(ZTile<T>::LZ * Plan<N>::P)
+k_z_c2r(const ZJob *__restrict__ jobs, int njobs, int nrows, Geo<T> g,
+        const typename C2<T>::type *__restrict__ tw, T scale) {
+    typedef typename C2<T>::type T2;
+    constexpr int LZ = ZTile<T>::LZ, P = Plan<N>::P, E = N / P, NZC = N / 2 + 1;
+    constexpr int LS = N + 1;  // padded line stride of the exchange buffer
+    extern __shared__ __align__(16) unsigned char kf_smem[];
+    T2 *half = reinterpret_cast<T2 *>(kf_smem);  // [2][LZ][NZC]
+    T2 *xch = half + 2 * LZ * NZC;               // [LZ][LS]
+    const int job = blockIdx.x % njobs, tile = blockIdx.x / njobs;
+    const ZJob J = jobs[job];
+    const int r0 = tile * LZ;
+    const T2 *inA = static_cast<const T2 *>(J.inA);
+    const T2 *inB = static_cast<const T2 *>(J.inB);
+    for (int idx = threadIdx.x; idx < 2 * LZ * NZC; idx += blockDim.x) {
+        const int which = idx / (LZ * NZC);
+        const int rem = idx - which * LZ * NZC;
+        const int l = rem / NZC, k = rem - l * NZC;
+        const int r = r0 + l;
+        const T2 *src = which ? inB : inA;
+        const int mul = which ? J.mulB : J.mulA;
+        T2 x = mk<T2>((T)0, (T)0);
+        if (src && r < nrows) {
+            x = src[(long)r * NZC + k];
+            if (mul == MUL_IK) x = mul_ik(x, g.kv[k]);
+        }
+        if (k == 0 || 2 * k == N) x.y = (T)0;
+        half[idx] = x;
+    }
+    __syncthreads();
+    const int p = threadIdx.x % P, l = threadIdx.x / P;
+    const T2 *hA = half + l * NZC;
+    const T2 *hB = half + LZ * NZC + l * NZC;
+    T2 v[E];
+#pragma unroll
+    for (int q = 0; q < E; ++q) {
+        const int k = reg_row<N, P, Plan<N>::R1>(p, q);
+        T2 a, b;
+        if (k < NZC) {
+            a = hA[k];
+            b = hB[k];
+        } else {
+            a = hA[N - k];
+            b = hB[N - k];
+            a.y = -a.y;
+            b.y = -b.y;
+        }
+        v[q] = mk<T2>(a.x - b.y, a.y + b.x);  // A + iB
+    }
+    Plan<N>::template fft<T2, +1>(v, xch + l * LS, 1, p, tw);
+    const int r = r0 + l;
+    if (r < nrows) {
+        T *oA = static_cast<T *>(J.outA) + (long)r * N;
+        T *oB = J.outB ? static_cast<T *>(J.outB) + (long)r * N : nullptr;
+#pragma unroll
+        for (int q = 0; q < E; ++q) {
+            const int z = reg_row<N, P, Plan<N>::RL>(p, q);
+            oA[z] = v[q].x * scale;
+            if (oB) oB[z] = v[q].y * scale;
+        }
+    }
+}
+
+// --------------------------------------------------------------- z r2c pass
+template <typename T, int N>
+__global__ void __launch_bounds__(ZTile<T>::LZ * Plan<N>::P)
+k_z_r2c(const ZJob *__restrict__ jobs, int njobs, int nrows,
+        const typename C2<T>::type *__restrict__ tw) {
+    typedef typename C2<T>::type T2;
+    constexpr int LZ = ZTile<T>::LZ, P = Plan<N>::P, E = N / P, NZC = N / 2 + 1;
+    constexpr int LS = N + 1;
+    extern __shared__ __align__(16) unsigned char kf_smem[];
+    T2 *xch = reinterpret_cast<T2 *>(kf_smem);  // [LZ][LS]
+    const int job = blockIdx.x % njobs, tile = blockIdx.x / njobs;
+    const ZJob J = jobs[job];
+    const int r0 = tile * LZ;
+    const int p = threadIdx.x % P, l = threadIdx.x / P;
+    const int r = r0 + l;
+    const T *iA = static_cast<const T *>(J.inA);
+    const T *iB = static_cast<const T *>(J.inB);
+    T2 v[E];
+#pragma unroll
+    for (int q = 0; q < E; ++q) {
+        const int z = reg_row<N, P, Plan<N>::R1>(p, q);
+        T a = (T)0, b = (T)0;
+        if (r < nrows) {
+            a = iA[(long)r * N + z];
+            if (iB) b = iB[(long)r * N + z];
+        }
+        v[q] = mk<T2>(a, b);
+    }
+    T2 *line = xch + l * LS;
+    Plan<N>::template fft<T2, -1>(v, line, 1, p, tw);
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < E; ++q) line[reg_row<N, P, Plan<N>::RL>(p, q)] = v[q];
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < LZ * NZC; idx += blockDim.x) {
+        const int ll = idx / NZC, k = idx - ll * NZC;
+        const int rr = r0 + ll;
+        if (rr >= nrows) continue;
+        const T2 zk = xch[ll * LS + k];
+        const T2 zm = xch[ll * LS + (N - k) % N];
+        const T cr = zm.x, ci = -zm.y;  // conj(Z[N-k])
+        T2 *oA = static_cast<T2 *>(J.outA) + (long)rr * NZC;
+        oA[k] = mk<T2>((T)0.5 * (zk.x + cr), (T)0.5 * (zk.y + ci));
+        if (J.outB) {
+            T2 *oB = static_cast<T2 *>(J.outB) + (long)rr * NZC;
+            oB[k] = mk<T2>((T)0.5 * (zk.y - ci), (T)-0.5 * (zk.x - cr));
+        }
+    }
+}
+
+// --------------------------------------------- spectral linear terms (FB parts)
+// lin_q is the part of rhs_standard's FBuffer_q (the negated right-hand side)
+// that is computed in k-space, in the reference's order of accumulation:
+//   u_c: (tau+SV) u^ [+ D|k|^2 u^] + i k_c (PF phi^ + s^/theta) + M i k_x P u^
+//        (rhs_standard.cpp:119-140, 218-248, 279-295)
+//   s  : SV s^ [+ D|k|^2 s^] + M i k_x P s^ + i k.P u^
+//        (rhs_standard.cpp:135-139, 304-319)
+template <typename T>
+__device__ __forceinline__ typename C2<T>::type lin_term(const RhsArgs<T> &a, const Geo<T> &g, int q,
+                                                         int i, int j, int k, long idx) {
+    typedef typename C2<T>::type T2;
+    const int Tm = a.terms;
+    const bool P = dealias_keep(g.q2, i, j, k);
+    const T kx = g.kv[i], ky = g.kv[j], kz = g.kv[k];
+    const T sv = a.SV[idx];
+    T2 fb;
+    if (q < 3) {
+        const T2 u = a.Y[q][idx];
+        const bool diss = Tm & T_DISSIPATION, svo = Tm & T_SVISCOSITY;
+        const T cf = diss && svo ? (a.tau + sv) : diss ? a.tau : svo ? sv : (T)0;
+        fb = mk<T2>(cf * u.x, cf * u.y);
+        if (Tm & T_DIFFUSION) {
+            const T k2 = kx * kx + ky * ky + kz * kz;
+            fb.x += a.D * k2 * u.x;
+            fb.y += a.D * k2 * u.y;
+        }
+        const bool pres = Tm & T_PRESSURE, eint = Tm & T_E_INT;
+        if (pres || eint) {
+            T2 F1 = mk<T2>((T)0, (T)0);
+            if (eint) {
+                F1 = a.phihat[idx];
+                if (pres) { const T pf = a.PF[idx]; F1.x *= pf; F1.y *= pf; }
+            }
+            if (pres) {
+                const T2 s = a.Y[3][idx];
+                F1.x += s.x / a.theta;
+                F1.y += s.y / a.theta;
+            }
+            const T kc = q == 0 ? kx : q == 1 ? ky : kz;
+            const T2 d = mul_ik(F1, kc);
+            fb.x += d.x;
+            fb.y += d.y;
+        }
+        if ((Tm & T_E_EXT) && P) {
+            const T2 d = mul_ik(u, kx);
+            fb.x += a.M * d.x;
+            fb.y += a.M * d.y;
+        }
+    } else {
+        const T2 s = a.Y[3][idx];
+        const T cf = (Tm & T_SVISCOSITY) ? sv : (T)0;
+        fb = mk<T2>(cf * s.x, cf * s.y);
+        if (Tm & T_DIFFUSION) {
+            const T k2 = kx * kx + ky * ky + kz * kz;
+            fb.x += a.D * k2 * s.x;
+            fb.y += a.D * k2 * s.y;
+        }
+        if ((Tm & T_E_EXT) && P) {
+            const T2 d = mul_ik(s, kx);
+            fb.x += a.M * d.x;
+            fb.y += a.M * d.y;
+        }
+        if ((Tm & T_CONTINUITY) && P) {
+            const T2 dx = mul_ik(a.Y[0][idx], kx);
+            const T2 dy = mul_ik(a.Y[1][idx], ky);
+            const T2 dz = mul_ik(a.Y[2][idx], kz);
+            fb.x += dx.x; fb.y += dx.y;
+            fb.x += dy.x; fb.y += dy.y;
+            fb.x += dz.x; fb.y += dz.y;
+        }
+    }
+    return fb;
+}
+
+// ------------------------------------ forward x pass + right-hand-side assembly
+// For each of the four output fields the forward x transform of the y-passed
+// product (or penalized) field is formed and combined per element:
+//   penalization off: K_q = -(lin_q + F_q)        (rhs_standard.cpp:538-560)
+//   penalization on : K_q = P(k) F_q              (the 2/3 filter after the
+//                     physical-space penalization, rhs_standard.cpp:491-532)
+// gridDim.x = number of column tiles; jobs[q].in = y-passed field, .out = K_q.
+template <typename T, int N>
+__global__ void __launch_bounds__(Tile<T>::TC * Plan<N>::P)
+k_xfwd_assemble(const AxisJob *__restrict__ jobs, Geo<T> g, RhsArgs<T> a,
+                const typename C2<T>::type *__restrict__ tw) {
+    typedef typename C2<T>::type T2;
+    constexpr int TC = Tile<T>::TC, P = Plan<N>::P, E = N / P;
+    extern __shared__ __align__(16) unsigned char kf_smem[];
+    T2 *sm = reinterpret_cast<T2 *>(kf_smem);
+    const int tile = blockIdx.x;
+    const int c = threadIdx.x % TC, p = threadIdx.x / TC;
+    const int n = g.n, nzc = g.nzc;
+    const int col = tile * TC + c;
+    const bool valid = col < n * nzc;
+    const long rstride = (long)n * nzc;
+    const int jj = col / nzc, kk = col - jj * nzc;
+    const bool pen = a.terms & T_PENALIZATION;
+    for (int q = 0; q < 4; ++q) {
+        const T2 *__restrict__ in = static_cast<const T2 *>(jobs[q].in);
+        T2 *__restrict__ out = static_cast<T2 *>(jobs[q].out);
+        T2 v[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int row = reg_row<N, P, Plan<N>::R1>(p, e);
+            v[e] = valid ? in[col + row * rstride] : mk<T2>((T)0, (T)0);
+        }
+        Plan<N>::template fft<T2, -1>(v, sm + c, TC, p, tw);
+        if (valid) {
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const int i = reg_row<N, P, Plan<N>::RL>(p, e);
+                const long idx = col + i * rstride;
+                T2 F = v[e];
+                T2 K;
+                if (pen) {
+                    K = dealias_keep(g.q2, i, jj, kk) ? F : mk<T2>((T)0, (T)0);
+                } else {
+                    T2 fb = lin_term(a, g, q, i, jj, kk, idx);
+                    K = mk<T2>(-(fb.x + F.x), -(fb.y + F.y));
+                }
+                out[idx] = K;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace kf

@@ -1,0 +1,132 @@
+// kf_pointwise.cuh -- physical-space products, Poisson source, RK4 stage updates.
+#pragma once
+
+#include "kf_passes.cuh"
+#include "kf_types.cuh"
+
+namespace kf {
+
+// Physical-space nonlinear terms, one thread per grid point:
+//   A_c = U_x d_x U_c + U_y d_y U_c + U_z d_z U_c   (rhs_standard.cpp:403-436)
+//   B   = d_x s U_x + d_y s U_y + d_z s U_z          (rhs_standard.cpp:323-342)
+// With penalization the masking form (effect_penalization.cpp:35) is applied to
+// the physical right-hand side  r_q = c2r(-lin_q) - prod_q:
+//   f_q = (1-H) r_q + H eta (q_d - q_fix),  q_fix = (-M, 0, 0, -10).
+template <typename T> struct ProdArgs {
+    const T *U[3];
+    const T *dU[3][3];  // dU[c][d] = d_d U_c
+    const T *ds[3];     // d_d s
+    const T *rl[4];     // c2r(-lin_q)        (penalization only)
+    const T *sd;        // c2r(P s^)           (penalization only)
+    const T *H;         // mask               (penalization only)
+    T *out[4];
+    T M, eta;
+    int terms;
+    long N;
+};
+
+template <typename T>
+__global__ void k_products(ProdArgs<T> a) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.N) return;
+    const T ux = a.U[0][i], uy = a.U[1][i], uz = a.U[2][i];
+    T pr[4];
+    const bool adv = a.terms & T_ADVECTION, cont = a.terms & T_CONTINUITY;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        T s = (T)0;
+        if (adv) {
+            s = ux * a.dU[c][0][i];
+            s += uy * a.dU[c][1][i];
+            s += uz * a.dU[c][2][i];
+        }
+        pr[c] = s;
+    }
+    {
+        T s = (T)0;
+        if (cont) {
+            s = a.ds[0][i] * ux;
+            s += a.ds[1][i] * uy;
+            s += a.ds[2][i] * uz;
+        }
+        pr[3] = s;
+    }
+    if (a.terms & T_PENALIZATION) {
+        const T h = a.H[i];
+        const T qd[4] = {ux, uy, uz, a.sd[i]};
+        const T qfix[4] = {-a.M, (T)0, (T)0, (T)-10};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const T r = a.rl[q][i] - pr[q];
+            a.out[q][i] = ((T)1 - h) * r + h * a.eta * (qd[q] - qfix[q]);
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) a.out[q][i] = pr[q];
+    }
+}
+
+// rl_q = -lin_q in k-space (penalization path; one thread per half-spectrum element)
+template <typename T>
+__global__ void k_lin(RhsArgs<T> a, Geo<T> g, typename C2<T>::type *o0, typename C2<T>::type *o1,
+                      typename C2<T>::type *o2, typename C2<T>::type *o3) {
+    typedef typename C2<T>::type T2;
+    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long Nc = (long)g.n * g.n * g.nzc;
+    if (idx >= Nc) return;
+    const int k = (int)(idx % g.nzc);
+    const long r = idx / g.nzc;
+    const int j = (int)(r % g.n), i = (int)(r / g.n);
+    T2 *o[4] = {o0, o1, o2, o3};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        T2 fb = lin_term(a, g, q, i, j, k, idx);
+        o[q][idx] = mk<T2>(-fb.x, -fb.y);
+    }
+}
+
+// rho = exp(s_d) + n_d in FP64 (rhs_standard.cpp:108-111)
+template <typename T>
+__global__ void k_rho(const T *__restrict__ sd, const double *__restrict__ nd, double *__restrict__ rho, long N) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) rho[i] = exp((double)sd[i]) + nd[i];
+}
+
+// RK4 stage combinations (RKO4.cpp:140-238), accumulated as
+//   acc = k1; acc += 2 k2; acc += 2 k3;  y = y0 + dt/6 (acc + k4)
+// mode 0: acc = K, ys = y0 + c K;  1: acc += 2K, ys = y0 + c K;  2: y0 += d (acc + K)
+template <typename T>
+__global__ void k_rk(typename C2<T>::type *__restrict__ y0, typename C2<T>::type *__restrict__ acc,
+                     typename C2<T>::type *__restrict__ ys, const typename C2<T>::type *__restrict__ K,
+                     T cdt, int mode, long M) {
+    typedef typename C2<T>::type T2;
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= M) return;
+    const T2 k = K[i];
+    const T2 y = y0[i];
+    if (mode == 0) {
+        acc[i] = k;
+        ys[i] = mk<T2>(y.x + cdt * k.x, y.y + cdt * k.y);
+    } else if (mode == 1) {
+        T2 a = acc[i];
+        acc[i] = mk<T2>(a.x + (T)2 * k.x, a.y + (T)2 * k.y);
+        ys[i] = mk<T2>(y.x + cdt * k.x, y.y + cdt * k.y);
+    } else {
+        T2 a = acc[i];
+        y0[i] = mk<T2>(y.x + cdt * (a.x + k.x), y.y + cdt * (a.y + k.y));
+    }
+}
+
+// FP64 <-> bulk precision conversion of interleaved complex / real arrays
+template <typename T>
+__global__ void k_from_f64(T *__restrict__ dst, const double *__restrict__ src, long M) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < M) dst[i] = (T)src[i];
+}
+template <typename T>
+__global__ void k_to_f64(double *__restrict__ dst, const T *__restrict__ src, long M) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < M) dst[i] = (double)src[i];
+}
+
+}  // namespace kf

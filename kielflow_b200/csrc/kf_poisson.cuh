@@ -1,0 +1,358 @@
+// kf_poisson.cuh -- FP64 kernels of the nonlinear Boltzmann-electron Poisson solve
+//   lap_h phi = exp(phi) - rho,   rho = exp(s) + n_d
+// (rhs_standard.cpp:100-113; solver_poisson_jacobi_nlin.cpp:140-265).
+//
+// The point update is the reference's: with the 7-point coefficients of the
+// axis spacings H[i] = x_i - x_{i-1},
+//   D = sum_axes 2/(H[i+1] H[i]),  A = 2 sum_nb phi_nb / (H(H[i+1]+H[i])) + rho,
+// phi_new solves A - D x - e^x = 0 by the damped Newton of newton_method.hpp:16-63.
+// Products and sums are spelled with __d*_rn intrinsics where the reference's
+// order must not be contracted into FMAs, so that the GPU reproduces the CPU
+// arithmetic up to the last-bit differences of exp().
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace kf {
+
+struct Lev {
+    int n;
+    const double *dd;  // 2/(H[i+1] H[i])
+    const double *dp;  // H[i+1] (H[i+1] + H[i])
+    const double *dm;  // H[i]   (H[i+1] + H[i])
+};
+
+__device__ __forceinline__ int wrapi(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+__device__ __forceinline__ long lidx(int i, int j, int k, int n) { return (long)k + n * ((long)j + (long)i * n); }
+
+__device__ __forceinline__ void point_coeffs(const double *__restrict__ p, const double *__restrict__ rho,
+                                             const Lev &L, int i, int j, int k, double &A, double &D) {
+    const int n = L.n;
+    D = __dadd_rn(__dadd_rn(L.dd[i], L.dd[j]), L.dd[k]);
+    A = p[lidx(wrapi(i + 1, n), j, k, n)] / L.dp[i];
+    A = __dadd_rn(A, p[lidx(wrapi(i - 1, n), j, k, n)] / L.dm[i]);
+    A = __dadd_rn(A, p[lidx(i, wrapi(j + 1, n), k, n)] / L.dp[j]);
+    A = __dadd_rn(A, p[lidx(i, wrapi(j - 1, n), k, n)] / L.dm[j]);
+    A = __dadd_rn(A, p[lidx(i, j, wrapi(k + 1, n), n)] / L.dp[k]);
+    A = __dadd_rn(A, p[lidx(i, j, wrapi(k - 1, n), n)] / L.dm[k]);
+    A = __dmul_rn(2., A);
+    if (rho) A = __dadd_rn(A, rho[lidx(i, j, k, n)]);
+}
+
+__device__ __forceinline__ double f_point(double A, double D, double x) {
+    return __dsub_rn(__dsub_rn(A, __dmul_rn(D, x)), exp(x));
+}
+
+// newton_method::solve (newton_method.hpp:16-63), eps 0.05, Nmax 20, g 0.8
+__device__ __forceinline__ double newton_point(double x, double A, double D) {
+    const double g = 0.8;
+    double omega = 1.;
+    double dx = 0.;
+    double ex = exp(x);
+    double dx_alt = __dsub_rn(__dsub_rn(A, __dmul_rn(D, x)), ex) / __dsub_rn(-D, ex);
+    int i = 0;
+    do {
+        x = __dsub_rn(x, __dmul_rn(omega, dx));
+        ex = exp(x);
+        dx = __dsub_rn(__dsub_rn(A, __dmul_rn(D, x)), ex) / __dsub_rn(-D, ex);
+        omega = fabs(dx) > fabs(dx_alt) ? __dmul_rn(g, omega) : __dadd_rn(__dmul_rn(1. - g, omega), g * 1.);
+        dx_alt = dx;
+        ++i;
+    } while (fabs(dx) > 0.05 && i < 20);
+    return __dsub_rn(x, dx);
+}
+
+// ------------------------------------------------------------ reductions
+// Block partials of the Jacobi sweep statistics; slot layout per block:
+// [0] max|dP|, [1] sum|dP|, [2] max P_new, [3] min P_new, [4] max|f(P_old)|
+constexpr int KF_RED = 5;
+
+// NaN-propagating max / min (fmax alone would drop a NaN)
+__device__ __forceinline__ double nmax(double a, double b) { return (a != a || b != b) ? a + b : fmax(a, b); }
+__device__ __forceinline__ double nmin(double a, double b) { return (a != a || b != b) ? a + b : fmin(a, b); }
+
+template <int BS>
+__device__ __forceinline__ void block_reduce5(double v[KF_RED], double *sh, double *out) {
+    // sh: [KF_RED][BS]
+    for (int s = 0; s < KF_RED; ++s) sh[s * BS + threadIdx.x] = v[s];
+    __syncthreads();
+    for (int w = BS / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) {
+            double *a = sh + threadIdx.x, *b = sh + threadIdx.x + w;
+            a[0] = nmax(a[0], b[0]);
+            a[BS] = __dadd_rn(a[BS], b[BS]);
+            a[2 * BS] = nmax(a[2 * BS], b[2 * BS]);
+            a[3 * BS] = nmin(a[3 * BS], b[3 * BS]);
+            a[4 * BS] = nmax(a[4 * BS], b[4 * BS]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int s = 0; s < KF_RED; ++s) out[s] = sh[s * BS];
+}
+
+// Jacobi sweep (iteration_loop, solver_poisson_jacobi_nlin.cpp:140-235)
+template <int BS>
+__global__ void __launch_bounds__(BS) k_jacobi(const double *__restrict__ in, double *__restrict__ out,
+                                               const double *__restrict__ rho, Lev L, double omega,
+                                               double *__restrict__ partial) {
+    __shared__ double sh[KF_RED * BS];
+    const int n = L.n;
+    const long N = (long)n * n * n;
+    double v[KF_RED] = {0., 0., -INFINITY, INFINITY, 0.};
+    if (blockIdx.x == 0 && threadIdx.x == 0) v[2] = v[3] = in[0];  // supremum = infinum = in.val[0] (:158-159)
+    for (long id = (long)blockIdx.x * BS + threadIdx.x; id < N; id += (long)gridDim.x * BS) {
+        const int k = (int)(id % n);
+        const long r = id / n;
+        const int j = (int)(r % n), i = (int)(r / n);
+        double A, D;
+        point_coeffs(in, rho, L, i, j, k, A, D);
+        const double P_old = in[id];
+        const double f0 = f_point(A, D, P_old);
+        const double P_new = newton_point(P_old, A, D);
+        const double delta = fabs(__dsub_rn(P_new, P_old));
+        out[id] = __dadd_rn(__dmul_rn(1. - omega, P_old), __dmul_rn(omega, P_new));
+        v[0] = nmax(v[0], delta);
+        v[1] = __dadd_rn(v[1], delta);
+        v[2] = nmax(v[2], P_new);
+        v[3] = nmin(v[3], P_new);
+        v[4] = nmax(v[4], fabs(f0));
+    }
+    block_reduce5<BS>(v, sh, partial + (long)blockIdx.x * KF_RED);
+}
+
+// Final fixed-order reduction of nb block partials into out[0..4].
+template <int BS>
+__global__ void __launch_bounds__(BS) k_reduce_final(const double *__restrict__ partial, int nb,
+                                                     double *__restrict__ out) {
+    __shared__ double sh[KF_RED * BS];
+    double v[KF_RED] = {0., 0., -INFINITY, INFINITY, 0.};
+    for (int b = threadIdx.x; b < nb; b += BS) {
+        const double *p = partial + (long)b * KF_RED;
+        v[0] = nmax(v[0], p[0]);
+        v[1] = __dadd_rn(v[1], p[1]);
+        v[2] = nmax(v[2], p[2]);
+        v[3] = nmin(v[3], p[3]);
+        v[4] = nmax(v[4], p[4]);
+    }
+    block_reduce5<BS>(v, sh, out);
+}
+
+// Pointwise residual r = f(phi) = lap_h phi + rho - e^phi (+ block max |r|, NaN-propagating)
+template <int BS>
+__global__ void __launch_bounds__(BS) k_residual(const double *__restrict__ phi, const double *__restrict__ rho,
+                                                 Lev L, double *__restrict__ r, double *__restrict__ partial) {
+    __shared__ double sh[KF_RED * BS];
+    const int n = L.n;
+    const long N = (long)n * n * n;
+    double v[KF_RED] = {0., 0., -INFINITY, INFINITY, 0.};
+    for (long id = (long)blockIdx.x * BS + threadIdx.x; id < N; id += (long)gridDim.x * BS) {
+        const int k = (int)(id % n);
+        const long rr = id / n;
+        const int j = (int)(rr % n), i = (int)(rr / n);
+        double A, D;
+        point_coeffs(phi, rho, L, i, j, k, A, D);
+        const double f = f_point(A, D, phi[id]);
+        if (r) r[id] = f;
+        const double af = fabs(f);
+        v[4] = nmax(v[4], af);
+        v[1] = __dadd_rn(v[1], af);
+    }
+    block_reduce5<BS>(v, sh, partial + (long)blockIdx.x * KF_RED);
+}
+
+// Red-black point-Newton Gauss-Seidel half sweep (colour (i+j+k)%2), omega = 1.
+__global__ void k_rbgs(double *__restrict__ phi, const double *__restrict__ rho, Lev L, int color) {
+    const int n = L.n, nh = n / 2;
+    const long M = (long)n * n * nh;
+    const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= M) return;
+    const int k2 = (int)(id % nh);
+    const long r = id / nh;
+    const int j = (int)(r % n), i = (int)(r / n);
+    const int k = 2 * k2 + ((i + j + color) & 1);
+    double A, D;
+    point_coeffs(phi, rho, L, i, j, k, A, D);
+    const long q = lidx(i, j, k, n);
+    phi[q] = newton_point(phi[q], A, D);
+}
+
+// Coarsest-level solve in one block: red-black sweeps until max |f| <= tol.
+__global__ void __launch_bounds__(1024) k_coarse_solve(double *__restrict__ phi, const double *__restrict__ rho,
+                                                       Lev L, double tol, int max_sweeps,
+                                                       int *__restrict__ sweeps_out) {
+    __shared__ double sh[32];
+    const int n = L.n;
+    const long N = (long)n * n * n;
+    int s = 0;
+    for (;; ++s) {
+        double m = 0.;
+        for (long id = threadIdx.x; id < N; id += blockDim.x) {
+            const int k = (int)(id % n);
+            const long r = id / n;
+            const int j = (int)(r % n), i = (int)(r / n);
+            double A, D;
+            point_coeffs(phi, rho, L, i, j, k, A, D);
+            const double af = fabs(f_point(A, D, phi[id]));
+            m = (af != af) ? af : fmax(m, af);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            double t = __shfl_xor_sync(0xffffffffu, m, o);
+            m = (t != t) ? t : fmax(m, t);
+        }
+        if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = m;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            double t = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.;
+            for (int o = 16; o > 0; o >>= 1) {
+                double u = __shfl_xor_sync(0xffffffffu, t, o);
+                t = (u != u) ? u : fmax(t, u);
+            }
+            if (threadIdx.x == 0) sh[0] = t;
+        }
+        __syncthreads();
+        const double res = sh[0];
+        __syncthreads();
+        if (!(res > tol) || s >= max_sweeps) break;  // converged, NaN or capped
+        for (int color = 0; color < 2; ++color) {
+            const long M = N / 2;
+            for (long id = threadIdx.x; id < M; id += blockDim.x) {
+                const int nh = n / 2;
+                const int k2 = (int)(id % nh);
+                const long r = id / nh;
+                const int j = (int)(r % n), i = (int)(r / n);
+                const int k = 2 * k2 + ((i + j + color) & 1);
+                double A, D;
+                point_coeffs(phi, rho, L, i, j, k, A, D);
+                const long q = lidx(i, j, k, n);
+                phi[q] = newton_point(phi[q], A, D);
+            }
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x == 0) *sweeps_out = s;
+}
+
+// Full-weighting restriction of r (fine n) and injection of phi:
+// rc = FW(r), phic = phic0 = phi[2i,2j,2k]  (field_interpolation.cpp:233-259 for phi)
+__global__ void k_restrict(const double *__restrict__ r, const double *__restrict__ phi, int nf,
+                           double *__restrict__ rc, double *__restrict__ phic, double *__restrict__ phic0) {
+    const int nc = nf / 2;
+    const long Mc = (long)nc * nc * nc;
+    const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= Mc) return;
+    const int k = (int)(id % nc);
+    const long rr = id / nc;
+    const int j = (int)(rr % nc), i = (int)(rr / nc);
+    const double w[3] = {0.25, 0.5, 0.25};
+    double s = 0.;
+    for (int a = -1; a <= 1; ++a) {
+        const int I = (2 * i + a + nf) % nf;
+        double sy = 0.;
+        for (int b = -1; b <= 1; ++b) {
+            const int J = (2 * j + b + nf) % nf;
+            double sz = 0.;
+            for (int c = -1; c <= 1; ++c) {
+                const int K = (2 * k + c + nf) % nf;
+                sz = __dadd_rn(sz, __dmul_rn(w[c + 1], r[lidx(I, J, K, nf)]));
+            }
+            sy = __dadd_rn(sy, __dmul_rn(w[b + 1], sz));
+        }
+        s = __dadd_rn(s, __dmul_rn(w[a + 1], sy));
+    }
+    rc[id] = s;
+    const double p = phi[lidx(2 * i, 2 * j, 2 * k, nf)];
+    phic[id] = p;
+    phic0[id] = p;
+}
+
+// rho_c = N_c(phi_c) + r_c with N(phi) = -lap_h phi + e^phi
+__global__ void k_fas_rhs(const double *__restrict__ phic, const double *__restrict__ rc, Lev L,
+                          double *__restrict__ rhoc) {
+    const int n = L.n;
+    const long N = (long)n * n * n;
+    const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= N) return;
+    const int k = (int)(id % n);
+    const long rr = id / n;
+    const int j = (int)(rr % n), i = (int)(rr / n);
+    double A, D;
+    point_coeffs(phic, nullptr, L, i, j, k, A, D);
+    const double Nc = __dsub_rn(0., f_point(A, D, phic[id]));
+    rhoc[id] = __dadd_rn(Nc, rc[id]);
+}
+
+// Trilinear prolongation of e = phic - phic0 in the z, y, x pass order of
+// OP_hto2h (field_interpolation.cpp:56-147), added to phi:  phi += P e.
+// gam[m] = (x_m - x_{m-1}) / (x_{m+1} - x_{m-1}) on the fine axis (odd m).
+__device__ __forceinline__ double e_c(const double *pc, const double *pc0, int nc, int I, int J, int K) {
+    const long q = lidx(I, J, K, nc);
+    return pc0 ? __dsub_rn(pc[q], pc0[q]) : pc[q];
+}
+__device__ __forceinline__ double pz(const double *pc, const double *pc0, const double *gam, int nf, int i, int j, int k) {
+    const int nc = nf / 2;
+    if ((k & 1) == 0) return e_c(pc, pc0, nc, i / 2, j / 2, k / 2);
+    const double g = gam[k];
+    const int k1 = (k - 1) / 2, k2 = ((k + 1) % nf) / 2;
+    return __dadd_rn(__dmul_rn(1. - g, e_c(pc, pc0, nc, i / 2, j / 2, k1)), __dmul_rn(g, e_c(pc, pc0, nc, i / 2, j / 2, k2)));
+}
+__device__ __forceinline__ double py(const double *pc, const double *pc0, const double *gam, int nf, int i, int j, int k) {
+    if ((j & 1) == 0) return pz(pc, pc0, gam, nf, i, j, k);
+    const double g = gam[j];
+    return __dadd_rn(__dmul_rn(1. - g, pz(pc, pc0, gam, nf, i, j - 1, k)),
+                     __dmul_rn(g, pz(pc, pc0, gam, nf, i, (j + 1) % nf, k)));
+}
+__global__ void k_prolong_add(double *__restrict__ phi, const double *__restrict__ pc, const double *__restrict__ pc0,
+                              const double *__restrict__ gam, int nf) {
+    const long N = (long)nf * nf * nf;
+    const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= N) return;
+    const int k = (int)(id % nf);
+    const long rr = id / nf;
+    const int j = (int)(rr % nf), i = (int)(rr / nf);
+    double e;
+    if ((i & 1) == 0) {
+        e = py(pc, pc0, gam, nf, i, j, k);
+    } else {
+        const double g = gam[i];
+        e = __dadd_rn(__dmul_rn(1. - g, py(pc, pc0, gam, nf, i - 1, j, k)),
+                      __dmul_rn(g, py(pc, pc0, gam, nf, (i + 1) % nf, j, k)));
+    }
+    phi[id] = __dadd_rn(phi[id], e);
+}
+
+// Strided injection (OP_2htoh_lvl0 / OP_4htoh / OP_8htoh)
+__global__ void k_inject(const double *__restrict__ in, int nf, int step, double *__restrict__ out) {
+    const int nc = nf / step;
+    const long M = (long)nc * nc * nc;
+    const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= M) return;
+    const int k = (int)(id % nc);
+    const long rr = id / nc;
+    const int j = (int)(rr % nc), i = (int)(rr / nc);
+    out[id] = in[lidx(step * i, step * j, step * k, nf)];
+}
+
+// OP_hto2h (plain, not a correction): out(2n) = trilinear(in(n)); used by the
+// cascadic plan.  Same pass order as k_prolong_add with phic0 == 0.
+__global__ void k_prolong_set(double *__restrict__ out, const double *__restrict__ pc,
+                              const double *__restrict__ gam, int nf) {
+    const double *zero = nullptr;
+    const long N = (long)nf * nf * nf;
+    const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= N) return;
+    const int k = (int)(id % nf);
+    const long rr = id / nf;
+    const int j = (int)(rr % nf), i = (int)(rr / nf);
+    double e;
+    if ((i & 1) == 0) {
+        e = py(pc, zero, gam, nf, i, j, k);
+    } else {
+        const double g = gam[i];
+        e = __dadd_rn(__dmul_rn(1. - g, py(pc, zero, gam, nf, i - 1, j, k)),
+                      __dmul_rn(g, py(pc, zero, gam, nf, (i + 1) % nf, j, k)));
+    }
+    out[id] = e;
+}
+
+}  // namespace kf

@@ -112,7 +112,7 @@ def noise_spectrum(n: int, seed: int, stream: int, amp: float = 1e-3, kmax: int 
 def initial_state(n: int, seed: int = 0, amp: float = 1e-3, kmax: int = 4):
     """(FUx, FUy, FUz, Fs): spectral u' (noise) and s = ln(1 + noise)."""
     Hu = [noise_spectrum(n, seed, q, amp, kmax) for q in range(3)]
-    eps_n = np.fft.irfftn(noise_spectrum(n, seed, 3, amp, kmax), s=(n, n, n))
+    eps_n = np.fft.irfftn(noise_spectrum(n, seed, 3, amp, kmax), s=(n, n, n), axes=(0, 1, 2))
     s = np.log1p(eps_n)
     Fs = np.fft.rfftn(s)
     return Hu[0], Hu[1], Hu[2], Fs
@@ -139,8 +139,8 @@ def cfl_dt(state, n: int, L: float, M: float, cfl: float = 0.2) -> float:
     """dt = cfl * h / max(|M + u'_x|, |u'_y|, |u'_z|) from the initial state,
     then held fixed (the reference's RK4 keeps dt_ fixed, RKO4.cpp:41-47)."""
     h = L / n
-    ux = np.fft.irfftn(state[0], s=(n, n, n))
-    uy = np.fft.irfftn(state[1], s=(n, n, n))
-    uz = np.fft.irfftn(state[2], s=(n, n, n))
+    ux = np.fft.irfftn(state[0], s=(n, n, n), axes=(0, 1, 2))
+    uy = np.fft.irfftn(state[1], s=(n, n, n), axes=(0, 1, 2))
+    uz = np.fft.irfftn(state[2], s=(n, n, n), axes=(0, 1, 2))
     vmax = max(np.abs(M + ux).max(), np.abs(uy).max(), np.abs(uz).max())
     return float(cfl * h / vmax)

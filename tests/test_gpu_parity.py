@@ -1,0 +1,161 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Tolerances: FP64 path 1e-12 relative (max-norm, per field) unless a test
+states otherwise; FP32-bulk path against the FP64 oracle 1e-5 relative.
+"""
+import numpy as np
+import pytest
+
+import kielflow_b200 as kf
+from kielflow_b200 import configs as C
+from kielflow_b200 import inputs as I
+from oracle import bind
+
+pytestmark = pytest.mark.gpu
+
+L = I.L_DEFAULT
+TOL64 = 1e-12
+TOL32 = 1e-5
+
+
+def rel(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def oracle_for(cfg):
+    return bind.Oracle(bind.KfoConfig(*[getattr(cfg, f) for f, _ in bind.KfoConfig._fields_]))
+
+
+@pytest.mark.parametrize("n", [16, 32, 64, 96, 128, 256])
+@pytest.mark.parametrize("prec", [kf.KF_FP64, kf.KF_FP32_BULK])
+def test_fft_r2c_c2r_vs_oracle(n, prec):
+    rng = np.random.default_rng(n)
+    x = rng.standard_normal((n, n, n))
+    with kf.Context(kf.Config.make(n, L, 0.8, precision=prec)) as ctx:
+        F = ctx.r2c(x)
+        Fo = bind.r2c(x)
+        tol = TOL64 if prec == kf.KF_FP64 else TOL32
+        assert rel(F, Fo) < tol / 10
+        xb = ctx.c2r(Fo)
+        assert rel(xb, bind.c2r(Fo)) < tol / 10
+        assert rel(xb, x) < tol / 10
+
+
+RHS_CASES = {
+    "linear": kf.KF_T_DISSIPATION | kf.KF_T_SVISCOSITY | kf.KF_T_PRESSURE | kf.KF_T_E_EXT | kf.KF_T_DIFFUSION,
+    "advection": kf.KF_T_ADVECTION,
+    "continuity": kf.KF_T_CONTINUITY,
+    "penalized": kf.KF_T_ADVECTION | kf.KF_T_CONTINUITY | kf.KF_T_E_EXT | kf.KF_T_PENALIZATION,
+    "shipped_jacobi": kf.KF_T_SHIPPED,
+    "all_jacobi": kf.KF_T_ALL,
+}
+
+
+@pytest.mark.parametrize("case", list(RHS_CASES))
+@pytest.mark.parametrize("n", [32, 64])
+def test_rhs_vs_oracle(case, n):
+    w = C.WORKLOADS["jacobi32"]
+    st, nd, mask, dt = C.make_inputs(w, n=n, seed=2)
+    cfg = C.config_for(w, n=n, terms=RHS_CASES[case], sv_cut=0.6)
+    with kf.Context(cfg) as ctx:
+        ctx.set_state(*st)
+        ctx.set_sources(nd, mask)
+        ctx.rhs()
+        g = ctx.get_state()
+        gphi = ctx.get_phi()
+    o = oracle_for(cfg)
+    o.set_state(st)
+    o.set_sources(nd, mask)
+    o.rhs()
+    r = o.get_state()
+    for q in range(4):
+        assert rel(g[q], r[q]) < TOL64, (case, q, rel(g[q], r[q]))
+    if RHS_CASES[case] & kf.KF_T_POISSON:
+        assert rel(gphi, o.get_phi()) < TOL64
+
+
+@pytest.mark.parametrize("mode", [kf.KF_PS_JACOBI_RES, kf.KF_PS_FAS, kf.KF_PS_CASCADIC, kf.KF_PS_JACOBI_REF])
+def test_poisson_vs_oracle(mode):
+    n = 32
+    st = I.initial_state(n, seed=5)
+    nd = I.gauss_charge(n, L, -10.0, 0.5)
+    rho = np.exp(np.fft.irfftn(st[3], s=(n, n, n), axes=(0, 1, 2))) + nd
+    cfg = kf.Config.make(n, L, 0.8, poisson_mode=mode, nlj_max_it=100000 if mode == 1 else 200,
+                         nlj_limit=1e-9, mg_levels=2, res_tol=1e-11)
+    with kf.Context(cfg) as ctx:
+        pg = ctx.poisson(np.zeros((n, n, n)), rho)
+        dg = ctx.diag()
+    o = oracle_for(cfg)
+    po = o.poisson(np.zeros((n, n, n)), rho)
+    so = o.stats()
+    assert rel(pg, po) < TOL64
+    if mode in (kf.KF_PS_JACOBI_RES, kf.KF_PS_FAS):
+        assert dg.last_residual <= 1e-11
+        assert dg.last_iterations == so.last_iterations
+
+
+def test_rk4_jacobi32_20_steps():
+    """Workload jacobi32 (32^3, FP64, Jacobi to residual 1e-10): 20 RK4 steps."""
+    w = C.WORKLOADS["jacobi32"]
+    st, nd, mask, dt = C.make_inputs(w)
+    cfg = C.config_for(w)
+    with kf.Context(cfg) as ctx:
+        ctx.set_state(*st)
+        ctx.set_sources(nd, mask)
+        ctx.rk4(dt, 20)
+        g = ctx.get_state()
+        gphi = ctx.get_phi()
+    o = oracle_for(cfg)
+    o.set_state(st)
+    o.set_sources(nd, mask)
+    o.rk4(dt, 20)
+    r = o.get_state()
+    for q in range(4):
+        assert rel(g[q], r[q]) < TOL64, (q, rel(g[q], r[q]))
+    assert rel(gphi, o.get_phi()) < TOL64
+
+
+@pytest.mark.parametrize("n,steps", [(64, 3), (128, 1)])
+def test_rk4_fas_vs_oracle(n, steps):
+    """Workload fas128 physics (FP64, FAS V-cycles, SV beyond 0.6 k_max)."""
+    w = C.WORKLOADS["fas128"]
+    st, nd, mask, dt = C.make_inputs(w, n=n)
+    cfg = C.config_for(w, n=n)
+    with kf.Context(cfg) as ctx:
+        ctx.set_state(*st)
+        ctx.set_sources(nd, mask)
+        ctx.rk4(dt, steps)
+        g = ctx.get_state()
+        gphi = ctx.get_phi()
+    o = oracle_for(cfg)
+    o.set_state(st)
+    o.set_sources(nd, mask)
+    o.rk4(dt, steps)
+    r = o.get_state()
+    for q in range(4):
+        assert rel(g[q], r[q]) < TOL64, (q, rel(g[q], r[q]))
+    assert rel(gphi, o.get_phi()) < TOL64
+
+
+def test_fp32_bulk_vs_fp64_oracle():
+    n, steps = 64, 3
+    w = C.WORKLOADS["fp32bulk256"]
+    st, nd, mask, dt = C.make_inputs(w, n=n)
+    cfg32 = C.config_for(w, n=n)
+    cfg64 = C.config_for(w, n=n, precision=kf.KF_FP64)
+    with kf.Context(cfg32) as ctx:
+        ctx.set_state(*st)
+        ctx.set_sources(nd, mask)
+        ctx.rk4(dt, steps)
+        g = ctx.get_state()
+        gphi = ctx.get_phi()
+    o = oracle_for(cfg64)
+    o.set_state(st)
+    o.set_sources(nd, mask)
+    o.rk4(dt, steps)
+    r = o.get_state()
+    # compare in physical space: n = e^s, u = u'
+    for q in range(3):
+        assert rel(bind.c2r(g[q]), bind.c2r(r[q])) < 1e-3  # u' is a 1e-3 perturbation
+    assert rel(np.exp(bind.c2r(g[3])), np.exp(bind.c2r(r[3]))) < TOL32
+    assert rel(gphi, o.get_phi()) < TOL32

@@ -1,0 +1,130 @@
+"""The CPU oracle: FFT shim vs numpy, restatement vs the reference's own code.
+
+The reference ships no tests or golden vectors (it has no test directory), so
+the oracle is pinned two ways: against the reference compiled here from its
+own sources (oracle/_ref, bit for bit) and against the committed fixtures in
+tests/golden/ that make_golden.py wrote from that build.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from kielflow_b200 import configs as C
+from kielflow_b200 import inputs as I
+from oracle import bind
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+L = I.L_DEFAULT
+
+
+def _gold(name):
+    return np.load(os.path.join(GOLD, name))
+
+
+@pytest.mark.parametrize("shape", [(4, 4, 4), (8, 6, 10), (16, 16, 16), (12, 24, 96), (32, 32, 32), (96, 8, 8)])
+def test_shim_fft_matches_numpy(shape):
+    rng = np.random.default_rng(sum(shape))
+    x = rng.standard_normal(shape)
+    Lb = bind.lib()
+    out = np.zeros(shape[:2] + (shape[2] // 2 + 1,), np.complex128)
+    Lb.kfs_r2c_3d(*shape, x.ctypes.data_as(bind._D), out.ctypes.data_as(bind._D))
+    ref = np.fft.rfftn(x)
+    assert np.abs(out - ref).max() <= 1e-15 * np.abs(ref).max() * 8
+    back = np.zeros(shape)
+    Lb.kfs_c2r_3d(*shape, ref.ctypes.data_as(bind._D), back.ctypes.data_as(bind._D))
+    assert np.abs(back / np.prod(shape) - x).max() <= 1e-15 * np.abs(x).max() * 8
+
+
+def test_oracle_ops_match_golden():
+    g = _gold("ops16.npz")
+    F = bind.r2c(g["x"])
+    assert np.array_equal(F, g["F"])
+    assert np.array_equal(bind.c2r(g["F"]), g["xb"])
+    o = bind.Oracle(bind.config(16, L, 0.8))
+    P, SV, PF = o.tables()
+    assert np.array_equal(g["F"] * P, g["dealiased"])
+    assert np.array_equal(g["F"] * PF, g["phifilt"])
+
+
+def test_oracle_transfer_matches_golden():
+    g = _gold("transfer.npz")
+    assert np.array_equal(bind.transfer(0, g["a8"], L), g["up"])
+    assert np.array_equal(bind.transfer(1, g["a16"], L), g["dn"])
+
+
+def test_oracle_jacobi_and_cascadic_match_golden():
+    g = _gold("poisson32.npz")
+    o = bind.Oracle(bind.config(32, L, 0.8, poisson_mode=bind.PS_JACOBI_REF, nlj_max_it=60, nlj_limit=1e-9))
+    phi = o.poisson(np.zeros((32, 32, 32)), g["rho"])
+    assert np.array_equal(phi, g["phi_jacobi60"])
+    o2 = bind.Oracle(bind.config(32, L, 0.8, poisson_mode=bind.PS_CASCADIC))
+    phi2 = o2.poisson(np.zeros((32, 32, 32)), g["rho"])
+    assert np.array_equal(phi2, g["phi_cascadic"])
+
+
+def test_oracle_shipped_rhs_and_rk4_match_golden():
+    g = _gold("shipped16.npz")
+    st = [g["s0_ux"], g["s0_uy"], g["s0_uz"], g["s0_s"]]
+    cfg = bind.config(int(g["n"]), L, float(g["M"]), tau=float(g["tau"]), theta=float(g["theta"]),
+                      terms=bind.KFO_SHIPPED, poisson_mode=bind.PS_CASCADIC)
+    o = bind.Oracle(cfg)
+    o.set_state(st)
+    o.set_sources(g["nd"], g["mask"])
+    o.rhs()
+    out = o.get_state()
+    for a, k in zip(out, ("rhs_ux", "rhs_uy", "rhs_uz", "rhs_s")):
+        assert np.array_equal(a, g[k]), k
+    assert np.array_equal(o.get_phi(), g["rhs_phi"])
+    o2 = bind.Oracle(cfg)
+    o2.set_state(st)
+    o2.set_sources(g["nd"], g["mask"])
+    o2.rk4(float(g["dt"]), int(g["nsteps"]))
+    for a, k in zip(o2.get_state(), ("rk_ux", "rk_uy", "rk_uz", "rk_s")):
+        assert np.array_equal(a, g[k]), k
+
+
+@pytest.mark.skipif(not bind.ref_available(), reason="reference not compiled here")
+def test_oracle_matches_reference_build_live():
+    """Same as the golden check, on a second seed, against the live reference build."""
+    n, M = 16, 1.1
+    st = I.initial_state(n, seed=11)
+    nd = I.gauss_charge(n, L, -5.0, 0.7)
+    mask = I.sphere_mask(n, L, 0.5)
+    R = bind.Reference(n, L, M, 0.2, 30.0, poisson_mode=1)
+    R.set_state(st)
+    R.set_real(0, nd)
+    R.set_real(1, mask)
+    R.rhs()
+    o = bind.Oracle(bind.config(n, L, M, tau=0.2, terms=bind.KFO_SHIPPED, poisson_mode=bind.PS_CASCADIC))
+    o.set_state(st)
+    o.set_sources(nd, mask)
+    o.rhs()
+    for a, b in zip(R.get_state(), o.get_state()):
+        assert np.array_equal(a, b)
+    assert np.array_equal(R.sv(), o.tables()[1])
+
+
+def test_oracle_fas_and_jacobi_agree_on_converged_phi():
+    """Both residual-stopped solvers reach the same discrete solution."""
+    n = 32
+    st = I.initial_state(n, seed=5)
+    nd = I.gauss_charge(n, L, -10.0, 0.5)
+    rho = np.exp(np.fft.irfftn(st[3], s=(n, n, n), axes=(0, 1, 2))) + nd
+    oj = bind.Oracle(bind.config(n, L, 0.8, poisson_mode=bind.PS_JACOBI_RES, nlj_max_it=100000, res_tol=1e-11))
+    of = bind.Oracle(bind.config(n, L, 0.8, poisson_mode=bind.PS_FAS, mg_levels=2, res_tol=1e-11))
+    pj = oj.poisson(np.zeros((n, n, n)), rho)
+    pf = of.poisson(np.zeros((n, n, n)), rho)
+    assert oj.residual(pj, rho) <= 1e-11 and of.residual(pf, rho) <= 1e-11
+    assert np.abs(pj - pf).max() < 1e-10
+
+
+def test_workload_inputs_are_deterministic():
+    w = C.WORKLOADS["jacobi32"]
+    a = C.make_inputs(w, n=16, seed=3)
+    b = C.make_inputs(w, n=16, seed=3)
+    for x, y in zip(a[0], b[0]):
+        assert np.array_equal(x, y)
+    assert a[3] == b[3]
+    u = np.fft.irfftn(a[0][0], s=(16, 16, 16), axes=(0, 1, 2))
+    assert 1e-4 < np.abs(u).max() < 1e-1
