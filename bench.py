@@ -1,0 +1,337 @@
+#!/usr/bin/env python
+"""RK4 time-step throughput of the kielflow hot path on B200.
+
+Workload (default ``fp32bulk256``): one RK4 step of the full right-hand side
+(R2C/C2R 3-D FFTs, 2/3 dealiasing, advection, continuity, E-force, pressure,
+friction, spectral viscosity beyond 0.6 k_max, Laplacian diffusion,
+penalization) and four FP64 nonlinear Poisson solves (FAS V-cycles, 4 levels,
+2+2 red-black point-Newton sweeps, residual <= 1e-10) on a 256^3 periodic box,
+FFTs / products / RK4 stages in FP32.  Metric: RK4 steps/s, with the plain
+FP64 path on the same workload and the relative phi error between the two.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 runs under torchrun, one independent replica (seed = rank) per GPU
+("replicas only": a single grid does not shard here); timing is the max over
+ranks of CUDA-event time on each rank's stream.  Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RK4 steps/s at 256^3 FP32-bulk vs plain FP64 on B200 at stated phi error; adj/fwd"
+UNIT = "steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="kf", choices=["kf", "reference"])
+    ap.add_argument("--workload", default="fp32bulk256")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison arm")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# --------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples (200 ms) during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-i", str(gpu_index), "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = [ln.strip().split(",") for ln in open(self.f.name) if ln.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower().startswith("active"):
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        loaded = [s for s in sm if s > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, or None."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    v = d.get(workload, {}).get(kernel)
+    return None if v is None else float(v)
+
+
+# --------------------------------------------------------------------- CPU leg
+def cpu_reference_rhs_seconds(nsamples: int, warmup: int, budget_s: float):
+    """The reference's own rhs_standard::solve (its sources compiled here,
+    shipped term set, cascadic multigrid plan of kielflow.cpp:207-217) at 128^3
+    with the workload's M, tau, dust; returns per-sample seconds."""
+    from kielflow_b200 import configs as C
+    from kielflow_b200 import inputs as I
+    from oracle import bind  # CPU baseline leg only
+    if not bind.ref_available():
+        return None, "oracle/_ref not built"
+    w = C.WORKLOADS["fp32bulk256"]
+    n = 128
+    st = I.initial_state(n, seed=0)
+    nd = I.gauss_charge(n, C.L_BOX, w["Q"], w["sigma"])
+    mask = I.sphere_mask(n, C.L_BOX, C.MASK_RADIUS)
+    R = bind.Reference(n, C.L_BOX, w["M"], w["tau"], C.THETA, poisson_mode=1)
+    R.set_real(0, nd)
+    R.set_real(1, mask)
+    times = []
+    t_start = time.time()
+    for i in range(warmup + nsamples):
+        R.set_state(st)
+        t0 = time.perf_counter()
+        R.rhs()
+        dt = time.perf_counter() - t0
+        if i >= warmup:
+            times.append(dt)
+        if time.time() - t_start > budget_s and times:
+            break
+    return times, None
+
+
+def cpu_baseline_entry(times, n_full=256, n_sample=128):
+    scale = (n_full / n_sample) ** 3
+    t = statistics.mean(times)
+    return {"value": 1.0 / (4.0 * scale * t), "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": (f"{len(times)} x rhs_standard::solve of the reference (its own sources, shipped "
+                       f"terms, cascadic MG) at {n_sample}^3, mean {t:.2f} s, scaled by the point "
+                       f"count ({scale:.0f}x) to one 256^3 RHS and by 4 RHS per RK4 step; single "
+                       f"thread (the reference has no parallel regions)")}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    times, err = cpu_reference_rhs_seconds(args.steps, min(args.warmup, 1), budget_s=150.0)
+    if times is None:
+        print(json.dumps({"impl": "reference", "unavailable": err}))
+        return 0
+    cb = cpu_baseline_entry(times)
+    v = cb["value"]
+    out = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": len(times),
+           "warmup": min(args.warmup, 1), "ms_per_step": 1000.0 / v, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": "fp32bulk256 (reference CPU path, sampled at 128^3)", "n": 256},
+           "impl": "reference", "cpu_baseline": cb,
+           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+    return 0
+
+
+# --------------------------------------------------------------------- GPU arm
+def run_kf(args):
+    import numpy as np
+    import torch
+
+    import kielflow_b200 as kf
+    from kielflow_b200 import configs as C
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    w = C.WORKLOADS[args.workload]
+    st, nd, mask, dt = C.make_inputs(w, seed=rank)
+    stream = torch.cuda.Stream()
+
+    def barrier():
+        if ws > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if ws == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed_arm(precision, profile=False, clocks=False):
+        cfg = C.config_for(w, precision=precision)
+        ctx = kf.Context(cfg)
+        ctx.set_stream(stream.cuda_stream)
+        ctx.set_state(*st)
+        ctx.set_sources(nd, mask)
+        ctx.rk4(dt, args.warmup)
+        ctx.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        sampler = ClockSampler(torch.cuda.current_device()) if clocks else None
+        if profile:
+            ctx.profile(True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = ctx.launch_count()
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            ctx.rk4(dt, args.steps)
+            e1.record(stream)
+        stream.synchronize()
+        torch.cuda.synchronize()
+        barrier()
+        launches = ctx.launch_count() - l0
+        prof = ctx.profile_read() if profile else None
+        if profile:
+            ctx.profile(False)
+        clk = sampler.stop() if sampler else None
+        ms = max_over_ranks(e0.elapsed_time(e1))
+        d = ctx.diag()
+        phi = ctx.get_phi()
+        return ctx, ms, launches, prof, clk, d, phi
+
+    ctx32, ms32, launches, prof, clk, d32, phi32 = timed_arm(w["precision"], profile=True, clocks=True)
+    value = ws * args.steps / (ms32 / 1000.0)
+
+    # end-to-end through the C ABI with host (pinned) buffers: H2D state, one
+    # RK4 step, D2H state, every step (interface_ode_solver::solve semantics)
+    shape_c = ctx32.shape_c
+    host = [torch.empty(shape_c, dtype=torch.complex128, pin_memory=True).numpy() for _ in range(4)]
+    for h, s in zip(host, st):
+        h[...] = s
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(args.e2e_steps):
+            ctx32.set_state(*host)
+            ctx32.rk4(dt, 1)
+            ctx32.get_state(host)
+        e1.record(stream)
+    stream.synchronize()
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1))
+    bytes_io = 4 * int(np.prod(shape_c)) * 16
+    e2e = {"value": ws * args.e2e_steps / (ms_e2e / 1000.0), "unit": UNIT, "h2d_bytes_per_step": bytes_io,
+           "d2h_bytes_per_step": bytes_io}
+    ctx32.close()
+    del ctx32
+
+    fp64 = None
+    if not args.no_fp64 and w["precision"] != kf.KF_FP64:
+        ctx64, ms64, _, _, _, d64, phi64 = timed_arm(kf.KF_FP64)
+        ctx64.close()
+        err = float(np.abs(phi32 - phi64).max() / np.abs(phi64).max())
+        fp64 = {"value": ws * args.steps / (ms64 / 1000.0), "ms_per_step": ms64 / args.steps,
+                "phi_rel_err_fp32_vs_fp64": max_over_ranks(err),
+                "charge_fp32": d32.charge, "charge_fp64": d64.charge,
+                "kinetic_fp32": d32.kinetic, "kinetic_fp64": d64.kinetic}
+
+    if rank != 0:
+        if ws > 1:
+            torch.distributed.destroy_process_group()
+        return 0
+
+    # roofline of the dominant kernel (largest share of profiled GPU time)
+    peak, peak_kind = measured_peaks()
+    total_ms = sum(v[0] for v in prof.values())
+    dom, (dms, dn, dbytes) = max(prof.items(), key=lambda kv: kv[1][0])
+    avg_ms = dms / dn
+    achieved = (dbytes / dn) / (avg_ms / 1000.0) / 1e9
+    traffic = ncu_traffic(dom, args.workload)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                "traffic": traffic, "alg_bytes_per_launch": dbytes / dn, "avg_launch_ms": avg_ms,
+                "share_of_gpu_time": dms / total_ms,
+                "kernels": {k: {"ms": v[0], "launches": v[1], "GB/s": (v[2] / v[0] / 1e6 if v[0] else 0.0),
+                                "share": v[0] / total_ms} for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}}
+
+    cpu = None
+    if not args.no_cpu and ws == 1:
+        times, err = cpu_reference_rhs_seconds(3, 0, budget_s=40.0)
+        cpu = cpu_baseline_entry(times) if times else {"unavailable": err}
+
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32 bulk + fp64 Poisson"
+        if w["precision"] == kf.KF_FP32_BULK else "f64",
+        "data": "synthetic (seeded noise, Gaussian dust; seed = rank)",
+        "config": {"workload": f"{args.workload}: {w['n']}^3 box 2*pi*4, M {w['M']}, nu {w['tau']}, "
+                               f"Q {w['Q']}, sigma {w['sigma']}, FAS 4 levels 2+2 to 1e-10, penalization, "
+                               f"diffusion 1e-3, SV > 0.6 k_max",
+                   "n": w["n"], "dt": dt, "l2": "inputs larger than L2 (state + work buffers > 2 GB)",
+                   "parallelism": f"replicas x{ws}"},
+        "gpu_launches": launches,
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "clocks": clk,
+        "poisson": {"solves": d32.solves, "v_cycles": d32.total_iterations,
+                    "last_residual": d32.last_residual, "not_converged": d32.not_converged},
+        "fp64": fp64,
+    }
+    print(json.dumps(out))
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_kf(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -138,6 +138,14 @@ int kf_state_device_ptrs(kf_ctx *ctx, void **FUx, void **FUy, void **FUz, void *
 /* Kernel launches issued by this context since creation (measurement aid). */
 long long kf_launch_count(const kf_ctx *ctx);
 
+/* Kernel profile: when enabled, every launch is bracketed by CUDA events on the
+ * context's stream and its algorithmic bytes (distinct inputs + outputs) are
+ * recorded per kernel class; enabling or disabling resets the totals.
+ * Classes 0..15; kf_profile_class_name gives the kernel name of each. */
+int kf_profile_enable(kf_ctx *ctx, int on);
+int kf_profile_read(kf_ctx *ctx, int cls, double *ms, long long *launches, double *bytes);
+const char *kf_profile_class_name(int cls);
+
 #ifdef __cplusplus
 }
 #endif

@@ -75,7 +75,9 @@ EXPORTS = [
     "kf_ctx_create", "kf_ctx_destroy", "kf_last_error", "kf_set_stream", "kf_synchronize", "kf_set_state",
     "kf_get_state", "kf_set_sources", "kf_set_phi", "kf_get_phi", "kf_rhs_eval", "kf_rk4_steps",
     "kf_poisson_solve", "kf_diag", "kf_fft_r2c", "kf_fft_c2r", "kf_state_device_ptrs", "kf_launch_count",
+    "kf_profile_enable", "kf_profile_read", "kf_profile_class_name",
 ]
+KCLASSES = 16
 
 _lib = None
 
@@ -111,6 +113,10 @@ def load_library():
                                        ctypes.POINTER(vp)]
     L.kf_launch_count.argtypes = [vp]
     L.kf_launch_count.restype = ctypes.c_longlong
+    L.kf_profile_enable.argtypes = [vp, ctypes.c_int]
+    L.kf_profile_read.argtypes = [vp, ctypes.c_int, _D, ctypes.POINTER(ctypes.c_longlong), _D]
+    L.kf_profile_class_name.argtypes = [ctypes.c_int]
+    L.kf_profile_class_name.restype = ctypes.c_char_p
     _lib = L
     return L
 
@@ -228,3 +234,16 @@ class Context:
 
     def launch_count(self) -> int:
         return int(self.L.kf_launch_count(self.h))
+
+    def profile(self, on: bool):
+        self._check(self.L.kf_profile_enable(self.h, 1 if on else 0))
+
+    def profile_read(self):
+        """{kernel class name: (ms, launches, algorithmic bytes)} since profile(True)."""
+        out = {}
+        for k in range(KCLASSES):
+            ms, n, b = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_double()
+            self._check(self.L.kf_profile_read(self.h, k, ctypes.byref(ms), ctypes.byref(n), ctypes.byref(b)))
+            if n.value:
+                out[self.L.kf_profile_class_name(k).decode()] = (ms.value, n.value, b.value)
+        return out

@@ -82,6 +82,15 @@ struct kf_ctx {
     double norm_max = 0., norm_sum = 0., norm_max_old = -1., norm_sum_old = -1.;
     double sup = 0., inf = 0., omega = 1.;
     kf_diag_out diag{};
+    // kernel profiling (CUDA events around each launch, when enabled)
+    bool prof = false;
+    struct ProfRec { int cls; cudaEvent_t a, b; double bytes; };
+    std::vector<ProfRec> recs;
+    std::vector<cudaEvent_t> evfree;
+    double prof_ms[16] = {}, prof_bytes[16] = {};
+    long long prof_n[16] = {};
+    std::vector<AxisJob> hj;
+    std::vector<ZJob> hz;
     // per-(precision, n) entry points
     void (*rhs_fn)(kf_ctx *) = nullptr;
     void (*r2c_fn)(kf_ctx *) = nullptr;
@@ -100,6 +109,64 @@ template <typename P> P *dalloc(kf_ctx *c, size_t bytes) {
 
 inline int nblk(long work, int bs) { return (int)((work + bs - 1) / bs); }
 
+// Kernel classes for the profile (kf_profile_read); names in kf_profile_class_name.
+enum KCls { KC_AXIS_INV, KC_AXIS_FWD, KC_Z_C2R, KC_Z_R2C, KC_XASM, KC_PROD, KC_LIN, KC_RHO, KC_RK,
+            KC_JACOBI, KC_RBGS, KC_RESID, KC_TRANSFER, KC_COARSE, KC_REDUCE, KC_MISC, KC_N };
+const char *const kKClsName[KC_N] = {"k_axis_pass(inverse)", "k_axis_pass(forward)", "k_z_c2r", "k_z_r2c",
+                                     "k_xfwd_assemble", "k_products", "k_lin", "k_rho", "k_rk", "k_jacobi",
+                                     "k_rbgs", "k_residual", "k_restrict/k_fas_rhs/k_prolong/k_inject",
+                                     "k_coarse_solve", "k_reduce_final", "conversion/diagnostics"};
+
+void prof_flush(kf_ctx *c) {
+    if (c->recs.empty()) return;
+    CK(cudaStreamSynchronize(c->st));
+    for (auto &r : c->recs) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, r.a, r.b));
+        c->prof_ms[r.cls] += ms;
+        c->prof_n[r.cls] += 1;
+        c->prof_bytes[r.cls] += r.bytes;
+        c->evfree.push_back(r.a);
+        c->evfree.push_back(r.b);
+    }
+    c->recs.clear();
+}
+
+cudaEvent_t prof_event(kf_ctx *c) {
+    if (c->evfree.empty()) {
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e));
+        return e;
+    }
+    cudaEvent_t e = c->evfree.back();
+    c->evfree.pop_back();
+    return e;
+}
+
+// One kernel launch: counts it and, when profiling, brackets it with events
+// on the context's stream and records its algorithmic bytes.
+struct Launch {
+    kf_ctx *c;
+    int cls;
+    double bytes;
+    cudaEvent_t a = nullptr;
+    Launch(kf_ctx *c_, int cls_, double bytes_) : c(c_), cls(cls_), bytes(bytes_) {
+        c->launches++;
+        if (c->prof) {
+            if (c->recs.size() > 16384) prof_flush(c);
+            a = prof_event(c);
+            CK(cudaEventRecord(a, c->st));
+        }
+    }
+    ~Launch() noexcept(false) {
+        if (c->prof) {
+            cudaEvent_t b = prof_event(c);
+            CK(cudaEventRecord(b, c->st));
+            c->recs.push_back(kf_ctx::ProfRec{cls, a, b, bytes});
+        }
+    }
+};
+
 // ------------------------------------------------------------------ host tables
 double k_val_at(int i, int n, double L) {  // axis_EqSt.cpp:57-61
     double pi = acos(-1.);
@@ -109,8 +176,10 @@ double val_at(int i, int n, double L) { return -0.5 * L + i * (L / n); }  // axi
 
 // ------------------------------------------------------------------ Poisson driver
 void reduce_read(kf_ctx *c, int nb) {
-    k_reduce_final<RBS><<<1, RBS, 0, c->st>>>(c->partial, nb, c->red);
-    c->launches++;
+    {
+        Launch L_(c, KC_REDUCE, 0.);
+        k_reduce_final<RBS><<<1, RBS, 0, c->st>>>(c->partial, nb, c->red);
+    }
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(c->h_red, c->red, sizeof(double) * KF_RED, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
@@ -124,8 +193,10 @@ int red_blocks(long N) {
 double max_residual(kf_ctx *c, const LevelBuf &L, const double *phi, const double *rho, double *r = nullptr) {
     const long N = (long)L.n * L.n * L.n;
     const int nb = red_blocks(N);
-    k_residual<RBS><<<nb, RBS, 0, c->st>>>(phi, rho, L.lev(), r, c->partial);
-    c->launches++;
+    {
+        Launch L_(c, KC_RESID, 16. * N + (r ? 8. * N : 0.));
+        k_residual<RBS><<<nb, RBS, 0, c->st>>>(phi, rho, L.lev(), r, c->partial);
+    }
     reduce_read(c, nb);
     return c->h_red[4];
 }
@@ -148,8 +219,10 @@ int jacobi_solve(kf_ctx *c, const LevelBuf &L, double *phi, double *tmp, const d
         iteration++;
         c->norm_sum_old = c->norm_sum;
         c->norm_max_old = c->norm_max;
-        k_jacobi<RBS><<<nb, RBS, 0, c->st>>>(cur, oth, rho, L.lev(), c->omega, c->partial);
-        c->launches++;
+        {
+            Launch L_(c, KC_JACOBI, 24. * N);
+            k_jacobi<RBS><<<nb, RBS, 0, c->st>>>(cur, oth, rho, L.lev(), c->omega, c->partial);
+        }
         reduce_read(c, nb);
         std::swap(cur, oth);
         c->norm_max = c->h_red[0];
@@ -184,29 +257,39 @@ void vcycle(kf_ctx *c, int l) {
     const int n = L.n;
     const long N = (long)n * n * n;
     if (l == (int)c->lv.size() - 1) {
+        Launch L_(c, KC_COARSE, 0.);
         k_coarse_solve<<<1, 1024, 0, c->st>>>(L.phi, L.rho, L.lev(), cf.coarse_tol, 1000, c->d_sweeps);
-        c->launches++;
         return;
     }
     const long Mh = N / 2;
     for (int s = 0; s < cf.mg_pre; ++s)
         for (int color = 0; color < 2; ++color) {
+            Launch L_(c, KC_RBGS, 16. * N);
             k_rbgs<<<nblk(Mh, 256), 256, 0, c->st>>>(L.phi, L.rho, L.lev(), color);
-            c->launches++;
         }
-    k_residual<RBS><<<red_blocks(N), RBS, 0, c->st>>>(L.phi, L.rho, L.lev(), L.r, c->partial);
+    {
+        Launch L_(c, KC_RESID, 24. * N);
+        k_residual<RBS><<<red_blocks(N), RBS, 0, c->st>>>(L.phi, L.rho, L.lev(), L.r, c->partial);
+    }
     LevelBuf &Lc = c->lv[l + 1];
     const long Nc3 = (long)Lc.n * Lc.n * Lc.n;
-    k_restrict<<<nblk(Nc3, 256), 256, 0, c->st>>>(L.r, L.phi, n, Lc.r, Lc.phi, Lc.phi0);
-    k_fas_rhs<<<nblk(Nc3, 256), 256, 0, c->st>>>(Lc.phi, Lc.r, Lc.lev(), Lc.rho);
-    c->launches += 3;
+    {
+        Launch L_(c, KC_TRANSFER, 8. * N + 32. * Nc3);
+        k_restrict<<<nblk(Nc3, 256), 256, 0, c->st>>>(L.r, L.phi, n, Lc.r, Lc.phi, Lc.phi0);
+    }
+    {
+        Launch L_(c, KC_TRANSFER, 24. * Nc3);
+        k_fas_rhs<<<nblk(Nc3, 256), 256, 0, c->st>>>(Lc.phi, Lc.r, Lc.lev(), Lc.rho);
+    }
     vcycle(c, l + 1);
-    k_prolong_add<<<nblk(N, 256), 256, 0, c->st>>>(L.phi, Lc.phi, Lc.phi0, L.gam, n);
-    c->launches++;
+    {
+        Launch L_(c, KC_TRANSFER, 16. * N + 16. * Nc3);
+        k_prolong_add<<<nblk(N, 256), 256, 0, c->st>>>(L.phi, Lc.phi, Lc.phi0, L.gam, n);
+    }
     for (int s = 0; s < cf.mg_post; ++s)
         for (int color = 0; color < 2; ++color) {
+            Launch L_(c, KC_RBGS, 16. * N);
             k_rbgs<<<nblk(Mh, 256), 256, 0, c->st>>>(L.phi, L.rho, L.lev(), color);
-            c->launches++;
         }
     CK(cudaGetLastError());
 }
@@ -230,21 +313,25 @@ int poisson(kf_ctx *c) {
         const double tol[4] = {0.01, 0.0005, 0.0001, 0.0001};
         const int n = c->n;
         LevelBuf &L3 = c->lv[3];
-        k_inject<<<nblk((long)L3.n * L3.n * L3.n, 256), 256, 0, c->st>>>(c->phi, n, 8, L3.phi);
-        c->launches++;
+        {
+            Launch L_(c, KC_TRANSFER, 16. * L3.n * L3.n * L3.n);
+            k_inject<<<nblk((long)L3.n * L3.n * L3.n, 256), 256, 0, c->st>>>(c->phi, n, 8, L3.phi);
+        }
         for (int cas = 0; cas < 4; ++cas) {
             const int l = 3 - cas;
             LevelBuf &L = c->lv[l];
             const long Nl = (long)L.n * L.n * L.n;
             if (cas > 0) {
                 double *dst = l == 0 ? c->phi : L.phi;
+                Launch L_(c, KC_TRANSFER, 9. * Nl);
                 k_prolong_set<<<nblk(Nl, 256), 256, 0, c->st>>>(dst, c->lv[l + 1].phi, L.gam, L.n);
-                c->launches++;
             }
             const double *rho_l = c->rho;
             if (l > 0) {
-                k_inject<<<nblk(Nl, 256), 256, 0, c->st>>>(c->rho, n, n / L.n, L.rho);
-                c->launches++;
+                {
+                    Launch L_(c, KC_TRANSFER, 16. * Nl);
+                    k_inject<<<nblk(Nl, 256), 256, 0, c->st>>>(c->rho, n, n / L.n, L.rho);
+                }
                 rho_l = L.rho;
             }
             double *phi_l = l == 0 ? c->phi : L.phi;
@@ -292,29 +379,55 @@ template <typename T, int N> struct Impl {
         done = true;
     }
 
+    static double job_bytes(kf_ctx *c, int off, int njobs) {
+        std::vector<const void *> u;
+        for (int j = 0; j < njobs; ++j) {
+            const void *p = c->hj[off + j].in;
+            bool seen = false;
+            for (auto q : u) seen |= q == p;
+            if (!seen) u.push_back(p);
+        }
+        return (double)(u.size() + njobs) * c->Nc * sizeof(T2);
+    }
     static void axis(kf_ctx *c, int off, int njobs, int ax, int sign) {
         const int ntiles = ax == 0 ? (N * NZC + TC - 1) / TC : N * ((NZC + TC - 1) / TC);
         const size_t smem = (size_t)N * TC * sizeof(T2);
+        Launch L_(c, sign > 0 ? KC_AXIS_INV : KC_AXIS_FWD, job_bytes(c, off, njobs));
         if (sign < 0)
             k_axis_pass<T, N, -1><<<njobs * ntiles, TC * P, smem, c->st>>>(c->dj + off, njobs, ax, geo(c), (const T2 *)c->tw);
         else
             k_axis_pass<T, N, +1><<<njobs * ntiles, TC * P, smem, c->st>>>(c->dj + off, njobs, ax, geo(c), (const T2 *)c->tw);
-        c->launches++;
+    }
+    static double z_bytes(kf_ctx *c, int off, int njobs, bool c2r) {
+        std::vector<const void *> u;
+        int outs = 0;
+        for (int j = 0; j < njobs; ++j) {
+            const ZJob &z = c->hz[off + j];
+            for (const void *p : {z.inA, z.inB}) {
+                if (!p) continue;
+                bool seen = false;
+                for (auto q : u) seen |= q == p;
+                if (!seen) u.push_back(p);
+            }
+            outs += (z.outA ? 1 : 0) + (z.outB ? 1 : 0);
+        }
+        const double cb = (double)c->Nc * sizeof(T2), rb = (double)c->N * sizeof(T);
+        return c2r ? u.size() * cb + outs * rb : u.size() * rb + outs * cb;
     }
     static void zc2r(kf_ctx *c, int off, int njobs) {
         const int nrows = N * N;
         const int ntiles = (nrows + LZ - 1) / LZ;
         const size_t smem = (size_t)(2 * LZ * NZC + LZ * (N + 1)) * sizeof(T2);
+        Launch L_(c, KC_Z_C2R, z_bytes(c, off, njobs, true));
         k_z_c2r<T, N><<<njobs * ntiles, LZ * P, smem, c->st>>>(c->dz + off, njobs, nrows, geo(c), (const T2 *)c->tw,
                                                              (T)(1. / ((double)N * N * N)));
-        c->launches++;
     }
     static void zr2c(kf_ctx *c, int off, int njobs) {
         const int nrows = N * N;
         const int ntiles = (nrows + LZ - 1) / LZ;
         const size_t smem = (size_t)(LZ * (N + 1)) * sizeof(T2);
+        Launch L_(c, KC_Z_R2C, z_bytes(c, off, njobs, false));
         k_z_r2c<T, N><<<njobs * ntiles, LZ * P, smem, c->st>>>(c->dz + off, njobs, nrows, (const T2 *)c->tw);
-        c->launches++;
     }
     static RhsArgs<T> rargs(kf_ctx *c) {
         RhsArgs<T> a;
@@ -340,8 +453,10 @@ template <typename T, int N> struct Impl {
         axis(c, c->jA_y, 3, 1, +1);
         if (pois || pen) zc2r(c, c->zA, 1);
         if (pois) {
-            k_rho<T><<<nblk(c->N, 256), 256, 0, c->st>>>((const T *)c->R[0], c->nd, c->rho, c->N);
-            c->launches++;
+            {
+                Launch L_(c, KC_RHO, (double)c->N * (sizeof(T) + 16));
+                k_rho<T><<<nblk(c->N, 256), 256, 0, c->st>>>((const T *)c->R[0], c->nd, c->rho, c->N);
+            }
             CK(cudaGetLastError());
             int rc = poisson(c);
             if (rc) throw KfError{KF_ERR_NOT_CONVERGED, "Poisson solve did not reach its tolerance"};
@@ -349,8 +464,8 @@ template <typename T, int N> struct Impl {
         // B
         if (Tm & T_E_INT) {
             if (c->fp32) {
+                Launch L_(c, KC_MISC, (double)c->N * (8 + sizeof(T)));
                 k_from_f64<T><<<nblk(c->N, 256), 256, 0, c->st>>>((T *)c->phiT, c->phi, c->N);
-                c->launches++;
             }
             zr2c(c, c->zB, 1);
             axis(c, c->jB_y, 1, 1, -1);
@@ -358,9 +473,9 @@ template <typename T, int N> struct Impl {
         }
         // C
         if (pen) {
+            Launch L_(c, KC_LIN, (double)c->Nc * (9 * sizeof(T2) + 2 * sizeof(T)));
             k_lin<T><<<nblk(c->Nc, 256), 256, 0, c->st>>>(rargs(c), geo(c), (T2 *)c->LIN[0], (T2 *)c->LIN[1],
                                                          (T2 *)c->LIN[2], (T2 *)c->LIN[3]);
-            c->launches++;
         }
         // D
         axis(c, c->jD_x, pen ? 10 : 6, 0, +1);
@@ -383,15 +498,20 @@ template <typename T, int N> struct Impl {
         pa.eta = (T)c->cfg.pen_eta;
         pa.terms = Tm;
         pa.N = c->N;
-        k_products<T><<<nblk(c->N, 256), 256, 0, c->st>>>(pa);
-        c->launches++;
+        {
+            Launch L_(c, KC_PROD, (double)c->N * sizeof(T) * (19 + (pen ? 6 : 0)));
+            k_products<T><<<nblk(c->N, 256), 256, 0, c->st>>>(pa);
+        }
         // F
         zr2c(c, c->zF, 2);
         axis(c, c->jF_y, 4, 1, -1);
         const int ntiles = (N * NZC + TC - 1) / TC;
-        k_xfwd_assemble<T, N><<<ntiles, TC * P, (size_t)N * TC * sizeof(T2), c->st>>>(c->dj + c->jF_x, geo(c), rargs(c),
-                                                                                     (const T2 *)c->tw);
-        c->launches++;
+        {
+            const double cb = (double)c->Nc * sizeof(T2), rb = (double)c->Nc * sizeof(T);
+            Launch L_(c, KC_XASM, pen ? 8 * cb : 8 * cb + 4 * cb + ((Tm & T_E_INT) ? cb : 0.) + 2 * rb);
+            k_xfwd_assemble<T, N><<<ntiles, TC * P, (size_t)N * TC * sizeof(T2), c->st>>>(c->dj + c->jF_x, geo(c),
+                                                                                         rargs(c), (const T2 *)c->tw);
+        }
         CK(cudaGetLastError());
     }
 
@@ -670,6 +790,8 @@ void build_jobs(kf_ctx *c) {
     c->zG = (int)Z.size();
     zj(CY[0], MUL_NONE, CY[1], MUL_NONE, R[20], R[21]);
     zj(CY[2], MUL_NONE, CY[3], MUL_NONE, R[22], R[23]);
+    c->hj = J;
+    c->hz = Z;
     c->dj = dalloc<AxisJob>(c, sizeof(AxisJob) * J.size());
     c->dz = dalloc<ZJob>(c, sizeof(ZJob) * Z.size());
     CK(cudaMemcpy(c->dj, J.data(), sizeof(AxisJob) * J.size(), cudaMemcpyHostToDevice));
@@ -741,8 +863,8 @@ void put_bulk(kf_ctx *c, void *dst, const double *src, long count) {
         CK(cudaMemcpyAsync(dst, src, 8 * count, cudaMemcpyHostToDevice, c->st));
     } else {
         CK(cudaMemcpyAsync(c->stage64, src, 8 * count, cudaMemcpyHostToDevice, c->st));
+        Launch L_(c, KC_MISC, 12. * count);
         k_from_f64<float><<<nblk(count, 256), 256, 0, c->st>>>((float *)dst, c->stage64, count);
-        c->launches++;
     }
 }
 
@@ -750,8 +872,10 @@ void get_bulk(kf_ctx *c, double *dst, const void *src, long count) {
     if (!c->fp32) {
         CK(cudaMemcpyAsync(dst, src, 8 * count, cudaMemcpyDeviceToHost, c->st));
     } else {
-        k_to_f64<float><<<nblk(count, 256), 256, 0, c->st>>>(c->stage64, (const float *)src, count);
-        c->launches++;
+        {
+            Launch L_(c, KC_MISC, 12. * count);
+            k_to_f64<float><<<nblk(count, 256), 256, 0, c->st>>>(c->stage64, (const float *)src, count);
+        }
         CK(cudaMemcpyAsync(dst, c->stage64, 8 * count, cudaMemcpyDeviceToHost, c->st));
     }
 }
@@ -764,13 +888,13 @@ void copy_state(kf_ctx *c, void *const *dst, void *const *src) {
 void rk_launch(kf_ctx *c, double cdt, int mode) {
     const long M = c->Nc;
     for (int q = 0; q < 4; ++q) {
+        Launch L_(c, KC_RK, (double)M * c->cs * (mode == 1 ? 5 : 4));
         if (c->fp32)
             k_rk<float><<<nblk(M, 256), 256, 0, c->st>>>((float2 *)c->Y[q], (float2 *)c->ACC[q], (float2 *)c->Ys[q],
                                                         (const float2 *)c->K[q], (float)cdt, mode, M);
         else
             k_rk<double><<<nblk(M, 256), 256, 0, c->st>>>((double2 *)c->Y[q], (double2 *)c->ACC[q], (double2 *)c->Ys[q],
                                                          (const double2 *)c->K[q], cdt, mode, M);
-        c->launches++;
     }
     CK(cudaGetLastError());
 }
@@ -814,6 +938,11 @@ int kf_ctx_create(const kf_config *cfg, kf_ctx **out) {
 int kf_ctx_destroy(kf_ctx *c) {
     if (!c) return KF_ERR_ARG;
     if (c->st) cudaStreamSynchronize(c->st);
+    for (auto &r : c->recs) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    for (auto e : c->evfree) cudaEventDestroy(e);
     for (void *p : c->allocs) cudaFree(p);
     if (c->h_red) cudaFreeHost(c->h_red);
     if (c->st && c->own_stream) cudaStreamDestroy(c->st);
@@ -930,6 +1059,7 @@ int kf_diag(kf_ctx *c, kf_diag_out *out) {
         if (!out) throw KfError{KF_ERR_ARG, "null output"};
         c->inv_state_fn(c);
         const int nb = red_blocks(c->N);
+        Launch L_(c, KC_MISC, (double)c->N * (4 * c->es + 16));
         if (c->fp32)
             k_diag_sums<float><<<nb, RBS, 0, c->st>>>((const float *)c->R[23], (const float *)c->R[20],
                                                      (const float *)c->R[21], (const float *)c->R[22], c->phi, c->nd,
@@ -939,7 +1069,7 @@ int kf_diag(kf_ctx *c, kf_diag_out *out) {
                                                       (const double *)c->R[21], (const double *)c->R[22], c->phi,
                                                       c->nd, c->cfg.M, c->N, c->partial);
         k_diag_final<<<1, 32, 0, c->st>>>(c->partial, nb, c->red);
-        c->launches += 2;
+        c->launches++;
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(c->h_red, c->red, sizeof(double) * 2, cudaMemcpyDeviceToHost, c->st));
         CK(cudaStreamSynchronize(c->st));
@@ -977,5 +1107,29 @@ int kf_state_device_ptrs(kf_ctx *c, void **ux, void **uy, void **uz, void **s) {
 }
 
 long long kf_launch_count(const kf_ctx *c) { return c ? c->launches : -1; }
+
+int kf_profile_enable(kf_ctx *c, int on) {
+    return guarded(c, [&] {
+        prof_flush(c);
+        for (int k = 0; k < KC_N; ++k) {
+            c->prof_ms[k] = 0.;
+            c->prof_bytes[k] = 0.;
+            c->prof_n[k] = 0;
+        }
+        c->prof = on != 0;
+    });
+}
+
+int kf_profile_read(kf_ctx *c, int cls, double *ms, long long *launches, double *bytes) {
+    return guarded(c, [&] {
+        if (cls < 0 || cls >= KC_N) throw KfError{KF_ERR_ARG, "kernel class out of range"};
+        prof_flush(c);
+        if (ms) *ms = c->prof_ms[cls];
+        if (launches) *launches = c->prof_n[cls];
+        if (bytes) *bytes = c->prof_bytes[cls];
+    });
+}
+
+const char *kf_profile_class_name(int cls) { return (cls >= 0 && cls < KC_N) ? kKClsName[cls] : ""; }
 
 }  // extern "C"

@@ -18,8 +18,16 @@ TOL64 = 1e-12
 TOL32 = 1e-5
 
 
-def rel(a, b):
-    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+def rel(a, b, scale=0.0):
+    """max|a-b| / max(max|b|, scale).  `scale` is the largest field of the same
+    output: the z transforms pack two real fields into one complex line, so a
+    field that is exactly zero picks up rounding noise of its partner's size."""
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), scale, 1e-300))
+
+
+def state_rel(g, r):
+    scale = max(np.abs(x).max() for x in r)
+    return [rel(a, b, scale) for a, b in zip(g, r)]
 
 
 def oracle_for(cfg):
@@ -68,8 +76,8 @@ def test_rhs_vs_oracle(case, n):
     o.set_sources(nd, mask)
     o.rhs()
     r = o.get_state()
-    for q in range(4):
-        assert rel(g[q], r[q]) < TOL64, (case, q, rel(g[q], r[q]))
+    errs = state_rel(g, r)
+    assert max(errs) < TOL64, (case, errs)
     if RHS_CASES[case] & kf.KF_T_POISSON:
         assert rel(gphi, o.get_phi()) < TOL64
 
@@ -110,8 +118,8 @@ def test_rk4_jacobi32_20_steps():
     o.set_sources(nd, mask)
     o.rk4(dt, 20)
     r = o.get_state()
-    for q in range(4):
-        assert rel(g[q], r[q]) < TOL64, (q, rel(g[q], r[q]))
+    errs = state_rel(g, r)
+    assert max(errs) < TOL64, errs
     assert rel(gphi, o.get_phi()) < TOL64
 
 
@@ -132,8 +140,8 @@ def test_rk4_fas_vs_oracle(n, steps):
     o.set_sources(nd, mask)
     o.rk4(dt, steps)
     r = o.get_state()
-    for q in range(4):
-        assert rel(g[q], r[q]) < TOL64, (q, rel(g[q], r[q]))
+    errs = state_rel(g, r)
+    assert max(errs) < TOL64, errs
     assert rel(gphi, o.get_phi()) < TOL64
 
 
