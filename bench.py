@@ -119,7 +119,29 @@ def ncu_traffic(kernel: str, workload: str):
 
 
 # --------------------------------------------------------------------- CPU leg
+class _QuietStdout:
+    """Silence C-level stdout (the reference prints progress from its
+    constructors, e.g. rhs_standard.cpp:32) so rank 0 prints one JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+        return self
+
+    def __exit__(self, *a):
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+
+
 def cpu_reference_rhs_seconds(nsamples: int, warmup: int, budget_s: float):
+    with _QuietStdout():
+        return _cpu_reference_rhs_seconds(nsamples, warmup, budget_s)
+
+
+def _cpu_reference_rhs_seconds(nsamples: int, warmup: int, budget_s: float):
     """The reference's own rhs_standard::solve (its sources compiled here,
     shipped term set, cascadic multigrid plan of kielflow.cpp:207-217) at 128^3
     with the workload's M, tau, dust; returns per-sample seconds."""

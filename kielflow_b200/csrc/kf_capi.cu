@@ -38,9 +38,9 @@ struct KfError {
 
 struct LevelBuf {
     int n = 0;
-    double *dd = nullptr, *dp = nullptr, *dm = nullptr, *gam = nullptr;
+    double *dd = nullptr, *dp = nullptr, *dm = nullptr, *ip = nullptr, *im = nullptr, *gam = nullptr;
     double *phi = nullptr, *rho = nullptr, *r = nullptr, *phi0 = nullptr;
-    Lev lev() const { return Lev{n, dd, dp, dm}; }
+    Lev lev() const { return Lev{n, dd, dp, dm, ip, im}; }
 };
 
 constexpr int RBS = 256;  // reduction block size
@@ -190,12 +190,15 @@ int red_blocks(long N) {
     return (int)(nb < 1184 ? nb : 1184);
 }
 
-double max_residual(kf_ctx *c, const LevelBuf &L, const double *phi, const double *rho, double *r = nullptr) {
+double max_residual(kf_ctx *c, const LevelBuf &L, const double *phi, const double *rho, bool fast) {
     const long N = (long)L.n * L.n * L.n;
     const int nb = red_blocks(N);
     {
-        Launch L_(c, KC_RESID, 16. * N + (r ? 8. * N : 0.));
-        k_residual<RBS><<<nb, RBS, 0, c->st>>>(phi, rho, L.lev(), r, c->partial);
+        Launch L_(c, KC_RESID, 16. * N);
+        if (fast)
+            k_residual<RBS, true><<<nb, RBS, 0, c->st>>>(phi, rho, L.lev(), nullptr, c->partial);
+        else
+            k_residual<RBS, false><<<nb, RBS, 0, c->st>>>(phi, rho, L.lev(), nullptr, c->partial);
     }
     reduce_read(c, nb);
     return c->h_red[4];
@@ -269,7 +272,7 @@ void vcycle(kf_ctx *c, int l) {
         }
     {
         Launch L_(c, KC_RESID, 24. * N);
-        k_residual<RBS><<<red_blocks(N), RBS, 0, c->st>>>(L.phi, L.rho, L.lev(), L.r, c->partial);
+        k_residual<RBS, true><<<red_blocks(N), RBS, 0, c->st>>>(L.phi, L.rho, L.lev(), L.r, c->partial);
     }
     LevelBuf &Lc = c->lv[l + 1];
     const long Nc3 = (long)Lc.n * Lc.n * Lc.n;
@@ -304,7 +307,7 @@ int poisson(kf_ctx *c) {
         rc = jacobi_solve(c, L0, c->phi, L0.r, c->rho, cf.nlj_max_it, cf.nlj_limit,
                           cf.poisson_mode == KF_PS_JACOBI_RES, cf.res_tol);
         if (cf.poisson_mode == KF_PS_JACOBI_REF) {
-            c->diag.last_residual = max_residual(c, L0, c->phi, c->rho);
+            c->diag.last_residual = max_residual(c, L0, c->phi, c->rho, false);
             rc = 0;  // the reference's plan has no failure on a sweep cap
         }
     } else if (cf.poisson_mode == KF_PS_CASCADIC) {
@@ -337,15 +340,15 @@ int poisson(kf_ctx *c) {
             double *phi_l = l == 0 ? c->phi : L.phi;
             jacobi_solve(c, L, phi_l, L.r, rho_l, steps[cas], tol[cas], false, 0.);
         }
-        c->diag.last_residual = max_residual(c, L0, c->phi, c->rho);
+        c->diag.last_residual = max_residual(c, L0, c->phi, c->rho, false);
         rc = 0;
     } else {
-        double r = max_residual(c, L0, c->phi, c->rho);
+        double r = max_residual(c, L0, c->phi, c->rho, true);
         int cyc = 0;
         while (r > cf.res_tol && cyc < cf.max_cycles) {
             vcycle(c, 0);
             ++cyc;
-            r = max_residual(c, L0, c->phi, c->rho);
+            r = max_residual(c, L0, c->phi, c->rho, true);
         }
         c->diag.last_iterations = cyc;
         c->diag.total_iterations += cyc;
@@ -682,12 +685,14 @@ void build_levels(kf_ctx *c) {
         const int n = c->n >> l;
         L.n = n;
         const double Lb = cf.L;
-        std::vector<double> H(n + 1), dd(n), dp(n), dm(n), gam(n, 0.);
+        std::vector<double> H(n + 1), dd(n), dp(n), dm(n), ip(n), im(n), gam(n, 0.);
         for (int i = 0; i < n + 1; ++i) H[i] = val_at(i, n, Lb) - val_at(i - 1, n, Lb);  // H_create (:112-126)
         for (int i = 0; i < n; ++i) {
             dd[i] = 2. / (H[i + 1] * H[i]);
             dp[i] = H[i + 1] * (H[i + 1] + H[i]);
             dm[i] = H[i] * (H[i + 1] + H[i]);
+            ip[i] = 2. / dp[i];
+            im[i] = 2. / dm[i];
         }
         for (int m = 1; m < n; m += 2) {  // OP_hto2h gamma on this (fine) axis
             const double x1 = val_at(m - 1, n, Lb), x2 = val_at(m + 1, n, Lb), x = val_at(m, n, Lb);
@@ -697,6 +702,10 @@ void build_levels(kf_ctx *c) {
         L.dp = dalloc<double>(c, 8 * n);
         L.dm = dalloc<double>(c, 8 * n);
         L.gam = dalloc<double>(c, 8 * n);
+        L.ip = dalloc<double>(c, 8 * n);
+        L.im = dalloc<double>(c, 8 * n);
+        CK(cudaMemcpy(L.ip, ip.data(), 8 * n, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(L.im, im.data(), 8 * n, cudaMemcpyHostToDevice));
         CK(cudaMemcpy(L.dd, dd.data(), 8 * n, cudaMemcpyHostToDevice));
         CK(cudaMemcpy(L.dp, dp.data(), 8 * n, cudaMemcpyHostToDevice));
         CK(cudaMemcpy(L.dm, dm.data(), 8 * n, cudaMemcpyHostToDevice));

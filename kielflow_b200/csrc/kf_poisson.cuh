@@ -20,6 +20,8 @@ struct Lev {
     const double *dd;  // 2/(H[i+1] H[i])
     const double *dp;  // H[i+1] (H[i+1] + H[i])
     const double *dm;  // H[i]   (H[i+1] + H[i])
+    const double *ip;  // 2/dp  (FAS cycle weights)
+    const double *im;  // 2/dm
 };
 
 __device__ __forceinline__ int wrapi(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
@@ -37,6 +39,34 @@ __device__ __forceinline__ void point_coeffs(const double *__restrict__ p, const
     A = __dadd_rn(A, p[lidx(i, j, wrapi(k - 1, n), n)] / L.dm[k]);
     A = __dmul_rn(2., A);
     if (rho) A = __dadd_rn(A, rho[lidx(i, j, k, n)]);
+}
+
+// The FAS cycle's stencil: the same operator with the weights 2/den
+// precomputed, products instead of divisions.
+__device__ __forceinline__ void point_coeffs_fast(const double *__restrict__ p, const double *__restrict__ rho,
+                                                  const Lev &L, int i, int j, int k, double &A, double &D) {
+    const int n = L.n;
+    D = __dadd_rn(__dadd_rn(L.dd[i], L.dd[j]), L.dd[k]);
+    A = __dmul_rn(p[lidx(wrapi(i + 1, n), j, k, n)], L.ip[i]);
+    A = __dadd_rn(A, __dmul_rn(p[lidx(wrapi(i - 1, n), j, k, n)], L.im[i]));
+    A = __dadd_rn(A, __dmul_rn(p[lidx(i, wrapi(j + 1, n), k, n)], L.ip[j]));
+    A = __dadd_rn(A, __dmul_rn(p[lidx(i, wrapi(j - 1, n), k, n)], L.im[j]));
+    A = __dadd_rn(A, __dmul_rn(p[lidx(i, j, wrapi(k + 1, n), n)], L.ip[k]));
+    A = __dadd_rn(A, __dmul_rn(p[lidx(i, j, wrapi(k - 1, n), n)], L.im[k]));
+    if (rho) A = __dadd_rn(A, rho[lidx(i, j, k, n)]);
+}
+
+template <bool FAST>
+__device__ __forceinline__ void coeffs_t(const double *__restrict__ p, const double *__restrict__ rho,
+                                         const Lev &L, int i, int j, int k, double &A, double &D) {
+    if (FAST) point_coeffs_fast(p, rho, L, i, j, k, A, D);
+    else point_coeffs(p, rho, L, i, j, k, A, D);
+}
+
+// one Newton step on A - D x - e^x = 0 (the FAS smoother's point update)
+__device__ __forceinline__ double newton_step(double x, double A, double D) {
+    const double ex = exp(x);
+    return __dsub_rn(x, __dsub_rn(__dsub_rn(A, __dmul_rn(D, x)), ex) / __dsub_rn(-D, ex));
 }
 
 __device__ __forceinline__ double f_point(double A, double D, double x) {
@@ -139,7 +169,7 @@ __global__ void __launch_bounds__(BS) k_reduce_final(const double *__restrict__ 
 }
 
 // Pointwise residual r = f(phi) = lap_h phi + rho - e^phi (+ block max |r|, NaN-propagating)
-template <int BS>
+template <int BS, bool FAST>
 __global__ void __launch_bounds__(BS) k_residual(const double *__restrict__ phi, const double *__restrict__ rho,
                                                  Lev L, double *__restrict__ r, double *__restrict__ partial) {
     __shared__ double sh[KF_RED * BS];
@@ -151,7 +181,7 @@ __global__ void __launch_bounds__(BS) k_residual(const double *__restrict__ phi,
         const long rr = id / n;
         const int j = (int)(rr % n), i = (int)(rr / n);
         double A, D;
-        point_coeffs(phi, rho, L, i, j, k, A, D);
+        coeffs_t<FAST>(phi, rho, L, i, j, k, A, D);
         const double f = f_point(A, D, phi[id]);
         if (r) r[id] = f;
         const double af = fabs(f);
@@ -161,7 +191,7 @@ __global__ void __launch_bounds__(BS) k_residual(const double *__restrict__ phi,
     block_reduce5<BS>(v, sh, partial + (long)blockIdx.x * KF_RED);
 }
 
-// Red-black point-Newton Gauss-Seidel half sweep (colour (i+j+k)%2), omega = 1.
+// Red-black Gauss-Seidel-Newton half sweep (colour (i+j+k)%2): one Newton step per point.
 __global__ void k_rbgs(double *__restrict__ phi, const double *__restrict__ rho, Lev L, int color) {
     const int n = L.n, nh = n / 2;
     const long M = (long)n * n * nh;
@@ -172,9 +202,9 @@ __global__ void k_rbgs(double *__restrict__ phi, const double *__restrict__ rho,
     const int j = (int)(r % n), i = (int)(r / n);
     const int k = 2 * k2 + ((i + j + color) & 1);
     double A, D;
-    point_coeffs(phi, rho, L, i, j, k, A, D);
+    point_coeffs_fast(phi, rho, L, i, j, k, A, D);
     const long q = lidx(i, j, k, n);
-    phi[q] = newton_point(phi[q], A, D);
+    phi[q] = newton_step(phi[q], A, D);
 }
 
 // Coarsest-level solve in one block: red-black sweeps until max |f| <= tol.
@@ -192,7 +222,7 @@ __global__ void __launch_bounds__(1024) k_coarse_solve(double *__restrict__ phi,
             const long r = id / n;
             const int j = (int)(r % n), i = (int)(r / n);
             double A, D;
-            point_coeffs(phi, rho, L, i, j, k, A, D);
+            point_coeffs_fast(phi, rho, L, i, j, k, A, D);
             const double af = fabs(f_point(A, D, phi[id]));
             m = (af != af) ? af : fmax(m, af);
         }
@@ -223,9 +253,9 @@ __global__ void __launch_bounds__(1024) k_coarse_solve(double *__restrict__ phi,
                 const int j = (int)(r % n), i = (int)(r / n);
                 const int k = 2 * k2 + ((i + j + color) & 1);
                 double A, D;
-                point_coeffs(phi, rho, L, i, j, k, A, D);
+                point_coeffs_fast(phi, rho, L, i, j, k, A, D);
                 const long q = lidx(i, j, k, n);
-                phi[q] = newton_point(phi[q], A, D);
+                phi[q] = newton_step(phi[q], A, D);
             }
             __syncthreads();
         }
@@ -277,7 +307,7 @@ __global__ void k_fas_rhs(const double *__restrict__ phic, const double *__restr
     const long rr = id / n;
     const int j = (int)(rr % n), i = (int)(rr / n);
     double A, D;
-    point_coeffs(phic, nullptr, L, i, j, k, A, D);
+    point_coeffs_fast(phic, nullptr, L, i, j, k, A, D);
     const double Nc = __dsub_rn(0., f_point(A, D, phic[id]));
     rhoc[id] = __dadd_rn(Nc, rc[id]);
 }

@@ -74,6 +74,7 @@ struct level {
     axis_eq ax;
     vec H;                  /* H[i] = val_at(i) - val_at(i-1), i = 0..n */
     vec dd, den_p, den_m;   /* 2/(H[i+1]H[i]), H[i+1](H[i+1]+H[i]), H[i](H[i+1]+H[i]) */
+    vec inv_p, inv_m;       /* 2/den_p, 2/den_m: stencil weights of the FAS cycle      */
     void init(int n_, double L) {
         n = n_;
         ax.l0 = -0.5 * L;
@@ -84,10 +85,14 @@ struct level {
         dd.resize(n);
         den_p.resize(n);
         den_m.resize(n);
+        inv_p.resize(n);
+        inv_m.resize(n);
         for (int i = 0; i < n; ++i) {
             dd[i] = 2. / (H[i + 1] * H[i]);
             den_p[i] = H[i + 1] * (H[i + 1] + H[i]);
             den_m[i] = H[i] * (H[i + 1] + H[i]);
+            inv_p[i] = 2. / den_p[i];
+            inv_m[i] = 2. / den_m[i];
         }
     }
     inline size_t idx(int i, int j, int k) const { return (size_t)k + n * ((size_t)j + (size_t)i * n); }
@@ -111,6 +116,25 @@ struct level {
     inline double resid(const double *p, const double *rho, int i, int j, int k) const {
         double A, D;
         coeffs(p, rho, i, j, k, A, D);
+        double x = p[idx(i, j, k)];
+        return A - D * x - exp(x);
+    }
+    /* the same stencil with the weights 2/den precomputed (FAS cycle): the
+     * factor 2 of :187 is folded into the weights, the divisions become products */
+    inline void coeffs_fast(const double *p, const double *rho, int i, int j, int k, double &A,
+                            double &D) const {
+        D = dd[i] + dd[j] + dd[k];
+        A = p[idx(wrap(i + 1), j, k)] * inv_p[i];
+        A += p[idx(wrap(i - 1), j, k)] * inv_m[i];
+        A += p[idx(i, wrap(j + 1), k)] * inv_p[j];
+        A += p[idx(i, wrap(j - 1), k)] * inv_m[j];
+        A += p[idx(i, j, wrap(k + 1))] * inv_p[k];
+        A += p[idx(i, j, wrap(k - 1))] * inv_m[k];
+        if (rho) A += rho[idx(i, j, k)];
+    }
+    inline double resid_fast(const double *p, const double *rho, int i, int j, int k) const {
+        double A, D;
+        coeffs_fast(p, rho, i, j, k, A, D);
         double x = p[idx(i, j, k)];
         return A - D * x - exp(x);
     }
@@ -339,27 +363,41 @@ double max_resid(const level &L, const vec &phi, const vec &rho) {
     return r;
 }
 
-/* Red-black point-Newton Gauss-Seidel sweep (omega = 1): the point update of
- * iteration_loop (:177-199) applied in place, colour (i+j+k)%2 == 0 first. */
+double max_resid_fast(const level &L, const vec &phi, const vec &rho) {
+    double r = 0.;
+    for (int i = 0; i < L.n; ++i)
+        for (int j = 0; j < L.n; ++j)
+            for (int k = 0; k < L.n; ++k) {
+                double f = fabs(L.resid_fast(phi.data(), rho.data(), i, j, k));
+                if (f > r) r = f;
+            }
+    return r;
+}
+
+/* Red-black Gauss-Seidel-Newton sweep: at each point one Newton step on the
+ * point equation A - D x - e^x = 0 of iteration_loop (:177-199), in place,
+ * colour (i+j+k)%2 == 0 first. */
 void rbgs_sweep(const level &L, vec &phi, const vec &rho) {
     for (int color = 0; color < 2; ++color)
         for (int i = 0; i < L.n; ++i)
             for (int j = 0; j < L.n; ++j)
                 for (int k = (i + j + color) & 1; k < L.n; k += 2) {
                     double A, D;
-                    L.coeffs(phi.data(), rho.data(), i, j, k, A, D);
-                    phi[L.idx(i, j, k)] = newton_point(phi[L.idx(i, j, k)], A, D);
+                    L.coeffs_fast(phi.data(), rho.data(), i, j, k, A, D);
+                    const size_t q = L.idx(i, j, k);
+                    const double x = phi[q], ex = exp(x);
+                    phi[q] = x - (A - D * x - ex) / (-D - ex);
                 }
 }
 
-/* N(phi) = -lap_h phi + e^phi = rho - f(phi) at every point */
-void apply_N(const level &L, const vec &phi, const vec &rho, vec &out) {
+/* N(phi) = -lap_h phi + e^phi = -f(phi; rho = 0) at every point */
+void apply_N(const level &L, const vec &phi, vec &out) {
     out.resize(phi.size());
     for (int i = 0; i < L.n; ++i)
         for (int j = 0; j < L.n; ++j)
             for (int k = 0; k < L.n; ++k) {
                 size_t q = L.idx(i, j, k);
-                out[q] = rho[q] - L.resid(phi.data(), rho.data(), i, j, k);
+                out[q] = 0. - L.resid_fast(phi.data(), nullptr, i, j, k);
             }
 }
 
@@ -368,7 +406,7 @@ void fas_vcycle(kfo_ctx *c, int l, vec &phi, const vec &rho) {
     const kfo_config &cf = c->cfg;
     if (l == (int)c->lv.size() - 1) {
         for (int s = 0; s < 1000; ++s) {
-            if (max_resid(L, phi, rho) <= cf.coarse_tol) break;
+            if (max_resid_fast(L, phi, rho) <= cf.coarse_tol) break;
             rbgs_sweep(L, phi, rho);
         }
         return;
@@ -377,13 +415,12 @@ void fas_vcycle(kfo_ctx *c, int l, vec &phi, const vec &rho) {
     vec r(phi.size());
     for (int i = 0; i < L.n; ++i)
         for (int j = 0; j < L.n; ++j)
-            for (int k = 0; k < L.n; ++k) r[L.idx(i, j, k)] = L.resid(phi.data(), rho.data(), i, j, k);
+            for (int k = 0; k < L.n; ++k) r[L.idx(i, j, k)] = L.resid_fast(phi.data(), rho.data(), i, j, k);
     vec phic, rc, Nc, rhoc;
     inject(L.n, 2, phi, phic);
     restrict_fw(L.n, r, rc);
     const level &Lc = c->lv[l + 1];
-    vec zero(phic.size(), 0.);
-    apply_N(Lc, phic, zero, Nc); /* -lap_c phic + e^phic */
+    apply_N(Lc, phic, Nc); /* -lap_c phic + e^phic */
     rhoc.resize(phic.size());
     for (size_t q = 0; q < phic.size(); ++q) rhoc[q] = Nc[q] + rc[q];
     vec phic0 = phic;
@@ -435,12 +472,12 @@ int poisson(kfo_ctx *c, vec &phi, const vec &rho) {
         cascadic_solve(c, phi, rho);
         c->stats.last_residual = max_resid(c->lv[0], phi, rho);
     } else {
-        double r = max_resid(c->lv[0], phi, rho);
+        double r = max_resid_fast(c->lv[0], phi, rho);
         int cyc = 0;
         while (r > cf.res_tol && cyc < cf.max_cycles) {
             fas_vcycle(c, 0, phi, rho);
             ++cyc;
-            r = max_resid(c->lv[0], phi, rho);
+            r = max_resid_fast(c->lv[0], phi, rho);
         }
         c->stats.last_iterations = cyc;
         c->stats.total_iterations += cyc;
