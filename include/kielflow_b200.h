@@ -76,6 +76,8 @@ typedef struct {
     int mg_post;       /* FAS post-smoothing sweeps                                  */
     double coarse_tol; /* FAS coarsest-level residual target                         */
     int max_cycles;    /* FAS V-cycle cap per solve                                  */
+    int phi_extrap;    /* 1: start each Poisson solve at a new time from the linear  */
+                       /*    extrapolation of the last two solutions in time         */
     int precision;     /* KF_FP64 or KF_FP32_BULK                                    */
 } kf_config;
 

@@ -49,7 +49,7 @@ def config_for(w: dict, n: int | None = None, precision: int | None = None, **ov
     kw = dict(tau=w["tau"], theta=THETA, diff_D=DIFF_D, sv_eps=0.5, sv_cut=0.6 if w["sv"] else 0.0,
               pen_eta=PEN_ETA, terms=terms, poisson_mode=w["poisson_mode"], nlj_max_it=100000,
               nlj_limit=0.5e-5, res_tol=1e-10, mg_levels=levels, mg_pre=2, mg_post=2, coarse_tol=1e-13,
-              max_cycles=100, precision=w["precision"] if precision is None else precision)
+              max_cycles=100, phi_extrap=1, precision=w["precision"] if precision is None else precision)
     kw.update(over)
     return Config.make(n, L_BOX, w["M"], **kw)
 

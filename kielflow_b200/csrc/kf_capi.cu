@@ -72,6 +72,12 @@ struct kf_ctx {
     double *red = nullptr;
     double *h_red = nullptr;
     int *d_sweeps = nullptr;
+    unsigned long long *d_max = nullptr;
+    // RK4 time (Runge_kutta_O4::t_) and the phi history for extrapolated starts
+    double t = 0., t_stage = 0.;
+    double *phi_a = nullptr;
+    double tau_a = 0., tau_b = 0.;
+    int nhist = 0;
     AxisJob *dj = nullptr;
     ZJob *dz = nullptr;
     // job-list offsets (into dj / dz) and counts
@@ -192,16 +198,18 @@ int red_blocks(long N) {
 
 double max_residual(kf_ctx *c, const LevelBuf &L, const double *phi, const double *rho, bool fast) {
     const long N = (long)L.n * L.n * L.n;
-    const int nb = red_blocks(N);
+    CK(cudaMemsetAsync(c->d_max, 0, sizeof(unsigned long long), c->st));
     {
         Launch L_(c, KC_RESID, 16. * N);
         if (fast)
-            k_residual<RBS, true><<<nb, RBS, 0, c->st>>>(phi, rho, L.lev(), nullptr, c->partial);
+            k_resmax<true><<<nblk(N, 256), 256, 0, c->st>>>(phi, rho, L.lev(), c->d_max);
         else
-            k_residual<RBS, false><<<nb, RBS, 0, c->st>>>(phi, rho, L.lev(), nullptr, c->partial);
+            k_resmax<false><<<nblk(N, 256), 256, 0, c->st>>>(phi, rho, L.lev(), c->d_max);
     }
-    reduce_read(c, nb);
-    return c->h_red[4];
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(c->h_red, c->d_max, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return c->h_red[0];
 }
 
 // solver_poisson_jacobi_nlin::solve (:50-108) on one level; phi, tmp: level-sized.
@@ -363,6 +371,23 @@ int poisson(kf_ctx *c) {
     return rc;
 }
 
+// Start of a solve at time t_stage: linear extrapolation of the last two
+// solutions at distinct times (returns whether t_stage is a new time).
+bool phi_guess(kf_ctx *c) {
+    const double t = c->t_stage;
+    const bool newtime = c->nhist == 0 || t != c->tau_b;
+    if (!c->cfg.phi_extrap || !newtime || c->nhist == 0) return newtime;
+    if (c->nhist >= 2) {
+        const double w = (t - c->tau_b) / (c->tau_b - c->tau_a);
+        Launch L_(c, KC_MISC, 24. * c->N);
+        k_extrap<<<nblk(c->N, 256), 256, 0, c->st>>>(c->phi, c->phi_a, w, c->N);
+    } else {
+        CK(cudaMemcpyAsync(c->phi_a, c->phi, 8 * c->N, cudaMemcpyDeviceToDevice, c->st));
+    }
+    c->tau_a = c->tau_b;
+    return newtime;
+}
+
 // ------------------------------------------------------------------ per-(T, N) implementation
 template <typename T, int N> struct Impl {
     typedef typename C2<T>::type T2;
@@ -461,8 +486,13 @@ template <typename T, int N> struct Impl {
                 k_rho<T><<<nblk(c->N, 256), 256, 0, c->st>>>((const T *)c->R[0], c->nd, c->rho, c->N);
             }
             CK(cudaGetLastError());
+            const bool newtime = phi_guess(c);
             int rc = poisson(c);
             if (rc) throw KfError{KF_ERR_NOT_CONVERGED, "Poisson solve did not reach its tolerance"};
+            if (c->cfg.phi_extrap && newtime) {
+                c->nhist = c->nhist < 2 ? c->nhist + 1 : 2;
+                c->tau_b = c->t_stage;
+            }
         }
         // B
         if (Tm & T_E_INT) {
@@ -859,6 +889,8 @@ void create(kf_ctx *c) {
     c->partial = dalloc<double>(c, sizeof(double) * KF_RED * c->npartial);
     c->red = dalloc<double>(c, sizeof(double) * 8);
     c->d_sweeps = dalloc<int>(c, sizeof(int) * 4);
+    c->d_max = dalloc<unsigned long long>(c, sizeof(unsigned long long));
+    if (cf.phi_extrap) c->phi_a = dalloc<double>(c, 8 * c->N);
     CK(cudaMallocHost(&c->h_red, sizeof(double) * 8));
     build_tables(c);
     build_levels(c);
@@ -985,6 +1017,7 @@ int kf_set_state(kf_ctx *c, const double *ux, const double *uy, const double *uz
         const double *src[4] = {ux, uy, uz, s};
         for (int q = 0; q < 4; ++q) put_bulk(c, c->Y[q], src[q], 2 * c->Nc);
         copy_state(c, c->Ys, c->Y);
+        c->nhist = 0;
         CK(cudaStreamSynchronize(c->st));
     });
 }
@@ -1009,6 +1042,7 @@ int kf_set_sources(kf_ctx *c, const double *nd, const double *mask) {
 int kf_set_phi(kf_ctx *c, const double *phi) {
     return guarded(c, [&] {
         CK(cudaMemcpyAsync(c->phi, phi, 8 * c->N, cudaMemcpyHostToDevice, c->st));
+        c->nhist = 0;
         CK(cudaStreamSynchronize(c->st));
     });
 }
@@ -1021,8 +1055,8 @@ int kf_get_phi(kf_ctx *c, double *phi) {
 }
 
 int kf_rhs_eval(kf_ctx *c, double t) {
-    (void)t;
     return guarded(c, [&] {
+        c->t_stage = t;  // selects the start of the Poisson solve only
         copy_state(c, c->Ys, c->Y);
         c->rhs_fn(c);
         copy_state(c, c->Y, c->K);
@@ -1035,16 +1069,22 @@ int kf_rk4_steps(kf_ctx *c, int nsteps, double dt) {
     return guarded(c, [&] {
         if (nsteps < 0) throw KfError{KF_ERR_ARG, "nsteps < 0"};
         for (int s = 0; s < nsteps; ++s) {
-            // Ys == Y on entry
+            // Ys == Y on entry; stage times t, t + dt/2, t + dt/2, t + dt (RKO4.cpp:105-212)
+            const double t0 = c->t;
+            c->t_stage = t0;
             c->rhs_fn(c);
             rk_launch(c, 0.5 * dt, 0);
+            c->t_stage = t0 + 0.5 * dt;
             c->rhs_fn(c);
             rk_launch(c, 0.5 * dt, 1);
+            c->t_stage = t0 + 0.5 * dt;
             c->rhs_fn(c);
             rk_launch(c, 1.0 * dt, 1);
+            c->t_stage = t0 + 1.0 * dt;
             c->rhs_fn(c);
             rk_launch(c, dt / 6., 2);
             copy_state(c, c->Ys, c->Y);
+            c->t = t0 + dt;
         }
         CK(cudaGetLastError());
     });

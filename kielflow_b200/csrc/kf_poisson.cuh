@@ -191,6 +191,36 @@ __global__ void __launch_bounds__(BS) k_residual(const double *__restrict__ phi,
     block_reduce5<BS>(v, sh, partial + (long)blockIdx.x * KF_RED);
 }
 
+// max |f(phi)| over the grid, one point per thread, combined with an atomic
+// max on the IEEE bit patterns (order-free; NaN sorts above +inf).
+template <bool FAST>
+__global__ void __launch_bounds__(256) k_resmax(const double *__restrict__ phi, const double *__restrict__ rho,
+                                                Lev L, unsigned long long *__restrict__ out) {
+    const int n = L.n;
+    const long N = (long)n * n * n;
+    const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    double af = 0.;
+    if (id < N) {
+        const int k = (int)(id % n);
+        const long rr = id / n;
+        const int j = (int)(rr % n), i = (int)(rr / n);
+        double A, D;
+        coeffs_t<FAST>(phi, rho, L, i, j, k, A, D);
+        af = fabs(f_point(A, D, phi[id]));
+    }
+    for (int o = 16; o > 0; o >>= 1) af = nmax(af, __shfl_xor_sync(0xffffffffu, af, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(af));
+}
+
+// phi <- phi + w (phi - phi_a), phi_a <- old phi  (start of a solve at a new time)
+__global__ void k_extrap(double *__restrict__ phi, double *__restrict__ phi_a, double w, long N) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const double b = phi[i], a = phi_a[i];
+    phi[i] = __dadd_rn(b, __dmul_rn(w, __dsub_rn(b, a)));
+    phi_a[i] = b;
+}
+
 // Red-black Gauss-Seidel-Newton half sweep (colour (i+j+k)%2): one Newton step per point.
 __global__ void k_rbgs(double *__restrict__ phi, const double *__restrict__ rho, Lev L, int color) {
     const int n = L.n, nh = n / 2;

@@ -156,6 +156,12 @@ struct kfo_ctx {
     double supremum = 0., infinum = 0., omega_SOR = 1.;
     kfo_poisson_stats stats{};
     std::vector<level> lv;     /* lv[0] finest */
+    /* time of the RK4 driver (Runge_kutta_O4::t_, RKO4.cpp:42,240) and the phi
+     * history used to extrapolate the start of each solve at a new time */
+    double t = 0.;
+    vec phi_a;
+    double tau_a = 0., tau_b = 0.;
+    int nhist = 0;
 };
 
 namespace {
@@ -491,8 +497,32 @@ int poisson(kfo_ctx *c, vec &phi, const vec &rho) {
 
 /* ------------------------------------------------------------------ the RHS */
 
+/* Start of the Poisson solve at time t: with two earlier solutions at distinct
+ * times, phi <- phi_b + (t - tau_b)/(tau_b - tau_a) (phi_b - phi_a). */
+void phi_guess(kfo_ctx *c, double t, bool &newtime) {
+    newtime = c->nhist == 0 || t != c->tau_b;
+    if (!c->cfg.phi_extrap || !newtime || c->nhist == 0) return;
+    if (c->nhist >= 2) {
+        const double w = (t - c->tau_b) / (c->tau_b - c->tau_a);
+        for (size_t i = 0; i < c->N; ++i) {
+            const double b = c->Phi[i], a = c->phi_a[i];
+            c->Phi[i] = b + w * (b - a);
+            c->phi_a[i] = b;
+        }
+    } else {
+        c->phi_a = c->Phi;
+    }
+    c->tau_a = c->tau_b;
+}
+
+void phi_record(kfo_ctx *c, double t, bool newtime) {
+    if (!c->cfg.phi_extrap || !newtime) return;
+    c->nhist = c->nhist < 2 ? c->nhist + 1 : 2;
+    c->tau_b = t;
+}
+
 /* rhs_standard::solve (rhs_standard.cpp:89-566) with runtime term switches. */
-int rhs(kfo_ctx *c, vec *FU, vec &Fni) {
+int rhs(kfo_ctx *c, vec *FU, vec &Fni, double t) {
     const int T = c->cfg.terms;
     const kfo_config &cf = c->cfg;
     const size_t Nc = c->Nc, N = c->N;
@@ -505,8 +535,11 @@ int rhs(kfo_ctx *c, vec *FU, vec &Fni) {
         dealias(c, F1);
         c2r(c, F1, b1);
         for (size_t i = 0; i < N; ++i) b1[i] = exp(b1[i]) + c->nd[i];
+        bool newtime;
+        phi_guess(c, t, newtime);
         rc = poisson(c, c->Phi, b1);
         if (rc) return rc;
+        phi_record(c, t, newtime);
     }
     /* [dissipation & spectral viscosity] :119-209 */
     const bool diss = T & KFO_DISSIPATION, sv = T & KFO_SVISCOSITY;
@@ -687,6 +720,7 @@ void kfo_set_state(kfo_ctx *c, const double *ux, const double *uy, const double 
     const double *src[3] = {ux, uy, uz};
     for (int q = 0; q < 3; ++q) std::memcpy(c->FU[q].data(), src[q], sizeof(double) * 2 * c->Nc);
     std::memcpy(c->Fs.data(), s, sizeof(double) * 2 * c->Nc);
+    c->nhist = 0;
 }
 
 void kfo_get_state(kfo_ctx *c, double *ux, double *uy, double *uz, double *s) {
@@ -700,12 +734,16 @@ void kfo_set_sources(kfo_ctx *c, const double *nd, const double *mask) {
     if (mask) std::memcpy(c->mask.data(), mask, sizeof(double) * c->N);
 }
 
-void kfo_set_phi(kfo_ctx *c, const double *phi) { std::memcpy(c->Phi.data(), phi, sizeof(double) * c->N); }
+void kfo_set_phi(kfo_ctx *c, const double *phi) {
+    std::memcpy(c->Phi.data(), phi, sizeof(double) * c->N);
+    c->nhist = 0;
+}
 void kfo_get_phi(kfo_ctx *c, double *phi) { std::memcpy(phi, c->Phi.data(), sizeof(double) * c->N); }
 
 int kfo_rhs(kfo_ctx *c, double t) {
-    (void)t; /* the right-hand side is autonomous (rhs_standard.cpp never reads t) */
-    return rhs(c, c->FU, c->Fs);
+    /* the right-hand side is autonomous (rhs_standard.cpp never reads t); t
+     * only selects the start of the Poisson solve */
+    return rhs(c, c->FU, c->Fs, t);
 }
 
 /* Runge_kutta_O4::solve (RKO4.cpp:50-241) */
@@ -715,30 +753,34 @@ int kfo_rk4(kfo_ctx *c, double dt, int nsteps) {
         vec R0[4], R1[4], R2[4], R3[4], R4[4];
         vec *Y[4] = {&c->FU[0], &c->FU[1], &c->FU[2], &c->Fs};
         for (int q = 0; q < 4; ++q) { R0[q] = *Y[q]; R1[q] = *Y[q]; }
-        int rc = rhs(c, R1, R1[3]);
+        const double t0 = c->t;
+        int rc = rhs(c, R1, R1[3], t0);
         if (rc) return rc;
         for (int q = 0; q < 4; ++q) {
             R2[q].resize(M);
             for (size_t i = 0; i < M; ++i) R2[q][i] = R0[q][i] + 0.5 * dt * R1[q][i];
         }
-        if ((rc = rhs(c, R2, R2[3]))) return rc;
+        if ((rc = rhs(c, R2, R2[3], t0 + 0.5 * dt))) return rc;
         for (int q = 0; q < 4; ++q) {
             R3[q].resize(M);
             for (size_t i = 0; i < M; ++i) R3[q][i] = R0[q][i] + 0.5 * dt * R2[q][i];
         }
-        if ((rc = rhs(c, R3, R3[3]))) return rc;
+        if ((rc = rhs(c, R3, R3[3], t0 + 0.5 * dt))) return rc;
         for (int q = 0; q < 4; ++q) {
             R4[q].resize(M);
             for (size_t i = 0; i < M; ++i) R4[q][i] = R0[q][i] + 1.0 * dt * R3[q][i];
         }
-        if ((rc = rhs(c, R4, R4[3]))) return rc;
+        if ((rc = rhs(c, R4, R4[3], t0 + 1.0 * dt))) return rc;
         for (int q = 0; q < 4; ++q)
             for (size_t i = 0; i < M; ++i)
                 (*Y[q])[i] = R0[q][i] + (dt / 6.) * (1. * R1[q][i] + 2. * R2[q][i] + 2. * R3[q][i] +
                                                       1. * R4[q][i]);
+        c->t = t0 + dt;
     }
     return 0;
 }
+
+double kfo_time(kfo_ctx *c) { return c->t; }
 
 int kfo_poisson(kfo_ctx *c, double *phi_io, const double *rho) {
     vec phi(phi_io, phi_io + c->N), r(rho, rho + c->N);

@@ -55,6 +55,7 @@ typedef struct {
     int mg_pre, mg_post; /* FAS smoothing sweeps                                 */
     double coarse_tol;   /* FAS coarsest-level residual target                   */
     int max_cycles;      /* FAS V-cycle cap per solve                            */
+    int phi_extrap;      /* linear extrapolation of phi in time for the start    */
 } kfo_config;
 
 typedef struct kfo_ctx kfo_ctx;
@@ -77,6 +78,7 @@ void kfo_set_phi(kfo_ctx *c, const double *phi);
 void kfo_get_phi(kfo_ctx *c, double *phi);
 int kfo_rhs(kfo_ctx *c, double t);
 int kfo_rk4(kfo_ctx *c, double dt, int nsteps);
+double kfo_time(kfo_ctx *c);
 int kfo_poisson(kfo_ctx *c, double *phi_io, const double *rho);
 void kfo_poisson_stats_get(kfo_ctx *c, kfo_poisson_stats *out);
 double kfo_residual(kfo_ctx *c, const double *phi, const double *rho);
