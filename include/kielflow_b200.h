@@ -148,6 +148,23 @@ int kf_profile_enable(kf_ctx *ctx, int on);
 int kf_profile_read(kf_ctx *ctx, int cls, double *ms, long long *launches, double *bytes);
 const char *kf_profile_class_name(int cls);
 
+/* kf_fft_r2c_noalloc -- no counterpart in the reference.  The forward 3-D
+ * transform of kf_fft_r2c for callers that cannot let a library allocate
+ * device memory (a host that owns a fixed device pool and only lends its
+ * plugins buffers, or a time-critical loop that cannot afford cudaMalloc's
+ * latency and device-wide synchronisation).  It needs no context and
+ * allocates nothing: in_real (n^3 doubles) and out_complex (n*n*(n/2+1)
+ * interleaved complex doubles) are device-accessible buffers the caller
+ * owns; the one intermediate array lives in a static device array of
+ * 2,166,784 bytes that every GPU loading this library holds until exit, so
+ * n is limited to 16, 32 or 64 (other n: KF_ERR_ARG).  Work is queued on
+ * cuda_stream (NULL: the legacy default stream) and the call returns
+ * without waiting.  All calls on one device share that array: calls that
+ * overlap on the GPU race and must be serialised by the caller.  The first
+ * call on each device looks up the array's device address; make it before
+ * any stream capture.  Errors are reported by kf_last_error(NULL). */
+int kf_fft_r2c_noalloc(int n, const double *in_real, double *out_complex, void *cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

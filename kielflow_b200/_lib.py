@@ -75,7 +75,7 @@ EXPORTS = [
     "kf_ctx_create", "kf_ctx_destroy", "kf_last_error", "kf_set_stream", "kf_synchronize", "kf_set_state",
     "kf_get_state", "kf_set_sources", "kf_set_phi", "kf_get_phi", "kf_rhs_eval", "kf_rk4_steps",
     "kf_poisson_solve", "kf_diag", "kf_fft_r2c", "kf_fft_c2r", "kf_state_device_ptrs", "kf_launch_count",
-    "kf_profile_enable", "kf_profile_read", "kf_profile_class_name",
+    "kf_profile_enable", "kf_profile_read", "kf_profile_class_name", "kf_fft_r2c_noalloc",
 ]
 KCLASSES = 16
 
@@ -117,6 +117,7 @@ def load_library():
     L.kf_profile_read.argtypes = [vp, ctypes.c_int, _D, ctypes.POINTER(ctypes.c_longlong), _D]
     L.kf_profile_class_name.argtypes = [ctypes.c_int]
     L.kf_profile_class_name.restype = ctypes.c_char_p
+    L.kf_fft_r2c_noalloc.argtypes = [ctypes.c_int, vp, vp, vp]
     _lib = L
     return L
 

@@ -956,10 +956,14 @@ template <typename F> int guarded(kf_ctx *c, F f) {
 
 }  // namespace
 
-// k_rk mode 2 writes the new state to y0; keep the stage input equal to it.
-extern "C" {
+// Message of the last failure that has no context (kf_ctx_create and the
+// context-free entry points); kf_last_error(NULL) returns it.
+std::string &kf_global_error() {
+    static thread_local std::string s;
+    return s;
+}
 
-static thread_local std::string g_create_err;
+extern "C" {
 
 int kf_ctx_create(const kf_config *cfg, kf_ctx **out) {
     if (!cfg || !out) return KF_ERR_ARG;
@@ -967,7 +971,7 @@ int kf_ctx_create(const kf_config *cfg, kf_ctx **out) {
     c->cfg = *cfg;
     int rc = guarded(c, [&] { create(c); });
     if (rc) {
-        g_create_err = c->err;
+        kf_global_error() = c->err;
         kf_ctx_destroy(c);
         *out = nullptr;
         return rc;
@@ -991,7 +995,7 @@ int kf_ctx_destroy(kf_ctx *c) {
     return KF_OK;
 }
 
-const char *kf_last_error(const kf_ctx *c) { return c ? c->err.c_str() : g_create_err.c_str(); }
+const char *kf_last_error(const kf_ctx *c) { return c ? c->err.c_str() : kf_global_error().c_str(); }
 
 int kf_set_stream(kf_ctx *c, void *stream) {
     return guarded(c, [&] {
