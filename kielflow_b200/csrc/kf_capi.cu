@@ -72,7 +72,7 @@ struct kf_ctx {
     double *red = nullptr;
     double *h_red = nullptr;
     int *d_sweeps = nullptr;
-    unsigned long long *d_max = nullptr;
+    unsigned long long *d_max = nullptr, *h_max = nullptr;
     // RK4 time (Runge_kutta_O4::t_) and the phi history for extrapolated starts
     double t = 0., t_stage = 0.;
     double *phi_a = nullptr;
@@ -198,18 +198,22 @@ int red_blocks(long N) {
 
 double max_residual(kf_ctx *c, const LevelBuf &L, const double *phi, const double *rho, bool fast) {
     const long N = (long)L.n * L.n * L.n;
-    CK(cudaMemsetAsync(c->d_max, 0, sizeof(unsigned long long), c->st));
+    CK(cudaMemsetAsync(c->d_max, 0, 64 * sizeof(unsigned long long), c->st));
     {
         Launch L_(c, KC_RESID, 16. * N);
         if (fast)
-            k_resmax<true><<<nblk(N, 256), 256, 0, c->st>>>(phi, rho, L.lev(), c->d_max);
+            k_resmax<true><<<mg_grid(L.n, L.n), mg_block(), 0, c->st>>>(phi, rho, L.lev(), c->d_max);
         else
-            k_resmax<false><<<nblk(N, 256), 256, 0, c->st>>>(phi, rho, L.lev(), c->d_max);
+            k_resmax<false><<<mg_grid(L.n, L.n), mg_block(), 0, c->st>>>(phi, rho, L.lev(), c->d_max);
     }
     CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(c->h_red, c->d_max, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(c->h_max, c->d_max, 64 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
-    return c->h_red[0];
+    unsigned long long m = 0;
+    for (int s = 0; s < 64; ++s) m = c->h_max[s] > m ? c->h_max[s] : m;
+    double r;
+    std::memcpy(&r, &m, sizeof(double));
+    return r;
 }
 
 // solver_poisson_jacobi_nlin::solve (:50-108) on one level; phi, tmp: level-sized.
@@ -272,35 +276,34 @@ void vcycle(kf_ctx *c, int l) {
         k_coarse_solve<<<1, 1024, 0, c->st>>>(L.phi, L.rho, L.lev(), cf.coarse_tol, 1000, c->d_sweeps);
         return;
     }
-    const long Mh = N / 2;
     for (int s = 0; s < cf.mg_pre; ++s)
         for (int color = 0; color < 2; ++color) {
             Launch L_(c, KC_RBGS, 16. * N);
-            k_rbgs<<<nblk(Mh, 256), 256, 0, c->st>>>(L.phi, L.rho, L.lev(), color);
+            k_rbgs<<<mg_grid(n / 2, n), mg_block(), 0, c->st>>>(L.phi, L.rho, L.lev(), color);
         }
     {
         Launch L_(c, KC_RESID, 24. * N);
-        k_residual<RBS, true><<<red_blocks(N), RBS, 0, c->st>>>(L.phi, L.rho, L.lev(), L.r, c->partial);
+        k_residual<true><<<mg_grid(n, n), mg_block(), 0, c->st>>>(L.phi, L.rho, L.lev(), L.r);
     }
     LevelBuf &Lc = c->lv[l + 1];
     const long Nc3 = (long)Lc.n * Lc.n * Lc.n;
     {
         Launch L_(c, KC_TRANSFER, 8. * N + 32. * Nc3);
-        k_restrict<<<nblk(Nc3, 256), 256, 0, c->st>>>(L.r, L.phi, n, Lc.r, Lc.phi, Lc.phi0);
+        k_restrict<<<mg_grid(Lc.n, Lc.n), mg_block(), 0, c->st>>>(L.r, L.phi, n, Lc.r, Lc.phi, Lc.phi0);
     }
     {
         Launch L_(c, KC_TRANSFER, 24. * Nc3);
-        k_fas_rhs<<<nblk(Nc3, 256), 256, 0, c->st>>>(Lc.phi, Lc.r, Lc.lev(), Lc.rho);
+        k_fas_rhs<<<mg_grid(Lc.n, Lc.n), mg_block(), 0, c->st>>>(Lc.phi, Lc.r, Lc.lev(), Lc.rho);
     }
     vcycle(c, l + 1);
     {
         Launch L_(c, KC_TRANSFER, 16. * N + 16. * Nc3);
-        k_prolong_add<<<nblk(N, 256), 256, 0, c->st>>>(L.phi, Lc.phi, Lc.phi0, L.gam, n);
+        k_prolong_add<<<mg_grid(n, n), mg_block(), 0, c->st>>>(L.phi, Lc.phi, Lc.phi0, L.gam, n);
     }
     for (int s = 0; s < cf.mg_post; ++s)
         for (int color = 0; color < 2; ++color) {
             Launch L_(c, KC_RBGS, 16. * N);
-            k_rbgs<<<nblk(Mh, 256), 256, 0, c->st>>>(L.phi, L.rho, L.lev(), color);
+            k_rbgs<<<mg_grid(n / 2, n), mg_block(), 0, c->st>>>(L.phi, L.rho, L.lev(), color);
         }
     CK(cudaGetLastError());
 }
@@ -326,7 +329,7 @@ int poisson(kf_ctx *c) {
         LevelBuf &L3 = c->lv[3];
         {
             Launch L_(c, KC_TRANSFER, 16. * L3.n * L3.n * L3.n);
-            k_inject<<<nblk((long)L3.n * L3.n * L3.n, 256), 256, 0, c->st>>>(c->phi, n, 8, L3.phi);
+            k_inject<<<mg_grid(L3.n, L3.n), mg_block(), 0, c->st>>>(c->phi, n, 8, L3.phi);
         }
         for (int cas = 0; cas < 4; ++cas) {
             const int l = 3 - cas;
@@ -335,13 +338,13 @@ int poisson(kf_ctx *c) {
             if (cas > 0) {
                 double *dst = l == 0 ? c->phi : L.phi;
                 Launch L_(c, KC_TRANSFER, 9. * Nl);
-                k_prolong_set<<<nblk(Nl, 256), 256, 0, c->st>>>(dst, c->lv[l + 1].phi, L.gam, L.n);
+                k_prolong_set<<<mg_grid(L.n, L.n), mg_block(), 0, c->st>>>(dst, c->lv[l + 1].phi, L.gam, L.n);
             }
             const double *rho_l = c->rho;
             if (l > 0) {
                 {
                     Launch L_(c, KC_TRANSFER, 16. * Nl);
-                    k_inject<<<nblk(Nl, 256), 256, 0, c->st>>>(c->rho, n, n / L.n, L.rho);
+                    k_inject<<<mg_grid(L.n, L.n), mg_block(), 0, c->st>>>(c->rho, n, n / L.n, L.rho);
                 }
                 rho_l = L.rho;
             }
@@ -445,7 +448,7 @@ template <typename T, int N> struct Impl {
     static void zc2r(kf_ctx *c, int off, int njobs) {
         const int nrows = N * N;
         const int ntiles = (nrows + LZ - 1) / LZ;
-        const size_t smem = (size_t)(2 * LZ * NZC + LZ * (N + 1)) * sizeof(T2);
+        const size_t smem = (size_t)(2 * LZ * NZC + LZ * PadLen<N>::value) * sizeof(T2);
         Launch L_(c, KC_Z_C2R, z_bytes(c, off, njobs, true));
         k_z_c2r<T, N><<<njobs * ntiles, LZ * P, smem, c->st>>>(c->dz + off, njobs, nrows, geo(c), (const T2 *)c->tw,
                                                              (T)(1. / ((double)N * N * N)));
@@ -453,7 +456,7 @@ template <typename T, int N> struct Impl {
     static void zr2c(kf_ctx *c, int off, int njobs) {
         const int nrows = N * N;
         const int ntiles = (nrows + LZ - 1) / LZ;
-        const size_t smem = (size_t)(LZ * (N + 1)) * sizeof(T2);
+        const size_t smem = (size_t)(LZ * PadLen<N>::value) * sizeof(T2);
         Launch L_(c, KC_Z_R2C, z_bytes(c, off, njobs, false));
         k_z_r2c<T, N><<<njobs * ntiles, LZ * P, smem, c->st>>>(c->dz + off, njobs, nrows, (const T2 *)c->tw);
     }
@@ -889,7 +892,8 @@ void create(kf_ctx *c) {
     c->partial = dalloc<double>(c, sizeof(double) * KF_RED * c->npartial);
     c->red = dalloc<double>(c, sizeof(double) * 8);
     c->d_sweeps = dalloc<int>(c, sizeof(int) * 4);
-    c->d_max = dalloc<unsigned long long>(c, sizeof(unsigned long long));
+    c->d_max = dalloc<unsigned long long>(c, 64 * sizeof(unsigned long long));
+    CK(cudaMallocHost(&c->h_max, 64 * sizeof(unsigned long long)));
     if (cf.phi_extrap) c->phi_a = dalloc<double>(c, 8 * c->N);
     CK(cudaMallocHost(&c->h_red, sizeof(double) * 8));
     build_tables(c);
@@ -990,6 +994,7 @@ int kf_ctx_destroy(kf_ctx *c) {
     for (auto e : c->evfree) cudaEventDestroy(e);
     for (void *p : c->allocs) cudaFree(p);
     if (c->h_red) cudaFreeHost(c->h_red);
+    if (c->h_max) cudaFreeHost(c->h_max);
     if (c->st && c->own_stream) cudaStreamDestroy(c->st);
     delete c;
     return KF_OK;

@@ -142,6 +142,16 @@ template <int SIGN> struct DFT<16, SIGN> : DFT2F<4, 4, SIGN> {};
 
 // ------------------------------------------------------------ stage engine
 
+// Shared-memory addressing of element r of a line.
+struct StrideAddr {  // columns interleaved: r * stride (+ the column offset in the base pointer)
+    int s;
+    __device__ __forceinline__ int operator()(int r) const { return r * s; }
+};
+struct PadAddr {  // one line contiguous, a pad word every 16: avoids the radix-16 scatter conflicts
+    __device__ __forceinline__ int operator()(int r) const { return r + (r >> 4); }
+};
+template <int N> struct PadLen { static constexpr int value = N + N / 16 + 1; };
+
 template <int... Rs> struct First;
 template <int R, int... Rest> struct First<R, Rest...> { static constexpr int value = R; };
 template <int... Rs> struct Last;
@@ -155,7 +165,8 @@ struct Stages {
     static constexpr int E = N / P;
     static constexpr int NB = N / (P * R);
     static_assert(NB * P * R == N, "radix does not tile the line");
-    __device__ __forceinline__ static void run(T2 *v, T2 *sm, int stride, int p, const T2 *__restrict__ tw) {
+    template <typename A>
+    __device__ __forceinline__ static void run(T2 *v, T2 *sm, A addr, int p, const T2 *__restrict__ tw) {
 #pragma unroll
         for (int b = 0; b < NB; ++b) {
             const int j = p + b * P;
@@ -178,7 +189,7 @@ struct Stages {
                 const int k = j % Ns;
                 const int idxD = (j / Ns) * Ns * R + k;
 #pragma unroll
-                for (int t = 0; t < R; ++t) sm[(idxD + t * Ns) * stride] = v[b * R + t];
+                for (int t = 0; t < R; ++t) sm[addr(idxD + t * Ns)] = v[b * R + t];
             }
             __syncthreads();
             constexpr int R2 = First<Rest...>::value;
@@ -186,16 +197,16 @@ struct Stages {
 #pragma unroll
             for (int b = 0; b < NB2; ++b)
 #pragma unroll
-                for (int t = 0; t < R2; ++t) v[b * R2 + t] = sm[(p + b * P + t * (N / R2)) * stride];
+                for (int t = 0; t < R2; ++t) v[b * R2 + t] = sm[addr(p + b * P + t * (N / R2))];
             __syncthreads();
-            Stages<T2, N, P, SIGN, Ns * R, Rest...>::run(v, sm, stride, p, tw);
+            Stages<T2, N, P, SIGN, Ns * R, Rest...>::run(v, sm, addr, p, tw);
         }
     }
 };
 
-template <typename T2, int N, int P, int SIGN, int... Rs>
-__device__ __forceinline__ void fft_line(T2 *v, T2 *sm, int stride, int p, const T2 *__restrict__ tw) {
-    Stages<T2, N, P, SIGN, 1, Rs...>::run(v, sm, stride, p, tw);
+template <typename T2, int N, int P, int SIGN, int... Rs, typename A>
+__device__ __forceinline__ void fft_line(T2 *v, T2 *sm, A addr, int p, const T2 *__restrict__ tw) {
+    Stages<T2, N, P, SIGN, 1, Rs...>::run(v, sm, addr, p, tw);
 }
 
 // Row index held by register q (= b*R + t) of thread p at the input of the
@@ -207,11 +218,11 @@ __device__ __forceinline__ int reg_row(int p, int q) {
 
 // Per-length launch plans: threads per line P and the radix sequence.
 template <int N> struct Plan;
-template <> struct Plan<16> { static constexpr int P = 4; template <typename T2, int S> __device__ static void fft(T2 *v, T2 *sm, int st, int p, const T2 *tw) { fft_line<T2, 16, 4, S, 4, 4>(v, sm, st, p, tw); } static constexpr int R1 = 4, RL = 4; };
-template <> struct Plan<32> { static constexpr int P = 4; template <typename T2, int S> __device__ static void fft(T2 *v, T2 *sm, int st, int p, const T2 *tw) { fft_line<T2, 32, 4, S, 8, 4>(v, sm, st, p, tw); } static constexpr int R1 = 8, RL = 4; };
-template <> struct Plan<64> { static constexpr int P = 8; template <typename T2, int S> __device__ static void fft(T2 *v, T2 *sm, int st, int p, const T2 *tw) { fft_line<T2, 64, 8, S, 8, 8>(v, sm, st, p, tw); } static constexpr int R1 = 8, RL = 8; };
-template <> struct Plan<96> { static constexpr int P = 8; template <typename T2, int S> __device__ static void fft(T2 *v, T2 *sm, int st, int p, const T2 *tw) { fft_line<T2, 96, 8, S, 6, 4, 4>(v, sm, st, p, tw); } static constexpr int R1 = 6, RL = 4; };
-template <> struct Plan<128> { static constexpr int P = 8; template <typename T2, int S> __device__ static void fft(T2 *v, T2 *sm, int st, int p, const T2 *tw) { fft_line<T2, 128, 8, S, 16, 8>(v, sm, st, p, tw); } static constexpr int R1 = 16, RL = 8; };
-template <> struct Plan<256> { static constexpr int P = 16; template <typename T2, int S> __device__ static void fft(T2 *v, T2 *sm, int st, int p, const T2 *tw) { fft_line<T2, 256, 16, S, 16, 16>(v, sm, st, p, tw); } static constexpr int R1 = 16, RL = 16; };
+template <> struct Plan<16> { static constexpr int P = 4; template <typename T2, int S, typename A> __device__ static void fft(T2 *v, T2 *sm, A a, int p, const T2 *tw) { fft_line<T2, 16, 4, S, 4, 4>(v, sm, a, p, tw); } static constexpr int R1 = 4, RL = 4; };
+template <> struct Plan<32> { static constexpr int P = 4; template <typename T2, int S, typename A> __device__ static void fft(T2 *v, T2 *sm, A a, int p, const T2 *tw) { fft_line<T2, 32, 4, S, 8, 4>(v, sm, a, p, tw); } static constexpr int R1 = 8, RL = 4; };
+template <> struct Plan<64> { static constexpr int P = 8; template <typename T2, int S, typename A> __device__ static void fft(T2 *v, T2 *sm, A a, int p, const T2 *tw) { fft_line<T2, 64, 8, S, 8, 8>(v, sm, a, p, tw); } static constexpr int R1 = 8, RL = 8; };
+template <> struct Plan<96> { static constexpr int P = 8; template <typename T2, int S, typename A> __device__ static void fft(T2 *v, T2 *sm, A a, int p, const T2 *tw) { fft_line<T2, 96, 8, S, 6, 4, 4>(v, sm, a, p, tw); } static constexpr int R1 = 6, RL = 4; };
+template <> struct Plan<128> { static constexpr int P = 8; template <typename T2, int S, typename A> __device__ static void fft(T2 *v, T2 *sm, A a, int p, const T2 *tw) { fft_line<T2, 128, 8, S, 16, 8>(v, sm, a, p, tw); } static constexpr int R1 = 16, RL = 8; };
+template <> struct Plan<256> { static constexpr int P = 16; template <typename T2, int S, typename A> __device__ static void fft(T2 *v, T2 *sm, A a, int p, const T2 *tw) { fft_line<T2, 256, 16, S, 16, 16>(v, sm, a, p, tw); } static constexpr int R1 = 16, RL = 16; };
 
 }  // namespace kf

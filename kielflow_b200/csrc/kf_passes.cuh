@@ -74,7 +74,7 @@ k_axis_pass(const AxisJob *__restrict__ jobs, int njobs, int axis, Geo<T> g,
         if (J.mul == MUL_P_IK || J.mul == MUL_IK) x = mul_ik(x, g.kv[row]);
         v[q] = x;
     }
-    Plan<N>::template fft<T2, SIGN>(v, sm + c, TC, p, tw);
+    Plan<N>::template fft<T2, SIGN>(v, sm + c, StrideAddr{TC}, p, tw);
     if (valid) {
 #pragma unroll
         for (int q = 0; q < E; ++q) {
@@ -98,7 +98,7 @@ k_z_c2r(const ZJob *__restrict__ jobs, int njobs, int nrows, Geo<T> g,
         const typename C2<T>::type *__restrict__ tw, T scale) {
     typedef typename C2<T>::type T2;
     constexpr int LZ = ZTile<T>::LZ, P = Plan<N>::P, E = N / P, NZC = N / 2 + 1;
-    constexpr int LS = N + 1;  // padded line stride of the exchange buffer
+    constexpr int LS = PadLen<N>::value;  // padded line of the exchange buffer
     extern __shared__ __align__(16) unsigned char kf_smem[];
     T2 *half = reinterpret_cast<T2 *>(kf_smem);  // [2][LZ][NZC]
     T2 *xch = half + 2 * LZ * NZC;               // [LZ][LS]
@@ -142,7 +142,7 @@ k_z_c2r(const ZJob *__restrict__ jobs, int njobs, int nrows, Geo<T> g,
         }
         v[q] = mk<T2>(a.x - b.y, a.y + b.x);  // A + iB
     }
-    Plan<N>::template fft<T2, +1>(v, xch + l * LS, 1, p, tw);
+    Plan<N>::template fft<T2, +1>(v, xch + l * LS, PadAddr{}, p, tw);
     const int r = r0 + l;
     if (r < nrows) {
         T *oA = static_cast<T *>(J.outA) + (long)r * N;
@@ -163,9 +163,9 @@ k_z_r2c(const ZJob *__restrict__ jobs, int njobs, int nrows,
         const typename C2<T>::type *__restrict__ tw) {
     typedef typename C2<T>::type T2;
     constexpr int LZ = ZTile<T>::LZ, P = Plan<N>::P, E = N / P, NZC = N / 2 + 1;
-    constexpr int LS = N + 1;
+    constexpr int LS = PadLen<N>::value;
     extern __shared__ __align__(16) unsigned char kf_smem[];
-    T2 *xch = reinterpret_cast<T2 *>(kf_smem);  // [LZ][LS]
+    T2 *xch = reinterpret_cast<T2 *>(kf_smem);  // [LZ][LS], padded lines
     const int job = blockIdx.x % njobs, tile = blockIdx.x / njobs;
     const ZJob J = jobs[job];
     const int r0 = tile * LZ;
@@ -185,17 +185,18 @@ k_z_r2c(const ZJob *__restrict__ jobs, int njobs, int nrows,
         v[q] = mk<T2>(a, b);
     }
     T2 *line = xch + l * LS;
-    Plan<N>::template fft<T2, -1>(v, line, 1, p, tw);
+    const PadAddr pa;
+    Plan<N>::template fft<T2, -1>(v, line, pa, p, tw);
     __syncthreads();
 #pragma unroll
-    for (int q = 0; q < E; ++q) line[reg_row<N, P, Plan<N>::RL>(p, q)] = v[q];
+    for (int q = 0; q < E; ++q) line[pa(reg_row<N, P, Plan<N>::RL>(p, q))] = v[q];
     __syncthreads();
     for (int idx = threadIdx.x; idx < LZ * NZC; idx += blockDim.x) {
         const int ll = idx / NZC, k = idx - ll * NZC;
         const int rr = r0 + ll;
         if (rr >= nrows) continue;
-        const T2 zk = xch[ll * LS + k];
-        const T2 zm = xch[ll * LS + (N - k) % N];
+        const T2 zk = xch[ll * LS + pa(k)];
+        const T2 zm = xch[ll * LS + pa((N - k) % N)];
         const T cr = zm.x, ci = -zm.y;  // conj(Z[N-k])
         T2 *oA = static_cast<T2 *>(J.outA) + (long)rr * NZC;
         oA[k] = mk<T2>((T)0.5 * (zk.x + cr), (T)0.5 * (zk.y + ci));
@@ -312,7 +313,7 @@ k_xfwd_assemble(const AxisJob *__restrict__ jobs, Geo<T> g, RhsArgs<T> a,
             const int row = reg_row<N, P, Plan<N>::R1>(p, e);
             v[e] = valid ? in[col + row * rstride] : mk<T2>((T)0, (T)0);
         }
-        Plan<N>::template fft<T2, -1>(v, sm + c, TC, p, tw);
+        Plan<N>::template fft<T2, -1>(v, sm + c, StrideAddr{TC}, p, tw);
         if (valid) {
 #pragma unroll
             for (int e = 0; e < E; ++e) {

@@ -168,48 +168,46 @@ __global__ void __launch_bounds__(BS) k_reduce_final(const double *__restrict__ 
     block_reduce5<BS>(v, sh, out);
 }
 
-// Pointwise residual r = f(phi) = lap_h phi + rho - e^phi (+ block max |r|, NaN-propagating)
-template <int BS, bool FAST>
-__global__ void __launch_bounds__(BS) k_residual(const double *__restrict__ phi, const double *__restrict__ rho,
-                                                 Lev L, double *__restrict__ r, double *__restrict__ partial) {
-    __shared__ double sh[KF_RED * BS];
+// Launch geometry of the multigrid kernels: block (32, 8), grid
+// (ceil(nx/32), ceil(n/8), n) over (k or k/2, j, i) -- no index division.
+inline dim3 mg_grid(int nx, int n) { return dim3((nx + 31) / 32, (n + 7) / 8, n); }
+inline dim3 mg_block() { return dim3(32, 8, 1); }
+
+// Pointwise residual r = f(phi) = lap_h phi + rho - e^phi on the whole level.
+template <bool FAST>
+__global__ void __launch_bounds__(256) k_residual(const double *__restrict__ phi, const double *__restrict__ rho,
+                                                  Lev L, double *__restrict__ r) {
     const int n = L.n;
-    const long N = (long)n * n * n;
-    double v[KF_RED] = {0., 0., -INFINITY, INFINITY, 0.};
-    for (long id = (long)blockIdx.x * BS + threadIdx.x; id < N; id += (long)gridDim.x * BS) {
-        const int k = (int)(id % n);
-        const long rr = id / n;
-        const int j = (int)(rr % n), i = (int)(rr / n);
-        double A, D;
-        coeffs_t<FAST>(phi, rho, L, i, j, k, A, D);
-        const double f = f_point(A, D, phi[id]);
-        if (r) r[id] = f;
-        const double af = fabs(f);
-        v[4] = nmax(v[4], af);
-        v[1] = __dadd_rn(v[1], af);
-    }
-    block_reduce5<BS>(v, sh, partial + (long)blockIdx.x * KF_RED);
+    const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, i = blockIdx.z;
+    if (k >= n || j >= n) return;
+    double A, D;
+    coeffs_t<FAST>(phi, rho, L, i, j, k, A, D);
+    const long id = lidx(i, j, k, n);
+    r[id] = f_point(A, D, phi[id]);
 }
 
-// max |f(phi)| over the grid, one point per thread, combined with an atomic
-// max on the IEEE bit patterns (order-free; NaN sorts above +inf).
+// max |f(phi)| over the level: block maximum, then an atomic max on the IEEE
+// bit pattern (order-free; NaN sorts above +inf) into one of 64 slots.
 template <bool FAST>
 __global__ void __launch_bounds__(256) k_resmax(const double *__restrict__ phi, const double *__restrict__ rho,
                                                 Lev L, unsigned long long *__restrict__ out) {
+    __shared__ double sh[8];
     const int n = L.n;
-    const long N = (long)n * n * n;
-    const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, i = blockIdx.z;
     double af = 0.;
-    if (id < N) {
-        const int k = (int)(id % n);
-        const long rr = id / n;
-        const int j = (int)(rr % n), i = (int)(rr / n);
+    if (k < n && j < n) {
         double A, D;
         coeffs_t<FAST>(phi, rho, L, i, j, k, A, D);
-        af = fabs(f_point(A, D, phi[id]));
+        af = fabs(f_point(A, D, phi[lidx(i, j, k, n)]));
     }
     for (int o = 16; o > 0; o >>= 1) af = nmax(af, __shfl_xor_sync(0xffffffffu, af, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(af));
+    if (threadIdx.x == 0) sh[threadIdx.y] = af;
+    __syncthreads();
+    if (threadIdx.y == 0 && threadIdx.x == 0) {
+        double m = sh[0];
+        for (int w = 1; w < 8; ++w) m = nmax(m, sh[w]);
+        atomicMax(out + (blockIdx.z & 63), (unsigned long long)__double_as_longlong(m));
+    }
 }
 
 // phi <- phi + w (phi - phi_a), phi_a <- old phi  (start of a solve at a new time)
@@ -221,15 +219,13 @@ __global__ void k_extrap(double *__restrict__ phi, double *__restrict__ phi_a, d
     phi_a[i] = b;
 }
 
-// Red-black Gauss-Seidel-Newton half sweep (colour (i+j+k)%2): one Newton step per point.
-__global__ void k_rbgs(double *__restrict__ phi, const double *__restrict__ rho, Lev L, int color) {
-    const int n = L.n, nh = n / 2;
-    const long M = (long)n * n * nh;
-    const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= M) return;
-    const int k2 = (int)(id % nh);
-    const long r = id / nh;
-    const int j = (int)(r % n), i = (int)(r / n);
+// Red-black Gauss-Seidel-Newton half sweep (colour (i+j+k)%2): one Newton
+// step per point; grid over (k/2, j, i).
+__global__ void __launch_bounds__(256) k_rbgs(double *__restrict__ phi, const double *__restrict__ rho, Lev L,
+                                              int color) {
+    const int n = L.n;
+    const int k2 = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, i = blockIdx.z;
+    if (2 * k2 >= n || j >= n) return;
     const int k = 2 * k2 + ((i + j + color) & 1);
     double A, D;
     point_coeffs_fast(phi, rho, L, i, j, k, A, D);
@@ -247,10 +243,10 @@ __global__ void __launch_bounds__(1024) k_coarse_solve(double *__restrict__ phi,
     int s = 0;
     for (;; ++s) {
         double m = 0.;
-        for (long id = threadIdx.x; id < N; id += blockDim.x) {
-            const int k = (int)(id % n);
-            const long r = id / n;
-            const int j = (int)(r % n), i = (int)(r / n);
+        for (int id = threadIdx.x; id < (int)N; id += blockDim.x) {
+            const int k = id % n;
+            const int r = id / n;
+            const int j = r % n, i = r / n;
             double A, D;
             point_coeffs_fast(phi, rho, L, i, j, k, A, D);
             const double af = fabs(f_point(A, D, phi[id]));
@@ -275,12 +271,12 @@ __global__ void __launch_bounds__(1024) k_coarse_solve(double *__restrict__ phi,
         __syncthreads();
         if (!(res > tol) || s >= max_sweeps) break;  // converged, NaN or capped
         for (int color = 0; color < 2; ++color) {
-            const long M = N / 2;
-            for (long id = threadIdx.x; id < M; id += blockDim.x) {
+            const int M = (int)(N / 2);
+            for (int id = threadIdx.x; id < M; id += blockDim.x) {
                 const int nh = n / 2;
-                const int k2 = (int)(id % nh);
-                const long r = id / nh;
-                const int j = (int)(r % n), i = (int)(r / n);
+                const int k2 = id % nh;
+                const int r = id / nh;
+                const int j = r % n, i = r / n;
                 const int k = 2 * k2 + ((i + j + color) & 1);
                 double A, D;
                 point_coeffs_fast(phi, rho, L, i, j, k, A, D);
@@ -295,15 +291,13 @@ __global__ void __launch_bounds__(1024) k_coarse_solve(double *__restrict__ phi,
 
 // Full-weighting restriction of r (fine n) and injection of phi:
 // rc = FW(r), phic = phic0 = phi[2i,2j,2k]  (field_interpolation.cpp:233-259 for phi)
-__global__ void k_restrict(const double *__restrict__ r, const double *__restrict__ phi, int nf,
-                           double *__restrict__ rc, double *__restrict__ phic, double *__restrict__ phic0) {
+__global__ void __launch_bounds__(256) k_restrict(const double *__restrict__ r, const double *__restrict__ phi, int nf,
+                                                  double *__restrict__ rc, double *__restrict__ phic,
+                                                  double *__restrict__ phic0) {
     const int nc = nf / 2;
-    const long Mc = (long)nc * nc * nc;
-    const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= Mc) return;
-    const int k = (int)(id % nc);
-    const long rr = id / nc;
-    const int j = (int)(rr % nc), i = (int)(rr / nc);
+    const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, i = blockIdx.z;
+    if (k >= nc || j >= nc) return;
+    const long id = lidx(i, j, k, nc);
     const double w[3] = {0.25, 0.5, 0.25};
     double s = 0.;
     for (int a = -1; a <= 1; ++a) {
@@ -327,15 +321,12 @@ __global__ void k_restrict(const double *__restrict__ r, const double *__restric
 }
 
 // rho_c = N_c(phi_c) + r_c with N(phi) = -lap_h phi + e^phi
-__global__ void k_fas_rhs(const double *__restrict__ phic, const double *__restrict__ rc, Lev L,
-                          double *__restrict__ rhoc) {
+__global__ void __launch_bounds__(256) k_fas_rhs(const double *__restrict__ phic, const double *__restrict__ rc, Lev L,
+                                                 double *__restrict__ rhoc) {
     const int n = L.n;
-    const long N = (long)n * n * n;
-    const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= N) return;
-    const int k = (int)(id % n);
-    const long rr = id / n;
-    const int j = (int)(rr % n), i = (int)(rr / n);
+    const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, i = blockIdx.z;
+    if (k >= n || j >= n) return;
+    const long id = lidx(i, j, k, n);
     double A, D;
     point_coeffs_fast(phic, nullptr, L, i, j, k, A, D);
     const double Nc = __dsub_rn(0., f_point(A, D, phic[id]));
@@ -362,14 +353,12 @@ __device__ __forceinline__ double py(const double *pc, const double *pc0, const 
     return __dadd_rn(__dmul_rn(1. - g, pz(pc, pc0, gam, nf, i, j - 1, k)),
                      __dmul_rn(g, pz(pc, pc0, gam, nf, i, (j + 1) % nf, k)));
 }
-__global__ void k_prolong_add(double *__restrict__ phi, const double *__restrict__ pc, const double *__restrict__ pc0,
-                              const double *__restrict__ gam, int nf) {
-    const long N = (long)nf * nf * nf;
-    const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= N) return;
-    const int k = (int)(id % nf);
-    const long rr = id / nf;
-    const int j = (int)(rr % nf), i = (int)(rr / nf);
+__global__ void __launch_bounds__(256) k_prolong_add(double *__restrict__ phi, const double *__restrict__ pc,
+                                                     const double *__restrict__ pc0, const double *__restrict__ gam,
+                                                     int nf) {
+    const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, i = blockIdx.z;
+    if (k >= nf || j >= nf) return;
+    const long id = lidx(i, j, k, nf);
     double e;
     if ((i & 1) == 0) {
         e = py(pc, pc0, gam, nf, i, j, k);
@@ -382,28 +371,22 @@ __global__ void k_prolong_add(double *__restrict__ phi, const double *__restrict
 }
 
 // Strided injection (OP_2htoh_lvl0 / OP_4htoh / OP_8htoh)
-__global__ void k_inject(const double *__restrict__ in, int nf, int step, double *__restrict__ out) {
+__global__ void __launch_bounds__(256) k_inject(const double *__restrict__ in, int nf, int step,
+                                                double *__restrict__ out) {
     const int nc = nf / step;
-    const long M = (long)nc * nc * nc;
-    const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= M) return;
-    const int k = (int)(id % nc);
-    const long rr = id / nc;
-    const int j = (int)(rr % nc), i = (int)(rr / nc);
-    out[id] = in[lidx(step * i, step * j, step * k, nf)];
+    const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, i = blockIdx.z;
+    if (k >= nc || j >= nc) return;
+    out[lidx(i, j, k, nc)] = in[lidx(step * i, step * j, step * k, nf)];
 }
 
 // OP_hto2h (plain, not a correction): out(2n) = trilinear(in(n)); used by the
 // cascadic plan.  Same pass order as k_prolong_add with phic0 == 0.
-__global__ void k_prolong_set(double *__restrict__ out, const double *__restrict__ pc,
-                              const double *__restrict__ gam, int nf) {
+__global__ void __launch_bounds__(256) k_prolong_set(double *__restrict__ out, const double *__restrict__ pc,
+                                                     const double *__restrict__ gam, int nf) {
     const double *zero = nullptr;
-    const long N = (long)nf * nf * nf;
-    const long id = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= N) return;
-    const int k = (int)(id % nf);
-    const long rr = id / nf;
-    const int j = (int)(rr % nf), i = (int)(rr / nf);
+    const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, i = blockIdx.z;
+    if (k >= nf || j >= nf) return;
+    const long id = lidx(i, j, k, nf);
     double e;
     if ((i & 1) == 0) {
         e = py(pc, zero, gam, nf, i, j, k);
