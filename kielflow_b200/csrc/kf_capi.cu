@@ -272,8 +272,10 @@ void vcycle(kf_ctx *c, int l) {
     const int n = L.n;
     const long N = (long)n * n * n;
     if (l == (int)c->lv.size() - 1) {
-        Launch L_(c, KC_COARSE, 0.);
-        k_coarse_solve<<<1, 1024, 0, c->st>>>(L.phi, L.rho, L.lev(), cf.coarse_tol, 1000, c->d_sweeps);
+        Launch L_(c, KC_COARSE, 16. * N);
+        const int bs = N >= 1024 ? 1024 : (int)((N + 31) / 32 * 32);
+        k_coarse_solve<<<1, bs, (size_t)(16 * N + 24 * n), c->st>>>(L.phi, L.rho, L.lev(), cf.coarse_tol, 1000,
+                                                                   c->d_sweeps);
         return;
     }
     for (int s = 0; s < cf.mg_pre; ++s)
@@ -297,8 +299,12 @@ void vcycle(kf_ctx *c, int l) {
     }
     vcycle(c, l + 1);
     {
-        Launch L_(c, KC_TRANSFER, 16. * N + 16. * Nc3);
-        k_prolong_add<<<mg_grid(n, n), mg_block(), 0, c->st>>>(L.phi, Lc.phi, Lc.phi0, L.gam, n);
+        Launch L_(c, KC_TRANSFER, 24. * Nc3);
+        k_correction<<<mg_grid(Lc.n, Lc.n), mg_block(), 0, c->st>>>(Lc.phi, Lc.phi0, Lc.n);
+    }
+    {
+        Launch L_(c, KC_TRANSFER, 16. * N + 8. * Nc3);
+        k_prolong_add<<<mg_grid(n, n), mg_block(), 0, c->st>>>(L.phi, Lc.phi0, nullptr, L.gam, n);
     }
     for (int s = 0; s < cf.mg_post; ++s)
         for (int color = 0; color < 2; ++color) {
@@ -710,8 +716,9 @@ void build_levels(kf_ctx *c) {
         if ((c->n >> l) < 2 || ((c->n >> (l - 1)) % 2))
             throw KfError{KF_ERR_ARG, "too many multigrid levels for this grid"};
     if (cf.poisson_mode == KF_PS_CASCADIC && c->n % 8) throw KfError{KF_ERR_ARG, "cascadic plan needs n % 8 == 0"};
-    if (cf.poisson_mode == KF_PS_FAS && ((long)(c->n >> (nl - 1)) * (c->n >> (nl - 1)) * (c->n >> (nl - 1)) > 64 * 1024))
-        throw KfError{KF_ERR_ARG, "coarsest FAS level above 40^3 points; add levels"};
+    if (cf.poisson_mode == KF_PS_FAS && ((long)(c->n >> (nl - 1)) * (c->n >> (nl - 1)) * (c->n >> (nl - 1)) > 8192))
+        throw KfError{KF_ERR_ARG, "coarsest FAS level above 8192 points (shared-memory solve); add levels"};
+    CK(cudaFuncSetAttribute(k_coarse_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     c->lv.resize(nl);
     for (int l = 0; l < nl; ++l) {
         LevelBuf &L = c->lv[l];

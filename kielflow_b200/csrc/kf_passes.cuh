@@ -18,7 +18,14 @@
 
 namespace kf {
 
-template <typename T> struct Tile { static constexpr int TC = sizeof(T) == 8 ? 8 : 16; };
+// Columns per x/y-pass tile: one 128-byte row segment per line by default.
+#ifndef KF_TC64
+#define KF_TC64 8
+#endif
+#ifndef KF_TC32
+#define KF_TC32 16
+#endif
+template <typename T> struct Tile { static constexpr int TC = sizeof(T) == 8 ? KF_TC64 : KF_TC32; };
 
 template <typename T2>
 __device__ __forceinline__ T2 mul_ik(T2 a, decltype(T2::x) k) {  // i k a

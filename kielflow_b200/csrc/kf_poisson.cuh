@@ -233,37 +233,46 @@ __global__ void __launch_bounds__(256) k_rbgs(double *__restrict__ phi, const do
     phi[q] = newton_step(phi[q], A, D);
 }
 
-// Coarsest-level solve in one block: red-black sweeps until max |f| <= tol.
+// Coarsest-level solve in one block: the level (phi, rho and the axis
+// tables) is staged in shared memory, red-black sweeps run until
+// max |f| <= tol (checked before every sweep, as the host loop of the oracle),
+// then phi is written back.  Dynamic shared memory: 16 n^3 + 24 n bytes.
 __global__ void __launch_bounds__(1024) k_coarse_solve(double *__restrict__ phi, const double *__restrict__ rho,
                                                        Lev L, double tol, int max_sweeps,
                                                        int *__restrict__ sweeps_out) {
+    extern __shared__ __align__(16) double cs_sm[];
     __shared__ double sh[32];
     const int n = L.n;
-    const long N = (long)n * n * n;
+    const int N = n * n * n;
+    double *sp = cs_sm, *sr = cs_sm + N, *sd = cs_sm + 2 * N, *si = sd + n, *sm_ = si + n;
+    for (int id = threadIdx.x; id < N; id += blockDim.x) {
+        sp[id] = phi[id];
+        sr[id] = rho[id];
+    }
+    for (int id = threadIdx.x; id < n; id += blockDim.x) {
+        sd[id] = L.dd[id];
+        si[id] = L.ip[id];
+        sm_[id] = L.im[id];
+    }
+    __syncthreads();
+    const Lev Ls{n, sd, nullptr, nullptr, si, sm_};
     int s = 0;
     for (;; ++s) {
         double m = 0.;
-        for (int id = threadIdx.x; id < (int)N; id += blockDim.x) {
+        for (int id = threadIdx.x; id < N; id += blockDim.x) {
             const int k = id % n;
             const int r = id / n;
             const int j = r % n, i = r / n;
             double A, D;
-            point_coeffs_fast(phi, rho, L, i, j, k, A, D);
-            const double af = fabs(f_point(A, D, phi[id]));
-            m = (af != af) ? af : fmax(m, af);
+            point_coeffs_fast(sp, sr, Ls, i, j, k, A, D);
+            m = nmax(m, fabs(f_point(A, D, sp[id])));
         }
-        for (int o = 16; o > 0; o >>= 1) {
-            double t = __shfl_xor_sync(0xffffffffu, m, o);
-            m = (t != t) ? t : fmax(m, t);
-        }
+        for (int o = 16; o > 0; o >>= 1) m = nmax(m, __shfl_xor_sync(0xffffffffu, m, o));
         if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = m;
         __syncthreads();
         if (threadIdx.x < 32) {
             double t = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.;
-            for (int o = 16; o > 0; o >>= 1) {
-                double u = __shfl_xor_sync(0xffffffffu, t, o);
-                t = (u != u) ? u : fmax(t, u);
-            }
+            for (int o = 16; o > 0; o >>= 1) t = nmax(t, __shfl_xor_sync(0xffffffffu, t, o));
             if (threadIdx.x == 0) sh[0] = t;
         }
         __syncthreads();
@@ -271,22 +280,31 @@ __global__ void __launch_bounds__(1024) k_coarse_solve(double *__restrict__ phi,
         __syncthreads();
         if (!(res > tol) || s >= max_sweeps) break;  // converged, NaN or capped
         for (int color = 0; color < 2; ++color) {
-            const int M = (int)(N / 2);
+            const int M = N / 2, nh = n / 2;
             for (int id = threadIdx.x; id < M; id += blockDim.x) {
-                const int nh = n / 2;
                 const int k2 = id % nh;
                 const int r = id / nh;
                 const int j = r % n, i = r / n;
                 const int k = 2 * k2 + ((i + j + color) & 1);
                 double A, D;
-                point_coeffs_fast(phi, rho, L, i, j, k, A, D);
-                const long q = lidx(i, j, k, n);
-                phi[q] = newton_step(phi[q], A, D);
+                point_coeffs_fast(sp, sr, Ls, i, j, k, A, D);
+                const int q = (int)lidx(i, j, k, n);
+                sp[q] = newton_step(sp[q], A, D);
             }
             __syncthreads();
         }
     }
+    for (int id = threadIdx.x; id < N; id += blockDim.x) phi[id] = sp[id];
     if (threadIdx.x == 0) *sweeps_out = s;
+}
+
+// e = phic - phic0 on the coarse level (the correction the prolongation carries)
+__global__ void __launch_bounds__(256) k_correction(const double *__restrict__ phic, double *__restrict__ phic0,
+                                                    int nc) {
+    const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, i = blockIdx.z;
+    if (k >= nc || j >= nc) return;
+    const long q = lidx(i, j, k, nc);
+    phic0[q] = __dsub_rn(phic[q], phic0[q]);
 }
 
 // Full-weighting restriction of r (fine n) and injection of phi:
