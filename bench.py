@@ -241,8 +241,6 @@ def run_kf(args):
         barrier()
         torch.cuda.synchronize()
         sampler = ClockSampler(torch.cuda.current_device()) if clocks else None
-        if profile:
-            ctx.profile(True)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         l0 = ctx.launch_count()
         with torch.cuda.stream(stream):
@@ -253,11 +251,16 @@ def run_kf(args):
         torch.cuda.synchronize()
         barrier()
         launches = ctx.launch_count() - l0
-        prof = ctx.profile_read() if profile else None
-        if profile:
-            ctx.profile(False)
         clk = sampler.stop() if sampler else None
         ms = max_over_ranks(e0.elapsed_time(e1))
+        prof = None
+        if profile:
+            # per-kernel CUDA-event profile of further steps of the same run
+            # (kernels launched one by one, each bracketed by events)
+            ctx.profile(True)
+            ctx.rk4(dt, max(1, min(args.steps, 3)))
+            prof = ctx.profile_read()
+            ctx.profile(False)
         d = ctx.diag()
         phi = ctx.get_phi()
         return ctx, ms, launches, prof, clk, d, phi

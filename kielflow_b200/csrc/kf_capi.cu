@@ -97,6 +97,9 @@ struct kf_ctx {
     long long prof_n[16] = {};
     std::vector<AxisJob> hj;
     std::vector<ZJob> hz;
+    // the FAS V-cycle captured once as a CUDA graph (replayed every cycle)
+    cudaGraphExec_t vgraph = nullptr;
+    long long vgraph_kernels = 0;
     // per-(precision, n) entry points
     void (*rhs_fn)(kf_ctx *) = nullptr;
     void (*r2c_fn)(kf_ctx *) = nullptr;
@@ -314,6 +317,30 @@ void vcycle(kf_ctx *c, int l) {
     CK(cudaGetLastError());
 }
 
+// One FAS V-cycle on the finest level: replayed from a CUDA graph captured on
+// first use (one launch instead of ~70), or launched kernel by kernel while
+// the per-launch profile is on.
+void run_vcycle(kf_ctx *c) {
+    if (c->prof) {
+        vcycle(c, 0);
+        return;
+    }
+    if (!c->vgraph) {
+        const long long l0 = c->launches;
+        CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+        vcycle(c, 0);
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamEndCapture(c->st, &g));
+        cudaError_t e = cudaGraphInstantiate(&c->vgraph, g, 0);
+        cudaGraphDestroy(g);
+        CK(e);
+        c->vgraph_kernels = c->launches - l0;
+        c->launches = l0;
+    }
+    CK(cudaGraphLaunch(c->vgraph, c->st));
+    c->launches += c->vgraph_kernels;
+}
+
 // Poisson solve on c->phi with source c->rho.  Returns KF_OK or KF_ERR_NOT_CONVERGED.
 int poisson(kf_ctx *c) {
     const kf_config &cf = c->cfg;
@@ -363,7 +390,7 @@ int poisson(kf_ctx *c) {
         double r = max_residual(c, L0, c->phi, c->rho, true);
         int cyc = 0;
         while (r > cf.res_tol && cyc < cf.max_cycles) {
-            vcycle(c, 0);
+            run_vcycle(c);
             ++cyc;
             r = max_residual(c, L0, c->phi, c->rho, true);
         }
@@ -402,7 +429,7 @@ template <typename T, int N> struct Impl {
     typedef typename C2<T>::type T2;
     static constexpr int TC = Tile<T>::TC, P = Plan<N>::P, LZ = ZTile<T>::LZ, NZC = N / 2 + 1;
 
-    static Geo<T> geo(kf_ctx *c) { return Geo<T>{c->n, c->nzc, (const T *)c->kv, c->q2}; }
+    static Geo<T> geo(kf_ctx *c) { return Geo<T>{c->n, c->nzc, (const T *)c->kv, c->q2, dealias_threshold()}; }
 
     static void set_attrs() {
         static bool done = false;
@@ -454,7 +481,8 @@ template <typename T, int N> struct Impl {
     static void zc2r(kf_ctx *c, int off, int njobs) {
         const int nrows = N * N;
         const int ntiles = (nrows + LZ - 1) / LZ;
-        const size_t smem = (size_t)(2 * LZ * NZC + LZ * PadLen<N>::value) * sizeof(T2);
+        const size_t smem = (size_t)(2 * LZ * NZC > LZ * PadLen<N>::value ? 2 * LZ * NZC : LZ * PadLen<N>::value) *
+                            sizeof(T2);
         Launch L_(c, KC_Z_C2R, z_bytes(c, off, njobs, true));
         k_z_c2r<T, N><<<njobs * ntiles, LZ * P, smem, c->st>>>(c->dz + off, njobs, nrows, geo(c), (const T2 *)c->tw,
                                                              (T)(1. / ((double)N * N * N)));
@@ -999,6 +1027,7 @@ int kf_ctx_destroy(kf_ctx *c) {
         cudaEventDestroy(r.b);
     }
     for (auto e : c->evfree) cudaEventDestroy(e);
+    if (c->vgraph) cudaGraphExecDestroy(c->vgraph);
     for (void *p : c->allocs) cudaFree(p);
     if (c->h_red) cudaFreeHost(c->h_red);
     if (c->h_max) cudaFreeHost(c->h_max);

@@ -223,6 +223,10 @@ template <> struct Plan<32> { static constexpr int P = 4; template <typename T2,
 template <> struct Plan<64> { static constexpr int P = 8; template <typename T2, int S, typename A> __device__ static void fft(T2 *v, T2 *sm, A a, int p, const T2 *tw) { fft_line<T2, 64, 8, S, 8, 8>(v, sm, a, p, tw); } static constexpr int R1 = 8, RL = 8; };
 template <> struct Plan<96> { static constexpr int P = 8; template <typename T2, int S, typename A> __device__ static void fft(T2 *v, T2 *sm, A a, int p, const T2 *tw) { fft_line<T2, 96, 8, S, 6, 4, 4>(v, sm, a, p, tw); } static constexpr int R1 = 6, RL = 4; };
 template <> struct Plan<128> { static constexpr int P = 8; template <typename T2, int S, typename A> __device__ static void fft(T2 *v, T2 *sm, A a, int p, const T2 *tw) { fft_line<T2, 128, 8, S, 16, 8>(v, sm, a, p, tw); } static constexpr int R1 = 16, RL = 8; };
+#ifdef KF_PLAN256_P32
+template <> struct Plan<256> { static constexpr int P = 32; template <typename T2, int S, typename A> __device__ static void fft(T2 *v, T2 *sm, A a, int p, const T2 *tw) { fft_line<T2, 256, 32, S, 8, 8, 4>(v, sm, a, p, tw); } static constexpr int R1 = 8, RL = 4; };
+#else
 template <> struct Plan<256> { static constexpr int P = 16; template <typename T2, int S, typename A> __device__ static void fft(T2 *v, T2 *sm, A a, int p, const T2 *tw) { fft_line<T2, 256, 16, S, 16, 16>(v, sm, a, p, tw); } static constexpr int R1 = 16, RL = 16; };
+#endif
 
 }  // namespace kf

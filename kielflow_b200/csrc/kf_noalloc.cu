@@ -92,7 +92,7 @@ cudaError_t run(const double *in, double *out, unsigned char *scratch, cudaStrea
     const AxisJob *aj = reinterpret_cast<const AxisJob *>(scratch + KF_NOALLOC_JOB_OFF);
     const ZJob *zj = reinterpret_cast<const ZJob *>(scratch + KF_NOALLOC_JOB_OFF + 2 * sizeof(AxisJob));
     constexpr int NZC = N / 2 + 1, LZ = ZTile<double>::LZ, P = Plan<N>::P, TC = Tile<double>::TC;
-    const Geo<double> g{N, NZC, nullptr, nullptr};  // no multipliers: the axis tables are not read
+    const Geo<double> g{N, NZC, nullptr, nullptr, 0.};  // no multipliers: the axis tables are not read
     const int nrows = N * N;
     k_z_r2c<double, N><<<(nrows + LZ - 1) / LZ, LZ * P, (size_t)LZ * PadLen<N>::value * sizeof(double2), st>>>(
         zj, 1, nrows, tw);

@@ -76,7 +76,7 @@ k_axis_pass(const AxisJob *__restrict__ jobs, int njobs, int axis, Geo<T> g,
         const int row = reg_row<N, P, Plan<N>::R1>(p, q);
         T2 x = valid ? in[base + row * rstride] : mk<T2>((T)0, (T)0);
         if (J.mul == MUL_P || J.mul == MUL_P_IK) {
-            if (!dealias_keep(g.q2, row, jj, kk)) x = mk<T2>((T)0, (T)0);
+            if (!dealias_keep(g.q2, g.thr, row, jj, kk)) x = mk<T2>((T)0, (T)0);
         }
         if (J.mul == MUL_P_IK || J.mul == MUL_IK) x = mul_ik(x, g.kv[row]);
         v[q] = x;
@@ -107,8 +107,8 @@ k_z_c2r(const ZJob *__restrict__ jobs, int njobs, int nrows, Geo<T> g,
     constexpr int LZ = ZTile<T>::LZ, P = Plan<N>::P, E = N / P, NZC = N / 2 + 1;
     constexpr int LS = PadLen<N>::value;  // padded line of the exchange buffer
     extern __shared__ __align__(16) unsigned char kf_smem[];
-    T2 *half = reinterpret_cast<T2 *>(kf_smem);  // [2][LZ][NZC]
-    T2 *xch = half + 2 * LZ * NZC;               // [LZ][LS]
+    T2 *half = reinterpret_cast<T2 *>(kf_smem);  // [2][LZ][NZC], staging of the half spectra
+    T2 *xch = half;                              // [LZ][LS], reused by the transform once staged
     const int job = blockIdx.x % njobs, tile = blockIdx.x / njobs;
     const ZJob J = jobs[job];
     const int r0 = tile * LZ;
@@ -149,6 +149,7 @@ k_z_c2r(const ZJob *__restrict__ jobs, int njobs, int nrows, Geo<T> g,
         }
         v[q] = mk<T2>(a.x - b.y, a.y + b.x);  // A + iB
     }
+    __syncthreads();  // staging consumed: the exchange buffer may overwrite it
     Plan<N>::template fft<T2, +1>(v, xch + l * LS, PadAddr{}, p, tw);
     const int r = r0 + l;
     if (r < nrows) {
@@ -226,7 +227,7 @@ __device__ __forceinline__ typename C2<T>::type lin_term(const RhsArgs<T> &a, co
                                                          int i, int j, int k, long idx) {
     typedef typename C2<T>::type T2;
     const int Tm = a.terms;
-    const bool P = dealias_keep(g.q2, i, j, k);
+    const bool P = dealias_keep(g.q2, g.thr, i, j, k);
     const T kx = g.kv[i], ky = g.kv[j], kz = g.kv[k];
     const T sv = a.SV[idx];
     T2 fb;
@@ -329,7 +330,7 @@ k_xfwd_assemble(const AxisJob *__restrict__ jobs, Geo<T> g, RhsArgs<T> a,
                 T2 F = v[e];
                 T2 K;
                 if (pen) {
-                    K = dealias_keep(g.q2, i, jj, kk) ? F : mk<T2>((T)0, (T)0);
+                    K = dealias_keep(g.q2, g.thr, i, jj, kk) ? F : mk<T2>((T)0, (T)0);
                 } else {
                     T2 fb = lin_term(a, g, q, i, jj, kk, idx);
                     K = mk<T2>(-(fb.x + F.x), -(fb.y + F.y));

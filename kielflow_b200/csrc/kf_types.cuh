@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cmath>
+
 #include "kf_fft.cuh"
 
 namespace kf {
@@ -45,12 +47,23 @@ template <typename T> struct Geo {
     int n, nzc;
     const T *kv;       // k_val_at(i), i < n                        (axis_EqSt.cpp:57-61)
     const double *q2;  // pow(k_val_at(i)/k_val_at(n/2), 2.), i < n  (OP_dealiasing.hpp:24-28)
+    double thr;        // smallest double s with sqrt(s) >= 2/3 (see dealias_threshold)
 };
 
-// 2/3 rule of rhs_standard.cpp:22 on the exact |k~| of OP_dealiasing.hpp:28.
-__device__ __forceinline__ bool dealias_keep(const double *__restrict__ q2, int i, int j, int k) {
-    double s = __dadd_rn(__dadd_rn(q2[i], q2[j]), q2[k]);
-    return sqrt(s) < (2. / 3.);
+// sqrt is correctly rounded and monotone, so sqrt(s) < 2/3 holds exactly when
+// s < thr for the smallest double thr with sqrt(thr) >= 2/3: the 2/3 rule of
+// rhs_standard.cpp:22 on |k~| (OP_dealiasing.hpp:28) without a square root.
+inline double dealias_threshold() {
+    const double c = 2. / 3.;
+    double s = c * c;
+    while (!(std::sqrt(s) < c)) s = std::nextafter(s, 0.);
+    while (std::sqrt(s) < c) s = std::nextafter(s, 1.);
+    return s;
+}
+
+// 2/3 rule of rhs_standard.cpp:22 on the exact |k~|^2 = (q2[i] + q2[j]) + q2[k].
+__device__ __forceinline__ bool dealias_keep(const double *__restrict__ q2, double thr, int i, int j, int k) {
+    return __dadd_rn(__dadd_rn(q2[i], q2[j]), q2[k]) < thr;
 }
 
 // Everything the spectral linear terms and the assembly need.

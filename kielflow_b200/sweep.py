@@ -40,3 +40,69 @@ def workload_of(inst: Instance) -> dict:
     w = dict(C.WORKLOADS["fp32bulk256"])
     w.update(n=inst.n, M=inst.M, tau=inst.tau, Q=inst.Q, sigma=0.5)
     return w
+
+
+def run_sweep(instances, steps: int, concurrent: bool = True, precision=None, max_threads: int = 64):
+    """Advance every instance `steps` RK4 steps on the current GPU.
+
+    Each instance is its own context (device memory, tables, CUDA stream).
+    concurrent=True drives all contexts from a pool of host threads (the C
+    calls release the GIL), so that their kernels overlap on the GPU; False
+    runs them one after another (the sequential baseline).  Returns
+    (wall seconds, [final state per instance], [diag per instance]).
+    """
+    import threading
+    import time
+
+    from ._lib import Context
+
+    ctxs, dts = [], []
+    for inst in instances:
+        w = workload_of(inst)
+        st, nd, mask, dt = C.make_inputs(w, seed=inst.seed)
+        ctx = Context(C.config_for(w, precision=precision))
+        ctx.set_state(*st)
+        ctx.set_sources(nd, mask)
+        ctxs.append(ctx)
+        dts.append(dt)
+    for ctx in ctxs:
+        ctx.synchronize()
+    errors = []
+
+    def work(i):
+        try:
+            ctxs[i].rk4(dts[i], steps)
+            ctxs[i].synchronize()
+        except Exception as e:  # surfaced after the join
+            errors.append((i, e))
+
+    t0 = time.perf_counter()
+    if concurrent:
+        nthreads = min(max_threads, len(ctxs))
+        pending = list(range(len(ctxs)))
+        lock = threading.Lock()
+
+        def runner():
+            while True:
+                with lock:
+                    if not pending:
+                        return
+                    i = pending.pop(0)
+                work(i)
+
+        threads = [threading.Thread(target=runner) for _ in range(nthreads)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+    else:
+        for i in range(len(ctxs)):
+            work(i)
+    wall = time.perf_counter() - t0
+    if errors:
+        raise errors[0][1]
+    states = [ctx.get_state() for ctx in ctxs]
+    diags = [ctx.diag() for ctx in ctxs]
+    for ctx in ctxs:
+        ctx.close()
+    return wall, states, diags
