@@ -108,14 +108,20 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(kernel: str, workload: str):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary, or None."""
+def ncu_traffic(kernel: str, workload: str, alg_bytes_per_launch: float):
+    """DRAM bytes per launch of `kernel`: the ratio DRAM bytes / algorithmic
+    bytes of one ncu capture of that kernel on this workload (profiles/
+    ncu_traffic.json), applied to the average algorithmic bytes of its launches
+    here (the capture is one launch of the finest level; the ratio carries to
+    the others).  None when no capture exists."""
     p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if not os.path.exists(p):
         return None
-    d = json.load(open(p))
-    v = d.get(workload, {}).get(kernel)
-    return None if v is None else float(v)
+    d = json.load(open(p)).get(workload, {})
+    v = d.get(kernel.split("(")[0].split("/")[0])
+    if not v or not v.get("traffic_over_alg"):
+        return None
+    return float(v["traffic_over_alg"]) * alg_bytes_per_launch
 
 
 # --------------------------------------------------------------------- CPU leg
@@ -314,7 +320,7 @@ def run_kf(args):
     dom, (dms, dn, dbytes) = max(prof.items(), key=lambda kv: kv[1][0])
     avg_ms = dms / dn
     achieved = (dbytes / dn) / (avg_ms / 1000.0) / 1e9
-    traffic = ncu_traffic(dom, args.workload)
+    traffic = ncu_traffic(dom, args.workload, dbytes / dn)
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                 "traffic": traffic, "alg_bytes_per_launch": dbytes / dn, "avg_launch_ms": avg_ms,
@@ -353,10 +359,52 @@ def run_kf(args):
     return 0
 
 
+def run_sweep_bench(args):
+    """The 48-instance sweep (16 each at 64^3, 96^3, 128^3): instance-steps/s
+    with all of a rank's instances driven concurrently, and the same instances
+    one after another.  Instances are partitioned across ranks by cost."""
+    import torch
+
+    from kielflow_b200 import dist as kdist
+    from kielflow_b200.sweep import run_sweep, sweep_instances
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+    torch.cuda.set_device(local)
+    inst = sweep_instances(seed=0)
+    mine = [inst[i] for i in kdist.partition([x.n for x in inst], ws)[rank]]
+    run_sweep(mine[:3], steps=1, concurrent=True)  # warm-up (module load, graph capture paths)
+    if ws > 1:
+        torch.distributed.barrier()
+    wall_c, _, dg = run_sweep(mine, steps=args.steps, concurrent=True)
+    wall_c = kdist.max_over_ranks(wall_c, device="cuda")
+    wall_s = None
+    if not args.no_fp64:  # the sequential reference run (skipped with --no-fp64 to save time)
+        wall_s, _, _ = run_sweep(mine, steps=args.steps, concurrent=False)
+        wall_s = kdist.max_over_ranks(wall_s, device="cuda")
+    if rank == 0:
+        total = len(inst) * args.steps
+        out = {"metric": "sweep instance-steps/s (48 instances, 64^3/96^3/128^3, FP32 bulk)",
+               "value": total / wall_c, "unit": "instance-steps/s", "n_gpus": ws, "steps": args.steps,
+               "warmup": 1, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+               "dtype": "fp32 bulk + fp64 Poisson", "data": "synthetic",
+               "config": {"workload": "sweep48", "timing": "host wall clock around fully synchronised runs"},
+               "sequential_value": (total / wall_s) if wall_s else None,
+               "batched_over_sequential": (wall_s / wall_c) if wall_s else None}
+        print(json.dumps(out))
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "sweep48":
+        return run_sweep_bench(args)
     return run_kf(args)
 
 

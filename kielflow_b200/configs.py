@@ -45,8 +45,17 @@ def config_for(w: dict, n: int | None = None, precision: int | None = None, **ov
     """kf_config of a workload dict (optionally on another grid size)."""
     n = n or w["n"]
     terms = KF_T_ALL if w["sv"] else (KF_T_ALL & ~KF_T_SVISCOSITY)
-    # multigrid levels: 4 at 128^3 (the stated plan), coarsest 8^3 at 256^3, else 16^3-ish
-    levels = 4 if n == 128 else (6 if n == 256 else max(1, int(math.log2(n)) - 3))
+    # multigrid levels: 4 at 128^3 (the stated plan), coarsest 8^3 at 256^3,
+    # otherwise halve while even until the coarsest level is at most 16^3
+    if n == 128:
+        levels = 4
+    elif n == 256:
+        levels = 6
+    else:
+        levels, m = 1, n
+        while m > 16 and m % 2 == 0:
+            m //= 2
+            levels += 1
     kw = dict(tau=w["tau"], theta=THETA, diff_D=DIFF_D, sv_eps=0.5, sv_cut=0.6 if w["sv"] else 0.0,
               pen_eta=PEN_ETA, terms=terms, poisson_mode=w["poisson_mode"], nlj_max_it=100000,
               nlj_limit=0.5e-5, res_tol=1e-10, mg_levels=levels, mg_pre=2, mg_post=2, coarse_tol=1e-13,

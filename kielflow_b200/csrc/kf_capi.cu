@@ -204,10 +204,12 @@ double max_residual(kf_ctx *c, const LevelBuf &L, const double *phi, const doubl
     CK(cudaMemsetAsync(c->d_max, 0, 64 * sizeof(unsigned long long), c->st));
     {
         Launch L_(c, KC_RESID, 16. * N);
+        dim3 g = mg_grid(L.n, L.n);
+        g.z = L.n < 16 ? L.n : 16;  // each block strides over the i-planes
         if (fast)
-            k_resmax<true><<<mg_grid(L.n, L.n), mg_block(), 0, c->st>>>(phi, rho, L.lev(), c->d_max);
+            k_resmax<true><<<g, mg_block(), 0, c->st>>>(phi, rho, L.lev(), c->d_max);
         else
-            k_resmax<false><<<mg_grid(L.n, L.n), mg_block(), 0, c->st>>>(phi, rho, L.lev(), c->d_max);
+            k_resmax<false><<<g, mg_block(), 0, c->st>>>(phi, rho, L.lev(), c->d_max);
     }
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(c->h_max, c->d_max, 64 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->st));
@@ -307,7 +309,7 @@ void vcycle(kf_ctx *c, int l) {
     }
     {
         Launch L_(c, KC_TRANSFER, 16. * N + 8. * Nc3);
-        k_prolong_add<<<mg_grid(n, n), mg_block(), 0, c->st>>>(L.phi, Lc.phi0, nullptr, L.gam, n);
+        k_prolong_add<<<mg_grid(Lc.n, Lc.n), mg_block(), 0, c->st>>>(L.phi, Lc.phi0, nullptr, L.gam, n);
     }
     for (int s = 0; s < cf.mg_post; ++s)
         for (int color = 0; color < 2; ++color) {

@@ -186,19 +186,23 @@ __global__ void __launch_bounds__(256) k_residual(const double *__restrict__ phi
     r[id] = f_point(A, D, phi[id]);
 }
 
-// max |f(phi)| over the level: block maximum, then an atomic max on the IEEE
-// bit pattern (order-free; NaN sorts above +inf) into one of 64 slots.
+// max |f(phi)| over the level: each block covers a (32 x 8) tile of (k, j) for
+// the i-planes blockIdx.z, blockIdx.z + gridDim.z, ...; block maximum, then an
+// atomic max on the IEEE bit pattern (order-free; NaN sorts above +inf) into
+// one of 64 slots.
 template <bool FAST>
 __global__ void __launch_bounds__(256) k_resmax(const double *__restrict__ phi, const double *__restrict__ rho,
                                                 Lev L, unsigned long long *__restrict__ out) {
     __shared__ double sh[8];
     const int n = L.n;
-    const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, i = blockIdx.z;
+    const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y;
     double af = 0.;
     if (k < n && j < n) {
-        double A, D;
-        coeffs_t<FAST>(phi, rho, L, i, j, k, A, D);
-        af = fabs(f_point(A, D, phi[lidx(i, j, k, n)]));
+        for (int i = blockIdx.z; i < n; i += gridDim.z) {
+            double A, D;
+            coeffs_t<FAST>(phi, rho, L, i, j, k, A, D);
+            af = nmax(af, fabs(f_point(A, D, phi[lidx(i, j, k, n)])));
+        }
     }
     for (int o = 16; o > 0; o >>= 1) af = nmax(af, __shfl_xor_sync(0xffffffffu, af, o));
     if (threadIdx.x == 0) sh[threadIdx.y] = af;
@@ -206,7 +210,8 @@ __global__ void __launch_bounds__(256) k_resmax(const double *__restrict__ phi, 
     if (threadIdx.y == 0 && threadIdx.x == 0) {
         double m = sh[0];
         for (int w = 1; w < 8; ++w) m = nmax(m, sh[w]);
-        atomicMax(out + (blockIdx.z & 63), (unsigned long long)__double_as_longlong(m));
+        atomicMax(out + ((blockIdx.x + blockIdx.y * gridDim.x + blockIdx.z) & 63),
+                  (unsigned long long)__double_as_longlong(m));
     }
 }
 
@@ -371,21 +376,58 @@ __device__ __forceinline__ double py(const double *pc, const double *pc0, const 
     return __dadd_rn(__dmul_rn(1. - g, pz(pc, pc0, gam, nf, i, j - 1, k)),
                      __dmul_rn(g, pz(pc, pc0, gam, nf, i, (j + 1) % nf, k)));
 }
-__global__ void __launch_bounds__(256) k_prolong_add(double *__restrict__ phi, const double *__restrict__ pc,
-                                                     const double *__restrict__ pc0, const double *__restrict__ gam,
-                                                     int nf) {
-    const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, i = blockIdx.z;
-    if (k >= nf || j >= nf) return;
-    const long id = lidx(i, j, k, nf);
-    double e;
-    if ((i & 1) == 0) {
-        e = py(pc, pc0, gam, nf, i, j, k);
-    } else {
-        const double g = gam[i];
-        e = __dadd_rn(__dmul_rn(1. - g, py(pc, pc0, gam, nf, i - 1, j, k)),
-                      __dmul_rn(g, py(pc, pc0, gam, nf, (i + 1) % nf, j, k)));
-    }
-    phi[id] = __dadd_rn(phi[id], e);
+// One thread per coarse cell (I, J, K): the 8 fine points (2I+a, 2J+b, 2K+c)
+// from the 8 corner values, with OP_hto2h's z, y, x passes and gammas (the
+// same operations per fine point as interpolating the whole field pass by pass).
+__global__ void __launch_bounds__(256) k_prolong_add(double *__restrict__ phi, const double *__restrict__ e,
+                                                     const double *__restrict__ unused,
+                                                     const double *__restrict__ gam, int nf) {
+    (void)unused;
+    const int nc = nf / 2;
+    const int K = blockIdx.x * 32 + threadIdx.x, J = blockIdx.y * 8 + threadIdx.y, I = blockIdx.z;
+    if (K >= nc || J >= nc) return;
+    const int I1 = I + 1 == nc ? 0 : I + 1, J1 = J + 1 == nc ? 0 : J + 1, K1 = K + 1 == nc ? 0 : K + 1;
+    // corner values e[I+di][J+dj][K+dk]
+    double c[2][2][2];
+    c[0][0][0] = e[lidx(I, J, K, nc)];
+    c[0][0][1] = e[lidx(I, J, K1, nc)];
+    c[0][1][0] = e[lidx(I, J1, K, nc)];
+    c[0][1][1] = e[lidx(I, J1, K1, nc)];
+    c[1][0][0] = e[lidx(I1, J, K, nc)];
+    c[1][0][1] = e[lidx(I1, J, K1, nc)];
+    c[1][1][0] = e[lidx(I1, J1, K, nc)];
+    c[1][1][1] = e[lidx(I1, J1, K1, nc)];
+    const double gz = gam[2 * K + 1], gy = gam[2 * J + 1], gx = gam[2 * I + 1];
+    // z pass on the even (i, j) columns: zc[di][dj][c] for fine k = 2K + c
+    double zc[2][2][2];
+#pragma unroll
+    for (int di = 0; di < 2; ++di)
+#pragma unroll
+        for (int dj = 0; dj < 2; ++dj) {
+            zc[di][dj][0] = c[di][dj][0];
+            zc[di][dj][1] = __dadd_rn(__dmul_rn(1. - gz, c[di][dj][0]), __dmul_rn(gz, c[di][dj][1]));
+        }
+    // y pass on the even i planes: yc[di][b][c] for fine j = 2J + b
+    double yc[2][2][2];
+#pragma unroll
+    for (int di = 0; di < 2; ++di)
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc) {
+            yc[di][0][cc] = zc[di][0][cc];
+            yc[di][1][cc] = __dadd_rn(__dmul_rn(1. - gy, zc[di][0][cc]), __dmul_rn(gy, zc[di][1][cc]));
+        }
+    // x pass and the update of the 8 fine points
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) {
+                const double v = a == 0 ? yc[0][b][cc]
+                                        : __dadd_rn(__dmul_rn(1. - gx, yc[0][b][cc]), __dmul_rn(gx, yc[1][b][cc]));
+                const long q = lidx(2 * I + a, 2 * J + b, 2 * K + cc, nf);
+                phi[q] = __dadd_rn(phi[q], v);
+            }
 }
 
 // Strided injection (OP_2htoh_lvl0 / OP_4htoh / OP_8htoh)
