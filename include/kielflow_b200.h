@@ -70,7 +70,10 @@ typedef struct {
     int poisson_mode;  /* KF_PS_*                                                    */
     int nlj_max_it;    /* Jacobi sweep cap (negative: 1000, as the reference)        */
     double nlj_limit;  /* relative-update limit (KF_PS_JACOBI_REF)                   */
-    double res_tol;    /* max-norm residual target (KF_PS_JACOBI_RES, KF_PS_FAS)     */
+    double res_tol;    /* max-norm residual target (KF_PS_JACOBI_RES, KF_PS_FAS);     */
+                       /* KF_PS_FAS with res_tol <= 0: exactly max_cycles V-cycles  */
+                       /* per solve (a smooth map of the inputs, for derivative     */
+                       /* checks by finite differences)                             */
     int mg_levels;     /* FAS levels, finest n ... coarsest n >> (levels-1)          */
     int mg_pre;        /* FAS pre-smoothing sweeps                                   */
     int mg_post;       /* FAS post-smoothing sweeps                                  */
@@ -143,10 +146,46 @@ long long kf_launch_count(const kf_ctx *ctx);
 /* Kernel profile: when enabled, every launch is bracketed by CUDA events on the
  * context's stream and its algorithmic bytes (distinct inputs + outputs) are
  * recorded per kernel class; enabling or disabling resets the totals.
- * Classes 0..15; kf_profile_class_name gives the kernel name of each. */
+ * Classes 0..17; kf_profile_class_name gives the kernel name of each. */
 int kf_profile_enable(kf_ctx *ctx, int on);
 int kf_profile_read(kf_ctx *ctx, int cls, double *ms, long long *launches, double *bytes);
 const char *kf_profile_class_name(int cls);
+
+/* ------------------------------------------------------------------ adjoint
+ * kf_adjoint_run -- no counterpart in the reference (the reference has no
+ * differentiation).  Gradients of the wake-potential functional
+ *     J = h^3 sum_x w(x) phi_T(x),   phi_T = Poisson solution of the state
+ *                                            after nsteps RK4 steps of size dt
+ * by the discrete adjoint of the FP64 time step: the transpose of every
+ * transform, product and linear term of the right-hand side, the adjoint of the
+ * converged Poisson solve  (-lap_h + diag e^phi) rho_bar = phi_bar  by linear
+ * multigrid, and the reverse RK4 recursion, with the forward states recomputed
+ * from checkpoints stored every ckpt_every steps.  Starts from the context's
+ * state, phi (the first solve's initial guess) and time; dt is held fixed.
+ * Requires a KF_FP64 context in KF_PS_FAS mode with KF_T_POISSON and
+ * KF_T_E_INT.  w: n^3 host doubles.  dJ_dn0 (n^3, may be NULL) receives the
+ * gradient with respect to the initial density n0 where the state's s^ =
+ * r2c(ln n0); lam0 (8*Nc doubles = the 4 half spectra, may be NULL) receives
+ * the gradient with respect to the initial spectral state.  On return the
+ * context holds the final state, phi_T and time t + nsteps*dt. */
+#define KF_ADJ_STORE_PHI 1 /* keep phi of every stage from the forward pass: the */
+                           /* recomputation then solves no Poisson problem       */
+                           /* (4 n^3 doubles per step of extra device memory)    */
+#define KF_ADJ_J_ONLY 2    /* forward pass and J only (finite-difference checks) */
+typedef struct {
+    double J;
+    double dJ_dM;        /* Mach number (parameters::M)                          */
+    double dJ_dtau;      /* friction (parameters::tau)                           */
+    double dJ_dnd;       /* d/de J(n_d -> (1+e) n_d) at e = 0: Q dJ/dQ for a     */
+                         /* dust charge n_d proportional to Q                    */
+    double fwd_ms;       /* device time of the checkpointed forward pass + J     */
+    double bwd_ms;       /* device time of recomputation + adjoint sweep         */
+    long long adj_cycles;/* V-cycles of the linear adjoint Poisson solves        */
+    int adj_solves;
+    int checkpoints;
+} kf_grad_out;
+int kf_adjoint_run(kf_ctx *ctx, int nsteps, double dt, int ckpt_every, int flags, const double *w,
+                   kf_grad_out *out, double *dJ_dn0, double *lam0);
 
 /* kf_fft_r2c_noalloc -- no counterpart in the reference.  The forward 3-D
  * transform of kf_fft_r2c for callers that cannot let a library allocate

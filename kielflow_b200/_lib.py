@@ -67,6 +67,20 @@ class DiagOut(ctypes.Structure):
                 ("not_converged", ctypes.c_int), ("charge", ctypes.c_double), ("kinetic", ctypes.c_double)]
 
 
+class GradOut(ctypes.Structure):
+    """kf_grad_out (include/kielflow_b200.h)."""
+    _fields_ = [("J", ctypes.c_double), ("dJ_dM", ctypes.c_double), ("dJ_dtau", ctypes.c_double),
+                ("dJ_dnd", ctypes.c_double), ("fwd_ms", ctypes.c_double), ("bwd_ms", ctypes.c_double),
+                ("adj_cycles", ctypes.c_longlong), ("adj_solves", ctypes.c_int), ("checkpoints", ctypes.c_int)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+KF_ADJ_STORE_PHI = 1
+KF_ADJ_J_ONLY = 2
+
+
 def library_path() -> str:
     return os.environ.get("KIELFLOW_B200_LIB", os.path.join(PKG, "libkf.so"))
 
@@ -75,9 +89,9 @@ EXPORTS = [
     "kf_ctx_create", "kf_ctx_destroy", "kf_last_error", "kf_set_stream", "kf_synchronize", "kf_set_state",
     "kf_get_state", "kf_set_sources", "kf_set_phi", "kf_get_phi", "kf_rhs_eval", "kf_rk4_steps",
     "kf_poisson_solve", "kf_diag", "kf_fft_r2c", "kf_fft_c2r", "kf_state_device_ptrs", "kf_launch_count",
-    "kf_profile_enable", "kf_profile_read", "kf_profile_class_name", "kf_fft_r2c_noalloc",
+    "kf_profile_enable", "kf_profile_read", "kf_profile_class_name", "kf_fft_r2c_noalloc", "kf_adjoint_run",
 ]
-KCLASSES = 16
+KCLASSES = 18
 
 _lib = None
 
@@ -118,6 +132,8 @@ def load_library():
     L.kf_profile_class_name.argtypes = [ctypes.c_int]
     L.kf_profile_class_name.restype = ctypes.c_char_p
     L.kf_fft_r2c_noalloc.argtypes = [ctypes.c_int, vp, vp, vp]
+    L.kf_adjoint_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, _D,
+                                 ctypes.POINTER(GradOut), _D, _D]
     _lib = L
     return L
 
@@ -204,6 +220,24 @@ class Context:
         rho = np.ascontiguousarray(rho, np.float64)
         self._check(self.L.kf_poisson_solve(self.h, _ptr(phi), _ptr(rho)))
         return phi
+
+    def adjoint(self, w, nsteps: int, dt: float, ckpt_every: int = 15, flags: int = 0,
+                want_dn0: bool = True, want_lam0: bool = False):
+        """kf_adjoint_run: J = h^3 sum w phi_T and its gradients (a dict; 'dn0' is
+        dJ/dn0 as an (n, n, n) array, 'lam0' the four spectral cotangents)."""
+        w = np.ascontiguousarray(w, np.float64)
+        if w.shape != self.shape_r:
+            raise ValueError(f"w must have shape {self.shape_r}")
+        g = GradOut()
+        dn0 = np.empty(self.shape_r, np.float64) if want_dn0 else None
+        lam0 = np.empty((4,) + self.shape_c, np.complex128) if want_lam0 else None
+        self._check(self.L.kf_adjoint_run(self.h, nsteps, dt, ckpt_every, flags, _ptr(w), ctypes.byref(g),
+                                          None if dn0 is None else _ptr(dn0),
+                                          None if lam0 is None else lam0.ctypes.data_as(_D)))
+        out = g.as_dict()
+        out["dn0"] = dn0
+        out["lam0"] = lam0
+        return out
 
     def diag(self) -> DiagOut:
         d = DiagOut()

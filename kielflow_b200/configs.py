@@ -64,6 +64,21 @@ def config_for(w: dict, n: int | None = None, precision: int | None = None, **ov
     return Config.make(n, L_BOX, w["M"], **kw)
 
 
+# objective of the adjoint workload: J = h^3 sum w phi_T with a Gaussian window
+# exp(-|x - x0|^2 / width^2) of width 2 centred 4 Debye lengths downstream
+# (+x, the direction of the mean flow M e_x) of the grain at the origin
+WAKE_X0 = (4.0, 0.0, 0.0)
+WAKE_WIDTH = 2.0
+
+
+def wake_window(n: int, L: float = L_BOX, x0=WAKE_X0, width: float = WAKE_WIDTH):
+    from . import inputs as I
+    x = I.axis_values(n, L)
+    r2 = ((x[:, None, None] - x0[0]) ** 2 + (x[None, :, None] - x0[1]) ** 2
+          + (x[None, None, :] - x0[2]) ** 2)
+    return __import__("numpy").exp(-r2 / (width * width))
+
+
 def make_inputs(w: dict, n: int | None = None, seed: int = 0):
     """(state, n_d, mask, dt) of a workload, from the seeded generator."""
     from . import inputs as I

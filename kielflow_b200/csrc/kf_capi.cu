@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/kielflow_b200.h"
+#include "kf_adjoint.cuh"
 #include "kf_passes.cuh"
 #include "kf_pointwise.cuh"
 #include "kf_poisson.cuh"
@@ -44,6 +45,8 @@ struct LevelBuf {
 };
 
 constexpr int RBS = 256;  // reduction block size
+
+struct AdjState;  // discrete-adjoint buffers (allocated by the first kf_adjoint_run)
 
 }  // namespace
 
@@ -93,8 +96,8 @@ struct kf_ctx {
     struct ProfRec { int cls; cudaEvent_t a, b; double bytes; };
     std::vector<ProfRec> recs;
     std::vector<cudaEvent_t> evfree;
-    double prof_ms[16] = {}, prof_bytes[16] = {};
-    long long prof_n[16] = {};
+    double prof_ms[32] = {}, prof_bytes[32] = {};
+    long long prof_n[32] = {};
     std::vector<AxisJob> hj;
     std::vector<ZJob> hz;
     // the FAS V-cycle captured once as a CUDA graph (replayed every cycle)
@@ -105,6 +108,13 @@ struct kf_ctx {
     void (*r2c_fn)(kf_ctx *) = nullptr;
     void (*c2r_fn)(kf_ctx *) = nullptr;
     void (*inv_state_fn)(kf_ctx *) = nullptr;
+    void (*adj_fn)(kf_ctx *, int) = nullptr;
+    // discrete adjoint: buffers, job-list offsets, and the "phi given" switch
+    // under which a right-hand side uses c->phi as it stands (no solve)
+    AdjState *adj = nullptr;
+    bool phi_given = false;
+    int jV_x = 0, jV_y = 0, zV = 0, zW = 0, nWz = 0, nWf = 0, jW_y = 0, jW_x = 0, zS = 0, jS_y = 0, jS_x = 0;
+    int jP_x = 0, jP_y = 0, zP = 0, jQ_x = 0, jQ_y = 0, zQ = 0;
 };
 
 namespace {
@@ -120,11 +130,14 @@ inline int nblk(long work, int bs) { return (int)((work + bs - 1) / bs); }
 
 // Kernel classes for the profile (kf_profile_read); names in kf_profile_class_name.
 enum KCls { KC_AXIS_INV, KC_AXIS_FWD, KC_Z_C2R, KC_Z_R2C, KC_XASM, KC_PROD, KC_LIN, KC_RHO, KC_RK,
-            KC_JACOBI, KC_RBGS, KC_RESID, KC_TRANSFER, KC_COARSE, KC_REDUCE, KC_MISC, KC_N };
+            KC_JACOBI, KC_RBGS, KC_RESID, KC_TRANSFER, KC_COARSE, KC_REDUCE, KC_MISC, KC_ADJ_PW, KC_ADJ_MG,
+            KC_N };
 const char *const kKClsName[KC_N] = {"k_axis_pass(inverse)", "k_axis_pass(forward)", "k_z_c2r", "k_z_r2c",
                                      "k_xfwd_assemble", "k_products", "k_lin", "k_rho", "k_rk", "k_jacobi",
                                      "k_rbgs", "k_residual", "k_restrict/k_fas_rhs/k_prolong/k_inject",
-                                     "k_coarse_solve", "k_reduce_final", "conversion/diagnostics"};
+                                     "k_coarse_solve", "k_reduce_final", "conversion/diagnostics",
+                                     "adjoint pointwise (k_prod_vjp/k_vjp_assemble/k_adj_stage/...)",
+                                     "adjoint Poisson (linear multigrid)"};
 
 void prof_flush(kf_ctx *c) {
     if (c->recs.empty()) return;
@@ -388,6 +401,15 @@ int poisson(kf_ctx *c) {
         }
         c->diag.last_residual = max_residual(c, L0, c->phi, c->rho, false);
         rc = 0;
+    } else if (!(cf.res_tol > 0.)) {
+        // fixed number of V-cycles: the result is a smooth function of rho
+        // and of the initial guess (no data-dependent stopping)
+        for (int cyc = 0; cyc < cf.max_cycles; ++cyc) run_vcycle(c);
+        const double r = max_residual(c, L0, c->phi, c->rho, true);
+        c->diag.last_iterations = cf.max_cycles;
+        c->diag.total_iterations += cf.max_cycles;
+        c->diag.last_residual = r;
+        if (r != r) throw KfError{KF_ERR_NAN, "NaN in the multigrid solve"};
     } else {
         double r = max_residual(c, L0, c->phi, c->rho, true);
         int cyc = 0;
@@ -480,14 +502,15 @@ template <typename T, int N> struct Impl {
         const double cb = (double)c->Nc * sizeof(T2), rb = (double)c->N * sizeof(T);
         return c2r ? u.size() * cb + outs * rb : u.size() * rb + outs * cb;
     }
-    static void zc2r(kf_ctx *c, int off, int njobs) {
+    // scale < 0: the 1/N of c2r; otherwise the given factor (1 for transposes)
+    static void zc2r(kf_ctx *c, int off, int njobs, double scale = -1.) {
         const int nrows = N * N;
         const int ntiles = (nrows + LZ - 1) / LZ;
         const size_t smem = (size_t)(2 * LZ * NZC > LZ * PadLen<N>::value ? 2 * LZ * NZC : LZ * PadLen<N>::value) *
                             sizeof(T2);
         Launch L_(c, KC_Z_C2R, z_bytes(c, off, njobs, true));
         k_z_c2r<T, N><<<njobs * ntiles, LZ * P, smem, c->st>>>(c->dz + off, njobs, nrows, geo(c), (const T2 *)c->tw,
-                                                             (T)(1. / ((double)N * N * N)));
+                                                             (T)(scale < 0. ? 1. / ((double)N * N * N) : scale));
     }
     static void zr2c(kf_ctx *c, int off, int njobs) {
         const int nrows = N * N;
@@ -519,7 +542,7 @@ template <typename T, int N> struct Impl {
         axis(c, c->jA_x, 2, 0, +1);
         axis(c, c->jA_y, 3, 1, +1);
         if (pois || pen) zc2r(c, c->zA, 1);
-        if (pois) {
+        if (pois && !c->phi_given) {
             {
                 Launch L_(c, KC_RHO, (double)c->N * (sizeof(T) + 16));
                 k_rho<T><<<nblk(c->N, 256), 256, 0, c->st>>>((const T *)c->R[0], c->nd, c->rho, c->N);
@@ -600,6 +623,51 @@ template <typename T, int N> struct Impl {
         zc2r(c, c->zT + 1, 1);
         CK(cudaGetLastError());
     }
+    // transform passes of the discrete adjoint (job lists of build_adj_jobs)
+    static void adj_pass(kf_ctx *c, int which) {
+        switch (which) {
+            case 0:  // forward intermediates s_d, U_c, d_d U_c, d_d s of the stage input in Ys
+                axis(c, c->jA_x, 2, 0, +1);
+                axis(c, c->jA_y, 3, 1, +1);
+                zc2r(c, c->zA, 1);
+                axis(c, c->jD_x, 6, 0, +1);
+                axis(c, c->jD_y, 9, 1, +1);
+                zc2r(c, c->zD, 8);
+                break;
+            case 1:  // f_bar = r2c^T(P Kbar) = c2r_unscaled(P Kbar / w)
+                axis(c, c->jV_x, 4, 0, +1);
+                axis(c, c->jV_y, 4, 1, +1);
+                zc2r(c, c->zV, 2, 1.);
+                break;
+            case 2:  // r2c of the physical cotangents
+                zr2c(c, c->zW, c->nWz);
+                axis(c, c->jW_y, c->nWf, 1, -1);
+                axis(c, c->jW_x, c->nWf, 0, -1);
+                break;
+            case 3:  // phi_bar = r2c^T(phihat_bar)
+                axis(c, c->jP_x, 1, 0, +1);
+                axis(c, c->jP_y, 1, 1, +1);
+                zc2r(c, c->zP, 1, 1.);
+                break;
+            case 4:  // r2c of s_d_bar
+                zr2c(c, c->zS, 1);
+                axis(c, c->jS_y, 1, 1, -1);
+                axis(c, c->jS_x, 1, 0, -1);
+                break;
+            case 5:  // r2c^T of the s cotangent, and c2r of the state's s
+                axis(c, c->jQ_x, 2, 0, +1);
+                axis(c, c->jQ_y, 2, 1, +1);
+                zc2r(c, c->zQ, 1, 1.);
+                zc2r(c, c->zQ + 1, 1);
+                break;
+            case 6:  // s_d only (the Poisson source of the state in Ys)
+                axis(c, c->jA_x, 2, 0, +1);
+                axis(c, c->jA_y, 3, 1, +1);
+                zc2r(c, c->zA, 1);
+                break;
+        }
+        CK(cudaGetLastError());
+    }
     // inverse transforms of the (undealiased) state into R[20..23] for diagnostics
     static void inv_state(kf_ctx *c) {
         axis(c, c->jG_x, 4, 0, +1);
@@ -619,6 +687,7 @@ template <typename T> struct Dispatch {
         c->r2c_fn = &Impl<T, NN>::r2c;                 \
         c->c2r_fn = &Impl<T, NN>::c2r;                 \
         c->inv_state_fn = &Impl<T, NN>::inv_state;     \
+        c->adj_fn = &Impl<T, NN>::adj_pass;            \
         return true;
             KF_CASE(16)
             KF_CASE(32)
@@ -981,6 +1050,31 @@ void rk_launch(kf_ctx *c, double cdt, int mode) {
     CK(cudaGetLastError());
 }
 
+// One RK4 step (RKO4.cpp:105-238) on Y (== Ys on entry).  Optional hooks of
+// the adjoint: X (16 buffers) receives the four stage inputs, PH (4) the four
+// stage potentials; with PHin the stage potentials are taken from there and
+// no Poisson problem is solved.
+void rk4_step(kf_ctx *c, double dt, void *const *X, double *const *PH, double *const *PHin) {
+    const double t0 = c->t;
+    const double ts[4] = {t0, t0 + 0.5 * dt, t0 + 0.5 * dt, t0 + 1.0 * dt};
+    const double cdt[4] = {0.5 * dt, 0.5 * dt, 1.0 * dt, dt / 6.};
+    const int mode[4] = {0, 1, 1, 2};
+    for (int i = 0; i < 4; ++i) {
+        c->t_stage = ts[i];
+        if (X) copy_state(c, X + 4 * i, c->Ys);
+        if (PHin) {
+            CK(cudaMemcpyAsync(c->phi, PHin[i], 8 * c->N, cudaMemcpyDeviceToDevice, c->st));
+            c->phi_given = true;
+        }
+        c->rhs_fn(c);
+        c->phi_given = false;
+        if (PH) CK(cudaMemcpyAsync(PH[i], c->phi, 8 * c->N, cudaMemcpyDeviceToDevice, c->st));
+        rk_launch(c, cdt[i], mode[i]);
+    }
+    copy_state(c, c->Ys, c->Y);
+    c->t = t0 + dt;
+}
+
 template <typename F> int guarded(kf_ctx *c, F f) {
     if (!c) return KF_ERR_ARG;
     try {
@@ -996,6 +1090,8 @@ template <typename F> int guarded(kf_ctx *c, F f) {
 }
 
 }  // namespace
+
+#include "kf_adjoint_host.cuh"
 
 // Message of the last failure that has no context (kf_ctx_create and the
 // context-free entry points); kf_last_error(NULL) returns it.
@@ -1030,6 +1126,7 @@ int kf_ctx_destroy(kf_ctx *c) {
     }
     for (auto e : c->evfree) cudaEventDestroy(e);
     if (c->vgraph) cudaGraphExecDestroy(c->vgraph);
+    adj_release(c);
     for (void *p : c->allocs) cudaFree(p);
     if (c->h_red) cudaFreeHost(c->h_red);
     if (c->h_max) cudaFreeHost(c->h_max);
@@ -1115,24 +1212,8 @@ int kf_rhs_eval(kf_ctx *c, double t) {
 int kf_rk4_steps(kf_ctx *c, int nsteps, double dt) {
     return guarded(c, [&] {
         if (nsteps < 0) throw KfError{KF_ERR_ARG, "nsteps < 0"};
-        for (int s = 0; s < nsteps; ++s) {
-            // Ys == Y on entry; stage times t, t + dt/2, t + dt/2, t + dt (RKO4.cpp:105-212)
-            const double t0 = c->t;
-            c->t_stage = t0;
-            c->rhs_fn(c);
-            rk_launch(c, 0.5 * dt, 0);
-            c->t_stage = t0 + 0.5 * dt;
-            c->rhs_fn(c);
-            rk_launch(c, 0.5 * dt, 1);
-            c->t_stage = t0 + 0.5 * dt;
-            c->rhs_fn(c);
-            rk_launch(c, 1.0 * dt, 1);
-            c->t_stage = t0 + 1.0 * dt;
-            c->rhs_fn(c);
-            rk_launch(c, dt / 6., 2);
-            copy_state(c, c->Ys, c->Y);
-            c->t = t0 + dt;
-        }
+        // Ys == Y on entry; stage times t, t + dt/2, t + dt/2, t + dt (RKO4.cpp:105-212)
+        for (int s = 0; s < nsteps; ++s) rk4_step(c, dt, nullptr, nullptr, nullptr);
         CK(cudaGetLastError());
     });
 }

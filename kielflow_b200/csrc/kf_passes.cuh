@@ -125,6 +125,7 @@ k_z_c2r(const ZJob *__restrict__ jobs, int njobs, int nrows, Geo<T> g,
         if (src && r < nrows) {
             x = src[(long)r * NZC + k];
             if (mul == MUL_IK) x = mul_ik(x, g.kv[k]);
+            if (mul == MUL_HALF && k > 0 && 2 * k < N) x = mk<T2>((T)0.5 * x.x, (T)0.5 * x.y);
         }
         if (k == 0 || 2 * k == N) x.y = (T)0;
         half[idx] = x;

@@ -16,6 +16,7 @@ enum Mul : int {
     MUL_P = 1,      // 2/3 dealiasing mask P(k)            (x pass only: needs i, j, k)
     MUL_P_IK = 2,   // P(k) * i k_axis                     (x pass only)
     MUL_IK = 3,     // i k_axis  (k of the pass's own axis)
+    MUL_HALF = 4,   // z c2r only: 1/2 for 0 < kz < n/2 (the half-spectrum weight of a transpose)
 };
 
 // Term bits (runtime form of rhs_standard.hpp:22-30 plus the added terms).
