@@ -340,22 +340,37 @@ __global__ void __launch_bounds__(256) k_fas_rhs_lin(const double *__restrict__ 
     rhoc[id] = __dadd_rn(Nc, rc[id]);
 }
 
-// Coarsest level of the linear solve in one block (global memory; the level
-// is small and stays in L2): red-black sweeps until the max residual has
-// dropped by rtol from its value at entry, or max_sweeps.
+// Coarsest level of the linear solve in one block, staged in shared memory
+// (psi, b, c and the axis tables: 24 n^3 + 24 n bytes): red-black sweeps
+// until the max residual has dropped by rtol from its value at entry
+// (checked every 4 sweeps), or max_sweeps.
 __global__ void __launch_bounds__(1024) k_coarse_solve_lin(double *__restrict__ phi, const double *__restrict__ rho,
                                                            const double *__restrict__ cl, Lev L, double rtol,
                                                            int max_sweeps) {
+    extern __shared__ __align__(16) double cl_sm[];
     __shared__ double sh[32];
     const int n = L.n, N = n * n * n;
+    double *sp = cl_sm, *sb = cl_sm + N, *sc = cl_sm + 2 * N, *sd = cl_sm + 3 * N, *si = sd + n, *sm_ = si + n;
+    for (int id = threadIdx.x; id < N; id += blockDim.x) {
+        sp[id] = phi[id];
+        sb[id] = rho[id];
+        sc[id] = cl[id];
+    }
+    for (int id = threadIdx.x; id < n; id += blockDim.x) {
+        sd[id] = L.dd[id];
+        si[id] = L.ip[id];
+        sm_[id] = L.im[id];
+    }
+    __syncthreads();
+    const Lev Ls{n, sd, nullptr, nullptr, si, sm_};
     double r0 = 0.;
-    for (int s = 0;; ++s) {
+    for (int s = 0;; s += 4) {
         double m = 0.;
         for (int id = threadIdx.x; id < N; id += blockDim.x) {
             const int k = id % n, r = id / n, j = r % n, i = r / n;
             double A, D;
-            point_coeffs_fast(phi, rho, L, i, j, k, A, D);
-            m = nmax(m, fabs(__dsub_rn(A, __dmul_rn(__dadd_rn(D, cl[id]), phi[id]))));
+            point_coeffs_fast(sp, sb, Ls, i, j, k, A, D);
+            m = nmax(m, fabs(__dsub_rn(A, __dmul_rn(__dadd_rn(D, sc[id]), sp[id]))));
         }
         for (int o = 16; o > 0; o >>= 1) m = nmax(m, __shfl_xor_sync(0xffffffffu, m, o));
         if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = m;
@@ -370,19 +385,47 @@ __global__ void __launch_bounds__(1024) k_coarse_solve_lin(double *__restrict__ 
         __syncthreads();
         if (s == 0) r0 = res;
         if (!(res > rtol * r0) || s >= max_sweeps) break;  // reached, zero, NaN or capped
-        for (int color = 0; color < 2; ++color) {
-            const int nh = n / 2;
-            for (int id = threadIdx.x; id < N / 2; id += blockDim.x) {
-                const int k2 = id % nh, r = id / nh, j = r % n, i = r / n;
-                const int k = 2 * k2 + ((i + j + color) & 1);
-                double A, D;
-                point_coeffs_fast(phi, rho, L, i, j, k, A, D);
-                const int q = (int)lidx(i, j, k, n);
-                phi[q] = A / __dadd_rn(D, cl[q]);
+        for (int sw = 0; sw < 4; ++sw)
+            for (int color = 0; color < 2; ++color) {
+                const int nh = n / 2;
+                for (int id = threadIdx.x; id < N / 2; id += blockDim.x) {
+                    const int k2 = id % nh, r = id / nh, j = r % n, i = r / n;
+                    const int k = 2 * k2 + ((i + j + color) & 1);
+                    double A, D;
+                    point_coeffs_fast(sp, sb, Ls, i, j, k, A, D);
+                    const int q = (int)lidx(i, j, k, n);
+                    sp[q] = A / __dadd_rn(D, sc[q]);
+                }
+                __syncthreads();
             }
-            __syncthreads();
-        }
     }
+    for (int id = threadIdx.x; id < N; id += blockDim.x) phi[id] = sp[id];
+}
+
+// Block sums of <b, bp> (slot 0) and <bp, bp> (slot 1): the least-squares
+// factor alpha = <b, bp> / <bp, bp> of the warm start alpha * psi_prev.
+template <int BS>
+__global__ void __launch_bounds__(BS) k_dot2(const double *__restrict__ b, const double *__restrict__ bp, long N,
+                                             double *__restrict__ part) {
+    __shared__ double sh[4 * BS];
+    double acc[4] = {0., 0., 0., 0.};
+    for (long i = (long)blockIdx.x * BS + threadIdx.x; i < N; i += (long)gridDim.x * BS) {
+        const double x = b[i], y = bp[i];
+        acc[0] += x * y;
+        acc[1] += y * y;
+    }
+    block_sum4<BS>(acc, sh, part);
+}
+
+// psi = alpha psi (alpha = sums[0] / sums[1], 0 when sums[1] == 0); bp = b
+__global__ void k_warm_scale(double *__restrict__ psi, double *__restrict__ bp, const double *__restrict__ b,
+                             const double *__restrict__ sums, long N) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const double den = sums[1];
+    const double alpha = den > 0. ? sums[0] / den : 0.;
+    psi[i] *= alpha;
+    bp[i] = b[i];
 }
 
 // max |x| over N values: block maxima, atomic max on the bit pattern (x >= 0)
