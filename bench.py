@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison arm")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--adjoint-steps", type=int, default=200,
+                    help="RK4 steps of the adjoint leg (128^3 FP64, checkpoints every 15); 0 skips it")
     return ap.parse_args()
 
 
@@ -209,6 +211,44 @@ def run_reference(args):
 
 
 # --------------------------------------------------------------------- GPU arm
+def adjoint_leg(nsteps: int, stream, ckpt_every: int = 15):
+    """Cost of the discrete adjoint against its forward pass on the
+    differentiation workload (128^3 FP64, M 0.9, nu 0.1, Q -20): device time
+    of nsteps RK4 steps + J alone, and of the full gradient run (checkpointed
+    forward pass, recomputation, reverse sweep), with and without the stored
+    stage potentials."""
+    import kielflow_b200 as kf
+    from kielflow_b200 import configs as C
+
+    w = C.WORKLOADS["adj128"]
+    st, nd, mask, dt = C.make_inputs(w)
+    win = C.wake_window(w["n"])
+    with kf.Context(C.config_for(w)) as ctx:
+        ctx.set_stream(stream.cuda_stream)
+        ctx.set_state(*st)
+        ctx.set_sources(nd, mask)
+        ctx.adjoint(win, 0, dt, 1, kf.KF_ADJ_J_ONLY, want_dn0=False)  # converged phi of the initial state
+        phi0 = ctx.get_phi()
+
+        def run(flags, steps):
+            ctx.set_state(*st)
+            ctx.set_phi(phi0)
+            return ctx.adjoint(win, steps, dt, ckpt_every, flags, want_dn0=False)
+
+        run(0, min(nsteps, 2 * ckpt_every))  # warm-up: buffers, graph capture
+        f = run(kf.KF_ADJ_J_ONLY, nsteps)
+        a = run(0, nsteps)
+        b = run(kf.KF_ADJ_STORE_PHI, nsteps)
+    tot_a, tot_b = a["fwd_ms"] + a["bwd_ms"], b["fwd_ms"] + b["bwd_ms"]
+    return {"workload": f"adj128: {w['n']}^3 FP64, M {w['M']}, nu {w['tau']}, Q {w['Q']}, {nsteps} RK4 steps, "
+                        f"checkpoints every {ckpt_every}; J = h^3 sum w phi_T, Gaussian window width 2 at (4,0,0)",
+            "J": a["J"], "dJ_dM": a["dJ_dM"], "dJ_dtau": a["dJ_dtau"], "dJ_dQ": a["dJ_dnd"] / w["Q"],
+            "forward_ms": f["fwd_ms"], "gradient_ms": tot_a, "adj_over_fwd": tot_a / f["fwd_ms"],
+            "gradient_ms_store_phi": tot_b, "adj_over_fwd_store_phi": tot_b / f["fwd_ms"],
+            "adjoint_poisson_solves": a["adj_solves"], "adjoint_v_cycles": a["adj_cycles"],
+            "timing": "CUDA events on the context's stream (kf_grad_out fwd_ms/bwd_ms)"}
+
+
 def run_kf(args):
     import numpy as np
     import torch
@@ -259,6 +299,8 @@ def run_kf(args):
         launches = ctx.launch_count() - l0
         clk = sampler.stop() if sampler else None
         ms = max_over_ranks(e0.elapsed_time(e1))
+        d = ctx.diag()
+        phi = ctx.get_phi()  # after warm-up + timed steps in both precisions
         prof = None
         if profile:
             # per-kernel CUDA-event profile of further steps of the same run
@@ -267,8 +309,6 @@ def run_kf(args):
             ctx.rk4(dt, max(1, min(args.steps, 3)))
             prof = ctx.profile_read()
             ctx.profile(False)
-        d = ctx.diag()
-        phi = ctx.get_phi()
         return ctx, ms, launches, prof, clk, d, phi
 
     ctx32, ms32, launches, prof, clk, d32, phi32 = timed_arm(w["precision"], profile=True, clocks=True)
@@ -308,6 +348,8 @@ def run_kf(args):
                 "phi_rel_err_fp32_vs_fp64": max_over_ranks(err),
                 "charge_fp32": d32.charge, "charge_fp64": d64.charge,
                 "kinetic_fp32": d32.kinetic, "kinetic_fp64": d64.kinetic}
+
+    adj = adjoint_leg(args.adjoint_steps, stream) if args.adjoint_steps > 0 else None
 
     if rank != 0:
         if ws > 1:
@@ -352,6 +394,7 @@ def run_kf(args):
         "poisson": {"solves": d32.solves, "v_cycles": d32.total_iterations,
                     "last_residual": d32.last_residual, "not_converged": d32.not_converged},
         "fp64": fp64,
+        "adjoint": adj,
     }
     print(json.dumps(out))
     if ws > 1:
