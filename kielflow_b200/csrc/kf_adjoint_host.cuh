@@ -246,11 +246,7 @@ void avcycle(kf_ctx *c, int l) {
                                                                         400);
         return;
     }
-    for (int s = 0; s < cf.mg_pre; ++s)
-        for (int color = 0; color < 2; ++color) {
-            Launch L_(c, KC_ADJ_MG, 24. * N);
-            k_rbgs_lin<<<mg_grid(n / 2, n), mg_block(), 0, c->st>>>(A.psi, A.b, A.cc, L.lev(), color);
-        }
+    smooth(c, L, A.psi, A.b, A.cc, cf.mg_pre, KC_ADJ_MG);
     {
         Launch L_(c, KC_ADJ_MG, 32. * N);
         k_residual_lin<<<mg_grid(n, n), mg_block(), 0, c->st>>>(A.psi, A.b, A.cc, L.lev(), A.r);
@@ -275,11 +271,7 @@ void avcycle(kf_ctx *c, int l) {
         Launch L_(c, KC_ADJ_MG, 16. * N + 8. * Nc3);
         k_prolong_add<<<mg_grid(Lc.n, Lc.n), mg_block(), 0, c->st>>>(A.psi, C.phi0, nullptr, L.gam, n);
     }
-    for (int s = 0; s < cf.mg_post; ++s)
-        for (int color = 0; color < 2; ++color) {
-            Launch L_(c, KC_ADJ_MG, 24. * N);
-            k_rbgs_lin<<<mg_grid(n / 2, n), mg_block(), 0, c->st>>>(A.psi, A.b, A.cc, L.lev(), color);
-        }
+    smooth(c, L, A.psi, A.b, A.cc, cf.mg_post, KC_ADJ_MG);
     CK(cudaGetLastError());
 }
 

@@ -284,6 +284,22 @@ int jacobi_solve(kf_ctx *c, const LevelBuf &L, double *phi, double *tmp, const d
     return converged ? 0 : 1;
 }
 
+// `sweeps` red-black Gauss-Seidel sweeps on level L (phi in place), two
+// half-sweep launches each.  cc: the adjoint's e^phi (linear point solve) or
+// nullptr (Newton step).
+void smooth(kf_ctx *c, LevelBuf &L, double *phi, const double *rho, const double *cc, int sweeps, int cls) {
+    const int n = L.n;
+    const long N = (long)n * n * n;
+    for (int s = 0; s < sweeps; ++s)
+        for (int color = 0; color < 2; ++color) {
+            Launch L_(c, cls, 16. * N);
+            if (cc)
+                k_rbgs_lin<<<mg_grid(n / 2, n), mg_block(), 0, c->st>>>(phi, rho, cc, L.lev(), color);
+            else
+                k_rbgs<<<mg_grid(n / 2, n), mg_block(), 0, c->st>>>(phi, rho, L.lev(), color);
+        }
+}
+
 void vcycle(kf_ctx *c, int l) {
     LevelBuf &L = c->lv[l];
     const kf_config &cf = c->cfg;
@@ -296,11 +312,7 @@ void vcycle(kf_ctx *c, int l) {
                                                                    c->d_sweeps);
         return;
     }
-    for (int s = 0; s < cf.mg_pre; ++s)
-        for (int color = 0; color < 2; ++color) {
-            Launch L_(c, KC_RBGS, 16. * N);
-            k_rbgs<<<mg_grid(n / 2, n), mg_block(), 0, c->st>>>(L.phi, L.rho, L.lev(), color);
-        }
+    smooth(c, L, L.phi, L.rho, nullptr, cf.mg_pre, KC_RBGS);
     {
         Launch L_(c, KC_RESID, 24. * N);
         k_residual<true><<<mg_grid(n, n), mg_block(), 0, c->st>>>(L.phi, L.rho, L.lev(), L.r);
@@ -324,11 +336,7 @@ void vcycle(kf_ctx *c, int l) {
         Launch L_(c, KC_TRANSFER, 16. * N + 8. * Nc3);
         k_prolong_add<<<mg_grid(Lc.n, Lc.n), mg_block(), 0, c->st>>>(L.phi, Lc.phi0, nullptr, L.gam, n);
     }
-    for (int s = 0; s < cf.mg_post; ++s)
-        for (int color = 0; color < 2; ++color) {
-            Launch L_(c, KC_RBGS, 16. * N);
-            k_rbgs<<<mg_grid(n / 2, n), mg_block(), 0, c->st>>>(L.phi, L.rho, L.lev(), color);
-        }
+    smooth(c, L, L.phi, L.rho, nullptr, cf.mg_post, KC_RBGS);
     CK(cudaGetLastError());
 }
 
