@@ -12,12 +12,14 @@
 //      K_q = -(lin_q + F_q)   (or P F_q with penalization)
 // RK4 (RKO4.cpp:50-241) combines four such evaluations with k_rk.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
 
 #include "../../include/kielflow_b200.h"
 #include "kf_adjoint.cuh"
+#include "kf_graph.cuh"
 #include "kf_passes.cuh"
 #include "kf_pointwise.cuh"
 #include "kf_poisson.cuh"
@@ -113,6 +115,16 @@ struct kf_ctx {
     // under which a right-hand side uses c->phi as it stands (no solve)
     AdjState *adj = nullptr;
     bool phi_given = false;
+    // one RK4 step captured as a CUDA graph (FAS or no Poisson, profile off):
+    // time / warm-start history and solve statistics live on the device
+    bool capturing = false;
+    cudaStream_t st_body = nullptr;  // stream on which conditional bodies are captured
+    DevTime *dtime = nullptr;
+    DevPois *dpois = nullptr;
+    DevPois hpois{};  // last values read back
+    cudaGraphExec_t step_graph = nullptr;
+    double step_dt = 0.;
+    long long step_kernels = 0, cycle_kernels = 0;
     int jV_x = 0, jV_y = 0, zV = 0, zW = 0, nWz = 0, nWf = 0, jW_y = 0, jW_x = 0, zS = 0, jS_y = 0, jS_x = 0;
     int jP_x = 0, jP_y = 0, zP = 0, jQ_x = 0, jQ_y = 0, zQ = 0;
 };
@@ -456,6 +468,72 @@ bool phi_guess(kf_ctx *c) {
     return newtime;
 }
 
+// The stage's Poisson solve inside the capture of a step graph: device-side
+// warm start, then the FAS loop as a conditional WHILE node whose body (one
+// V-cycle + the max-residual test) is captured on st_body.
+void poisson_captured(kf_ctx *c) {
+    const kf_config &cf = c->cfg;
+    const bool extrap = cf.phi_extrap != 0;
+    if (extrap) {
+        Launch L_(c, KC_MISC, 24. * c->N);
+        k_guess<<<nblk(c->N, 256), 256, 0, c->st>>>(c->phi, c->phi_a, c->dtime, c->N);
+    }
+    if (extrap) {
+        Launch L_(c, KC_MISC, 0.);
+        k_guess_post<<<1, 32, 0, c->st>>>(c->dtime);
+    }
+    LevelBuf &L0 = c->lv[0];
+    const bool fixed = !(cf.res_tol > 0.);
+    auto resmax = [&](cudaStream_t st) {
+        CK(cudaMemsetAsync(c->d_max, 0, 64 * sizeof(unsigned long long), st));
+        Launch L_(c, KC_RESID, 16. * c->N);
+        dim3 g = mg_grid(L0.n, L0.n);
+        g.z = L0.n < 16 ? L0.n : 16;
+        k_resmax<true><<<g, mg_block(), 0, st>>>(c->phi, c->rho, L0.lev(), c->d_max);
+    };
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamGetCaptureInfo(c->st, &cs, nullptr, &g, nullptr, nullptr));
+    cudaGraphConditionalHandle h;
+    CK(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
+    resmax(c->st);
+    {
+        Launch L_(c, KC_MISC, 0.);
+        k_fas_check<<<1, 32, 0, c->st>>>(c->d_max, c->dpois, cf.res_tol, cf.max_cycles, 1, fixed, h);
+    }
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    CK(cudaStreamGetCaptureInfo(c->st, &cs, nullptr, &g, &deps, &ndeps));
+    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, g, deps, ndeps, &cp));
+    CK(cudaStreamUpdateCaptureDependencies(c->st, &node, 1, cudaStreamSetCaptureDependencies));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    const long long l0 = c->launches;
+    cudaStream_t outer = c->st;
+    c->st = c->st_body;
+    CK(cudaStreamBeginCaptureToGraph(c->st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    vcycle(c, 0);
+    resmax(c->st);
+    {
+        Launch L_(c, KC_MISC, 0.);
+        k_fas_check<<<1, 32, 0, c->st>>>(c->d_max, c->dpois, cf.res_tol, cf.max_cycles, 0, fixed, h);
+    }
+    cudaGraph_t body_out = nullptr;
+    cudaError_t e = cudaStreamEndCapture(c->st, &body_out);
+    c->st = outer;
+    CK(e);
+    c->cycle_kernels = c->launches - l0;
+    if (extrap) {
+        Launch L_(c, KC_MISC, 0.);
+        k_hist_post<<<1, 32, 0, c->st>>>(c->dtime);
+    }
+    CK(cudaGetLastError());
+}
+
 // ------------------------------------------------------------------ per-(T, N) implementation
 template <typename T, int N> struct Impl {
     typedef typename C2<T>::type T2;
@@ -556,12 +634,16 @@ template <typename T, int N> struct Impl {
                 k_rho<T><<<nblk(c->N, 256), 256, 0, c->st>>>((const T *)c->R[0], c->nd, c->rho, c->N);
             }
             CK(cudaGetLastError());
-            const bool newtime = phi_guess(c);
-            int rc = poisson(c);
-            if (rc) throw KfError{KF_ERR_NOT_CONVERGED, "Poisson solve did not reach its tolerance"};
-            if (c->cfg.phi_extrap && newtime) {
-                c->nhist = c->nhist < 2 ? c->nhist + 1 : 2;
-                c->tau_b = c->t_stage;
+            if (c->capturing) {
+                poisson_captured(c);
+            } else {
+                const bool newtime = phi_guess(c);
+                int rc = poisson(c);
+                if (rc) throw KfError{KF_ERR_NOT_CONVERGED, "Poisson solve did not reach its tolerance"};
+                if (c->cfg.phi_extrap && newtime) {
+                    c->nhist = c->nhist < 2 ? c->nhist + 1 : 2;
+                    c->tau_b = c->t_stage;
+                }
             }
         }
         // B
@@ -977,6 +1059,7 @@ void create(kf_ctx *c) {
     if (!ok) throw KfError{KF_ERR_ARG, "grid size must be one of 16, 32, 64, 96, 128, 256"};
     CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
     c->own_stream = true;
+    CK(cudaStreamCreateWithFlags(&c->st_body, cudaStreamNonBlocking));
     const size_t cb = c->cs * c->Nc, rb = c->es * c->N;
     for (int q = 0; q < 4; ++q) {
         c->Y[q] = dalloc<void>(c, cb);
@@ -1010,6 +1093,10 @@ void create(kf_ctx *c) {
     CK(cudaMallocHost(&c->h_max, 64 * sizeof(unsigned long long)));
     if (cf.phi_extrap) c->phi_a = dalloc<double>(c, 8 * c->N);
     CK(cudaMallocHost(&c->h_red, sizeof(double) * 8));
+    c->dtime = dalloc<DevTime>(c, sizeof(DevTime));
+    c->dpois = dalloc<DevPois>(c, sizeof(DevPois));
+    CK(cudaMemset(c->dtime, 0, sizeof(DevTime)));
+    CK(cudaMemset(c->dpois, 0, sizeof(DevPois)));
     build_tables(c);
     build_levels(c);
     build_jobs(c);
@@ -1083,6 +1170,106 @@ void rk4_step(kf_ctx *c, double dt, void *const *X, double *const *PH, double *c
     c->t = t0 + dt;
 }
 
+// Whether kf_rk4_steps replays a captured step graph: every decision of the
+// step can be taken on the device (FAS or no Poisson solve; the Jacobi and
+// cascadic solvers steer their sweeps from the host) and the per-launch
+// profile is off.  KIELFLOW_B200_NO_GRAPH=1 forces the host-driven path.
+bool graph_path(kf_ctx *c) {
+    const kf_config &cf = c->cfg;
+    static const bool off = [] {
+        const char *e = std::getenv("KIELFLOW_B200_NO_GRAPH");
+        return e && e[0] == '1';
+    }();
+    if (c->prof || off) return false;
+    const bool pois = (cf.terms & T_POISSON) && (cf.terms & T_E_INT);
+    return !pois || cf.poisson_mode == KF_PS_FAS;
+}
+
+// Capture one RK4 step (the sequence of rk4_step) with device-side stage
+// times, warm starts and convergence loops.
+void build_step_graph(kf_ctx *c, double dt) {
+    if (c->step_graph && c->step_dt == dt) return;
+    if (c->step_graph) {
+        cudaGraphExecDestroy(c->step_graph);
+        c->step_graph = nullptr;
+    }
+    const double xs[4] = {0., 0.5 * dt, 0.5 * dt, 1.0 * dt};
+    const double cdt[4] = {0.5 * dt, 0.5 * dt, 1.0 * dt, dt / 6.};
+    const int mode[4] = {0, 1, 1, 2};
+    const kf_config &cf = c->cfg;
+    const bool pois = (cf.terms & T_POISSON) && (cf.terms & T_E_INT);
+    const long long l0 = c->launches;
+    c->cycle_kernels = 0;
+    c->capturing = true;
+    CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+    try {
+        for (int i = 0; i < 4; ++i) {
+            {
+                Launch L_(c, KC_MISC, 0.);
+                k_time<<<1, 32, 0, c->st>>>(c->dtime, xs[i], 0);
+            }
+            c->rhs_fn(c);
+            rk_launch(c, cdt[i], mode[i]);
+        }
+        copy_state(c, c->Ys, c->Y);
+        {
+            Launch L_(c, KC_MISC, 0.);
+            k_time<<<1, 32, 0, c->st>>>(c->dtime, dt, 1);
+        }
+    } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(c->st, &g);
+        if (g) cudaGraphDestroy(g);
+        c->capturing = false;
+        c->launches = l0;
+        throw;
+    }
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(c->st, &g);
+    c->capturing = false;
+    CK(e);
+    e = cudaGraphInstantiate(&c->step_graph, g, 0);
+    cudaGraphDestroy(g);
+    CK(e);
+    c->step_kernels = c->launches - l0 - (pois ? 4 * c->cycle_kernels : 0);
+    c->launches = l0;
+    c->step_dt = dt;
+}
+
+// nsteps replays of the step graph; the host's time and warm-start record is
+// handed to the device before and read back after, with the solve statistics.
+void rk4_steps_graph(kf_ctx *c, int nsteps, double dt) {
+    build_step_graph(c, dt);
+    DevTime ht{c->t, c->t_stage, c->tau_a, c->tau_b, c->nhist, 0, 0, 0};
+    CK(cudaMemcpyAsync(c->dtime, &ht, sizeof(DevTime), cudaMemcpyHostToDevice, c->st));
+    for (int s = 0; s < nsteps; ++s) {
+        CK(cudaGraphLaunch(c->step_graph, c->st));
+        c->launches += c->step_kernels;
+    }
+    DevPois hp;
+    CK(cudaMemcpyAsync(&ht, c->dtime, sizeof(DevTime), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(&hp, c->dpois, sizeof(DevPois), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    c->t = ht.t;
+    c->t_stage = ht.t_stage;
+    c->tau_a = ht.tau_a;
+    c->tau_b = ht.tau_b;
+    c->nhist = ht.nhist;
+    const DevPois &o = c->hpois;
+    c->launches += (hp.total_cycles - o.total_cycles) * c->cycle_kernels;
+    c->diag.solves += hp.solves - o.solves;
+    c->diag.total_iterations += hp.total_cycles - o.total_cycles;
+    if (hp.solves != o.solves) {
+        c->diag.last_iterations = hp.last_cycles;
+        c->diag.last_residual = hp.last_residual;
+    }
+    c->diag.not_converged += hp.not_converged - o.not_converged;
+    const bool nan = hp.nans != o.nans, nc = hp.not_converged != o.not_converged;
+    c->hpois = hp;
+    if (nan) throw KfError{KF_ERR_NAN, "NaN in the multigrid solve"};
+    if (nc) throw KfError{KF_ERR_NOT_CONVERGED, "Poisson solve did not reach its tolerance"};
+}
+
 template <typename F> int guarded(kf_ctx *c, F f) {
     if (!c) return KF_ERR_ARG;
     try {
@@ -1134,6 +1321,8 @@ int kf_ctx_destroy(kf_ctx *c) {
     }
     for (auto e : c->evfree) cudaEventDestroy(e);
     if (c->vgraph) cudaGraphExecDestroy(c->vgraph);
+    if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+    if (c->st_body) cudaStreamDestroy(c->st_body);
     adj_release(c);
     for (void *p : c->allocs) cudaFree(p);
     if (c->h_red) cudaFreeHost(c->h_red);
@@ -1221,6 +1410,10 @@ int kf_rk4_steps(kf_ctx *c, int nsteps, double dt) {
     return guarded(c, [&] {
         if (nsteps < 0) throw KfError{KF_ERR_ARG, "nsteps < 0"};
         // Ys == Y on entry; stage times t, t + dt/2, t + dt/2, t + dt (RKO4.cpp:105-212)
+        if (nsteps > 0 && graph_path(c)) {
+            rk4_steps_graph(c, nsteps, dt);
+            return;
+        }
         for (int s = 0; s < nsteps; ++s) rk4_step(c, dt, nullptr, nullptr, nullptr);
         CK(cudaGetLastError());
     });

@@ -1,0 +1,62 @@
+"""The captured step (kf_rk4_steps replaying one CUDA graph per RK4 step, with
+the stage times, warm starts and FAS convergence loops decided on the device)
+against the host-driven step (the per-launch profile forces it): identical
+states, potentials and solve statistics, bit for bit."""
+import numpy as np
+import pytest
+
+import kielflow_b200 as kf
+from kielflow_b200 import configs as C
+
+pytestmark = pytest.mark.gpu
+
+
+def run(w, n, steps, host, **over):
+    st, nd, mask, dt = C.make_inputs(w, n)
+    with kf.Context(C.config_for(w, n, **over)) as ctx:
+        ctx.set_state(*st)
+        ctx.set_sources(nd, mask)
+        if host:
+            ctx.profile(True)
+        l0 = ctx.launch_count()
+        ctx.rk4(dt, steps)
+        launches = ctx.launch_count() - l0
+        d = ctx.diag()
+        return ctx.get_state(), ctx.get_phi(), (d.solves, d.total_iterations, d.last_iterations), launches
+
+
+@pytest.mark.parametrize("name,n,over", [
+    ("fas128", 64, {}),
+    ("fp32bulk256", 64, {}),
+    ("fas128", 32, dict(res_tol=-1.0, max_cycles=5)),
+    ("fas128", 128, {}),
+])
+def test_graph_step_matches_host_step(name, n, over):
+    w = C.WORKLOADS[name]
+    sg, pg, dg, lg = run(w, n, 3, host=False, **over)
+    sh, ph, dh, lh = run(w, n, 3, host=True, **over)
+    for a, b in zip(sg, sh):
+        assert np.array_equal(a, b)
+    assert np.array_equal(pg, ph)
+    assert dg == dh
+    # kernels counted per executed V-cycle on both paths; the graph adds its
+    # one-thread control kernels (stage time, warm start, convergence test)
+    assert lg >= lh > 0
+
+
+def test_graph_step_in_pieces():
+    """3 calls of 1 step and 1 call of 3 steps: the device record carries the
+    time and the warm-start history across calls."""
+    w = C.WORKLOADS["fas128"]
+    st, nd, mask, dt = C.make_inputs(w, 64)
+    out = []
+    for pieces in ([3], [1, 1, 1]):
+        with kf.Context(C.config_for(w, 64)) as ctx:
+            ctx.set_state(*st)
+            ctx.set_sources(nd, mask)
+            for k in pieces:
+                ctx.rk4(dt, k)
+            out.append((ctx.get_state(), ctx.get_phi()))
+    for a, b in zip(out[0][0], out[1][0]):
+        assert np.array_equal(a, b)
+    assert np.array_equal(out[0][1], out[1][1])
