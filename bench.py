@@ -418,23 +418,29 @@ def run_sweep_bench(args):
     torch.cuda.set_device(local)
     inst = sweep_instances(seed=0)
     mine = [inst[i] for i in kdist.partition([x.n for x in inst], ws)[rank]]
-    run_sweep(mine[:3], steps=1, concurrent=True)  # warm-up (module load, graph capture paths)
     if ws > 1:
         torch.distributed.barrier()
-    wall_c, _, dg = run_sweep(mine, steps=args.steps, concurrent=True)
+    wall_c, _, dg = run_sweep(mine, steps=args.steps, mode="batched", warmup=args.warmup)
     wall_c = kdist.max_over_ranks(wall_c, device="cuda")
-    wall_s = None
+    wall_s = wall_t = None
     if not args.no_fp64:  # the sequential reference run (skipped with --no-fp64 to save time)
-        wall_s, _, _ = run_sweep(mine, steps=args.steps, concurrent=False)
+        wall_s, _, _ = run_sweep(mine, steps=args.steps, mode="sequential", warmup=args.warmup)
         wall_s = kdist.max_over_ranks(wall_s, device="cuda")
+        wall_t, _, _ = run_sweep(mine, steps=args.steps, mode="threads", warmup=args.warmup)
+        wall_t = kdist.max_over_ranks(wall_t, device="cuda")
     if rank == 0:
         total = len(inst) * args.steps
         out = {"metric": "sweep instance-steps/s (48 instances, 64^3/96^3/128^3, FP32 bulk)",
                "value": total / wall_c, "unit": "instance-steps/s", "n_gpus": ws, "steps": args.steps,
-               "warmup": 1, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+               "warmup": args.warmup, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
                "dtype": "fp32 bulk + fp64 Poisson", "data": "synthetic",
-               "config": {"workload": "sweep48", "timing": "host wall clock around fully synchronised runs"},
+               "config": {"workload": "sweep48: 16 x 64^3, 16 x 96^3, 16 x 128^3; M ~ U[0.3,1.5], nu ~ U[0.01,0.3], "
+                                      "Q ~ U[-50,-5] (seed 0); FP32 bulk, FP64 FAS Poisson",
+                          "timing": "host wall clock around fully synchronised runs; warm-up steps "
+                                    "(graph capture) outside", "batched": "kf_batch_rk4_steps",
+                          "sequential": "kf_rk4_steps per instance, one after another"},
                "sequential_value": (total / wall_s) if wall_s else None,
+               "threads_value": (total / wall_t) if wall_t else None,
                "batched_over_sequential": (wall_s / wall_c) if wall_s else None}
         print(json.dumps(out))
     if ws > 1:

@@ -121,8 +121,24 @@ int kf_get_phi(kf_ctx *ctx, double *phi);
 int kf_rhs_eval(kf_ctx *ctx, double t);
 
 /* interface_ode_solver::solve (interface_ODE_solver.hpp:11-12; RKO4.cpp:50-241):
- * nsteps classic RK4 steps of size dt on the device-resident state. */
+ * nsteps classic RK4 steps of size dt on the device-resident state.  With
+ * KF_PS_FAS (or no Poisson solve) and the profile off, each step is one
+ * replay of a captured CUDA graph whose stage times, warm starts and V-cycle
+ * loops are decided on the device, and the call returns after the steps have
+ * finished; a solve that missed its tolerance is then reported for the call
+ * (KF_ERR_NOT_CONVERGED / KF_ERR_NAN) rather than at its stage.  Otherwise
+ * the host drives every stage (the Jacobi and cascadic solvers) and the call
+ * may return before the GPU has finished. */
 int kf_rk4_steps(kf_ctx *ctx, int nsteps, double dt);
+
+/* Batched form of kf_rk4_steps for independent contexts (a parameter sweep;
+ * grids may differ): dts[i] is context i's step.  One host thread queues every
+ * context's captured step on the context's own stream, step by step, so the
+ * instances' kernels overlap on the GPU; returns after all have finished.  Each
+ * context must qualify for the captured step (KF_PS_FAS or no Poisson solve,
+ * profile off).  The first failing context's code is returned; its message is
+ * in kf_last_error(that context) and kf_last_error(NULL). */
+int kf_batch_rk4_steps(kf_ctx *const *ctxs, int nctx, int nsteps, const double *dts);
 
 /* interface_poisson_solver::solve (interface_poisson_solver.hpp:18): phi_io is
  * the initial guess and the result, rho is read only; host arrays, n^3 doubles. */

@@ -90,6 +90,7 @@ EXPORTS = [
     "kf_get_state", "kf_set_sources", "kf_set_phi", "kf_get_phi", "kf_rhs_eval", "kf_rk4_steps",
     "kf_poisson_solve", "kf_diag", "kf_fft_r2c", "kf_fft_c2r", "kf_state_device_ptrs", "kf_launch_count",
     "kf_profile_enable", "kf_profile_read", "kf_profile_class_name", "kf_fft_r2c_noalloc", "kf_adjoint_run",
+    "kf_batch_rk4_steps",
 ]
 KCLASSES = 18
 
@@ -132,6 +133,7 @@ def load_library():
     L.kf_profile_class_name.argtypes = [ctypes.c_int]
     L.kf_profile_class_name.restype = ctypes.c_char_p
     L.kf_fft_r2c_noalloc.argtypes = [ctypes.c_int, vp, vp, vp]
+    L.kf_batch_rk4_steps.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int, _D]
     L.kf_adjoint_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, _D,
                                  ctypes.POINTER(GradOut), _D, _D]
     _lib = L
@@ -142,6 +144,20 @@ def _ptr(a: np.ndarray):
     if not a.flags["C_CONTIGUOUS"]:
         raise ValueError("array must be C-contiguous")
     return a.ctypes.data_as(_D)
+
+
+def batch_rk4(contexts, dts, nsteps: int):
+    """kf_batch_rk4_steps: nsteps RK4 steps of every context (its own dt),
+    queued from this thread on the contexts' streams; returns when all are done."""
+    L = load_library()
+    n = len(contexts)
+    arr = (ctypes.c_void_p * n)(*[c.h.value for c in contexts])
+    d = np.ascontiguousarray(dts, np.float64)
+    if d.shape != (n,):
+        raise ValueError("one dt per context")
+    rc = L.kf_batch_rk4_steps(arr, n, nsteps, _ptr(d))
+    if rc:
+        raise KfError(rc, L.kf_last_error(None).decode())
 
 
 class Context:

@@ -1238,14 +1238,19 @@ void build_step_graph(kf_ctx *c, double dt) {
 
 // nsteps replays of the step graph; the host's time and warm-start record is
 // handed to the device before and read back after, with the solve statistics.
-void rk4_steps_graph(kf_ctx *c, int nsteps, double dt) {
+void graph_begin(kf_ctx *c, double dt) {
     build_step_graph(c, dt);
     DevTime ht{c->t, c->t_stage, c->tau_a, c->tau_b, c->nhist, 0, 0, 0};
     CK(cudaMemcpyAsync(c->dtime, &ht, sizeof(DevTime), cudaMemcpyHostToDevice, c->st));
-    for (int s = 0; s < nsteps; ++s) {
-        CK(cudaGraphLaunch(c->step_graph, c->st));
-        c->launches += c->step_kernels;
-    }
+}
+
+void graph_step(kf_ctx *c) {
+    CK(cudaGraphLaunch(c->step_graph, c->st));
+    c->launches += c->step_kernels;
+}
+
+void graph_end(kf_ctx *c) {
+    DevTime ht;
     DevPois hp;
     CK(cudaMemcpyAsync(&ht, c->dtime, sizeof(DevTime), cudaMemcpyDeviceToHost, c->st));
     CK(cudaMemcpyAsync(&hp, c->dpois, sizeof(DevPois), cudaMemcpyDeviceToHost, c->st));
@@ -1268,6 +1273,12 @@ void rk4_steps_graph(kf_ctx *c, int nsteps, double dt) {
     c->hpois = hp;
     if (nan) throw KfError{KF_ERR_NAN, "NaN in the multigrid solve"};
     if (nc) throw KfError{KF_ERR_NOT_CONVERGED, "Poisson solve did not reach its tolerance"};
+}
+
+void rk4_steps_graph(kf_ctx *c, int nsteps, double dt) {
+    graph_begin(c, dt);
+    for (int s = 0; s < nsteps; ++s) graph_step(c);
+    graph_end(c);
 }
 
 template <typename F> int guarded(kf_ctx *c, F f) {
@@ -1417,6 +1428,47 @@ int kf_rk4_steps(kf_ctx *c, int nsteps, double dt) {
         for (int s = 0; s < nsteps; ++s) rk4_step(c, dt, nullptr, nullptr, nullptr);
         CK(cudaGetLastError());
     });
+}
+
+int kf_batch_rk4_steps(kf_ctx *const *ctxs, int nctx, int nsteps, const double *dts) {
+    if (!ctxs || !dts || nctx < 0 || nsteps < 0) {
+        kf_global_error() = "kf_batch_rk4_steps: invalid argument";
+        return KF_ERR_ARG;
+    }
+    for (int i = 0; i < nctx; ++i) {
+        if (!ctxs[i]) {
+            kf_global_error() = "kf_batch_rk4_steps: null context";
+            return KF_ERR_ARG;
+        }
+        if (!graph_path(ctxs[i])) {
+            ctxs[i]->err = "kf_batch_rk4_steps needs a context whose step can be captured "
+                           "(KF_PS_FAS or no Poisson solve, profile off)";
+            kf_global_error() = ctxs[i]->err;
+            return KF_ERR_ARG;
+        }
+    }
+    int rc = KF_OK;
+    std::vector<char> begun(nctx, 0);
+    for (int i = 0; i < nctx && rc == KF_OK; ++i) {
+        rc = guarded(ctxs[i], [&] { graph_begin(ctxs[i], dts[i]); });
+        begun[i] = rc == KF_OK;
+        if (rc != KF_OK) kf_global_error() = ctxs[i]->err;
+    }
+    // step-major: every instance's step s is queued before any step s + 1
+    for (int s = 0; s < nsteps && rc == KF_OK; ++s)
+        for (int i = 0; i < nctx && rc == KF_OK; ++i) {
+            rc = guarded(ctxs[i], [&] { graph_step(ctxs[i]); });
+            if (rc != KF_OK) kf_global_error() = ctxs[i]->err;
+        }
+    for (int i = 0; i < nctx; ++i) {
+        if (!begun[i]) continue;
+        const int r = guarded(ctxs[i], [&] { graph_end(ctxs[i]); });
+        if (r != KF_OK && rc == KF_OK) {
+            rc = r;
+            kf_global_error() = ctxs[i]->err;
+        }
+    }
+    return rc;
 }
 
 int kf_poisson_solve(kf_ctx *c, double *phi_io, const double *rho) {

@@ -42,19 +42,26 @@ def workload_of(inst: Instance) -> dict:
     return w
 
 
-def run_sweep(instances, steps: int, concurrent: bool = True, precision=None, max_threads: int = 64):
+def run_sweep(instances, steps: int, mode: str = "batched", precision=None, warmup: int = 1,
+              max_threads: int = 64):
     """Advance every instance `steps` RK4 steps on the current GPU.
 
-    Each instance is its own context (device memory, tables, CUDA stream).
-    concurrent=True drives all contexts from a pool of host threads (the C
-    calls release the GIL), so that their kernels overlap on the GPU; False
-    runs them one after another (the sequential baseline).  Returns
-    (wall seconds, [final state per instance], [diag per instance]).
+    Each instance is its own context (device memory, tables, CUDA stream,
+    captured step graph).  Modes:
+      "batched"    -- one kf_batch_rk4_steps call: this thread queues every
+                      instance's step graph on its own stream, step by step,
+                      so the instances' kernels overlap on the GPU;
+      "threads"    -- a pool of host threads, one kf_rk4_steps call each
+                      (the C calls release the GIL);
+      "sequential" -- one instance after another (the baseline).
+    `warmup` steps per instance run first, outside the timed region (graph
+    capture, first-touch of the buffers).  Returns (wall seconds of the timed
+    steps, [final state per instance], [diag per instance]).
     """
     import threading
     import time
 
-    from ._lib import Context
+    from ._lib import Context, batch_rk4
 
     ctxs, dts = [], []
     for inst in instances:
@@ -65,6 +72,9 @@ def run_sweep(instances, steps: int, concurrent: bool = True, precision=None, ma
         ctx.set_sources(nd, mask)
         ctxs.append(ctx)
         dts.append(dt)
+    if warmup > 0:
+        for ctx, dt in zip(ctxs, dts):
+            ctx.rk4(dt, warmup)
     for ctx in ctxs:
         ctx.synchronize()
     errors = []
@@ -77,7 +87,9 @@ def run_sweep(instances, steps: int, concurrent: bool = True, precision=None, ma
             errors.append((i, e))
 
     t0 = time.perf_counter()
-    if concurrent:
+    if mode == "batched":
+        batch_rk4(ctxs, dts, steps)
+    elif mode == "threads":
         nthreads = min(max_threads, len(ctxs))
         pending = list(range(len(ctxs)))
         lock = threading.Lock()
@@ -95,9 +107,11 @@ def run_sweep(instances, steps: int, concurrent: bool = True, precision=None, ma
             t.start()
         for t in threads:
             t.join()
-    else:
+    elif mode == "sequential":
         for i in range(len(ctxs)):
             work(i)
+    else:
+        raise ValueError(f"unknown mode {mode!r}")
     wall = time.perf_counter() - t0
     if errors:
         raise errors[0][1]
