@@ -240,8 +240,9 @@ __global__ void __launch_bounds__(256) k_rbgs(double *__restrict__ phi, const do
 
 // Coarsest-level solve in one block: the level (phi, rho and the axis
 // tables) is staged in shared memory, red-black sweeps run until
-// max |f| <= tol (checked before every sweep, as the host loop of the oracle),
-// then phi is written back.  Dynamic shared memory: 16 n^3 + 24 n bytes.
+// max |f| <= max(tol, 1e-4 max |f| at entry) (checked before every sweep, as
+// the host loop of the oracle), then phi is written back.  Dynamic shared
+// memory: 16 n^3 + 24 n bytes.
 __global__ void __launch_bounds__(1024) k_coarse_solve(double *__restrict__ phi, const double *__restrict__ rho,
                                                        Lev L, double tol, int max_sweeps,
                                                        int *__restrict__ sweeps_out) {
@@ -262,6 +263,7 @@ __global__ void __launch_bounds__(1024) k_coarse_solve(double *__restrict__ phi,
     __syncthreads();
     const Lev Ls{n, sd, nullptr, nullptr, si, sm_};
     int s = 0;
+    double r0 = 0.;
     for (;; ++s) {
         double m = 0.;
         for (int id = threadIdx.x; id < N; id += blockDim.x) {
@@ -283,7 +285,8 @@ __global__ void __launch_bounds__(1024) k_coarse_solve(double *__restrict__ phi,
         __syncthreads();
         const double res = sh[0];
         __syncthreads();
-        if (!(res > tol) || s >= max_sweeps) break;  // converged, NaN or capped
+        if (s == 0) r0 = res;
+        if (!(res > fmax(tol, 1e-4 * r0)) || s >= max_sweeps) break;  // converged, NaN or capped
         for (int color = 0; color < 2; ++color) {
             const int M = N / 2, nh = n / 2;
             for (int id = threadIdx.x; id < M; id += blockDim.x) {

@@ -24,6 +24,7 @@
  */
 #include "kf_oracle.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -411,8 +412,13 @@ void fas_vcycle(kfo_ctx *c, int l, vec &phi, const vec &rho) {
     const level &L = c->lv[l];
     const kfo_config &cf = c->cfg;
     if (l == (int)c->lv.size() - 1) {
+        /* coarsest level: relaxed until its max residual is at most
+           max(coarse_tol, 1e-4 x its value at entry), at most 1000 sweeps */
+        double r0 = 0.;
         for (int s = 0; s < 1000; ++s) {
-            if (max_resid_fast(L, phi, rho) <= cf.coarse_tol) break;
+            const double r = max_resid_fast(L, phi, rho);
+            if (s == 0) r0 = r;
+            if (r <= std::max(cf.coarse_tol, 1e-4 * r0)) break;
             rbgs_sweep(L, phi, rho);
         }
         return;
