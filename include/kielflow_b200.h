@@ -94,6 +94,7 @@ typedef struct {
     int not_converged;      /* solves that hit their cap                        */
     double charge;          /* sum(e^s - e^phi + n_d) h^3 (FP64)                */
     double kinetic;         /* sum 0.5 e^s |u|^2 h^3, u = u' + M e_x (FP64)     */
+    long long stage_cycles[4]; /* FAS V-cycles spent in RK stages 1..4          */
 } kf_diag_out;
 
 /* Context lifetime.  Replaces constructing the reference's rhs_standard

@@ -64,7 +64,8 @@ class Config(ctypes.Structure):
 class DiagOut(ctypes.Structure):
     _fields_ = [("solves", ctypes.c_int), ("last_iterations", ctypes.c_int),
                 ("total_iterations", ctypes.c_longlong), ("last_residual", ctypes.c_double),
-                ("not_converged", ctypes.c_int), ("charge", ctypes.c_double), ("kinetic", ctypes.c_double)]
+                ("not_converged", ctypes.c_int), ("charge", ctypes.c_double), ("kinetic", ctypes.c_double),
+                ("stage_cycles", ctypes.c_longlong * 4)]
 
 
 class GradOut(ctypes.Structure):

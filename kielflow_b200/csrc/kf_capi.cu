@@ -115,6 +115,7 @@ struct kf_ctx {
     // under which a right-hand side uses c->phi as it stands (no solve)
     AdjState *adj = nullptr;
     bool phi_given = false;
+    int stage_idx = 0;  // RK stage of the right-hand side being evaluated (0..3)
     // one RK4 step captured as a CUDA graph (FAS or no Poisson, profile off):
     // time / warm-start history and solve statistics live on the device
     bool capturing = false;
@@ -428,6 +429,7 @@ int poisson(kf_ctx *c) {
         const double r = max_residual(c, L0, c->phi, c->rho, true);
         c->diag.last_iterations = cf.max_cycles;
         c->diag.total_iterations += cf.max_cycles;
+        c->diag.stage_cycles[c->stage_idx & 3] += cf.max_cycles;
         c->diag.last_residual = r;
         if (r != r) throw KfError{KF_ERR_NAN, "NaN in the multigrid solve"};
     } else {
@@ -439,6 +441,7 @@ int poisson(kf_ctx *c) {
             r = max_residual(c, L0, c->phi, c->rho, true);
         }
         c->diag.last_iterations = cyc;
+        c->diag.stage_cycles[c->stage_idx & 3] += cyc;
         c->diag.total_iterations += cyc;
         c->diag.last_residual = r;
         if (r != r) throw KfError{KF_ERR_NAN, "NaN in the multigrid solve"};
@@ -499,7 +502,7 @@ void poisson_captured(kf_ctx *c) {
     resmax(c->st);
     {
         Launch L_(c, KC_MISC, 0.);
-        k_fas_check<<<1, 32, 0, c->st>>>(c->d_max, c->dpois, cf.res_tol, cf.max_cycles, 1, fixed, h);
+        k_fas_check<<<1, 32, 0, c->st>>>(c->d_max, c->dpois, cf.res_tol, cf.max_cycles, 1, fixed, c->stage_idx, h);
     }
     const cudaGraphNode_t *deps = nullptr;
     size_t ndeps = 0;
@@ -520,7 +523,7 @@ void poisson_captured(kf_ctx *c) {
     resmax(c->st);
     {
         Launch L_(c, KC_MISC, 0.);
-        k_fas_check<<<1, 32, 0, c->st>>>(c->d_max, c->dpois, cf.res_tol, cf.max_cycles, 0, fixed, h);
+        k_fas_check<<<1, 32, 0, c->st>>>(c->d_max, c->dpois, cf.res_tol, cf.max_cycles, 0, fixed, c->stage_idx, h);
     }
     cudaGraph_t body_out = nullptr;
     cudaError_t e = cudaStreamEndCapture(c->st, &body_out);
@@ -1156,6 +1159,7 @@ void rk4_step(kf_ctx *c, double dt, void *const *X, double *const *PH, double *c
     const int mode[4] = {0, 1, 1, 2};
     for (int i = 0; i < 4; ++i) {
         c->t_stage = ts[i];
+        c->stage_idx = i;
         if (X) copy_state(c, X + 4 * i, c->Ys);
         if (PHin) {
             CK(cudaMemcpyAsync(c->phi, PHin[i], 8 * c->N, cudaMemcpyDeviceToDevice, c->st));
@@ -1208,6 +1212,7 @@ void build_step_graph(kf_ctx *c, double dt) {
                 Launch L_(c, KC_MISC, 0.);
                 k_time<<<1, 32, 0, c->st>>>(c->dtime, xs[i], 0);
             }
+            c->stage_idx = i;
             c->rhs_fn(c);
             rk_launch(c, cdt[i], mode[i]);
         }
@@ -1269,6 +1274,7 @@ void graph_end(kf_ctx *c) {
         c->diag.last_residual = hp.last_residual;
     }
     c->diag.not_converged += hp.not_converged - o.not_converged;
+    for (int s = 0; s < 4; ++s) c->diag.stage_cycles[s] += hp.stage_cycles[s] - o.stage_cycles[s];
     const bool nan = hp.nans != o.nans, nc = hp.not_converged != o.not_converged;
     c->hpois = hp;
     if (nan) throw KfError{KF_ERR_NAN, "NaN in the multigrid solve"};
@@ -1409,6 +1415,7 @@ int kf_get_phi(kf_ctx *c, double *phi) {
 int kf_rhs_eval(kf_ctx *c, double t) {
     return guarded(c, [&] {
         c->t_stage = t;  // selects the start of the Poisson solve only
+        c->stage_idx = 0;
         copy_state(c, c->Ys, c->Y);
         c->rhs_fn(c);
         copy_state(c, c->Y, c->K);

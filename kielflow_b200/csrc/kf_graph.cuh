@@ -25,6 +25,7 @@ struct DevPois {
     int cyc;                 // V-cycles of the current solve
     int last_cycles;
     int solves, not_converged, nans, pad;
+    long long stage_cycles[4];  // per RK stage
 };
 
 // mode 0: t_stage = t + x;  mode 1: t = t + x
@@ -76,7 +77,7 @@ __global__ void k_hist_post(DevTime *d) {
 // continue while r > tol and cyc < max_cycles (fixed: while cyc < max_cycles).
 // The loop is bounded by max_cycles whatever r is (NaN included).
 __global__ void k_fas_check(const unsigned long long *__restrict__ slots, DevPois *p, double tol, int max_cycles,
-                            int first, int fixed, cudaGraphConditionalHandle h) {
+                            int first, int fixed, int stage, cudaGraphConditionalHandle h) {
     if (threadIdx.x || blockIdx.x) return;
     unsigned long long m = 0;
     for (int s = 0; s < 64; ++s) m = slots[s] > m ? slots[s] : m;
@@ -90,6 +91,7 @@ __global__ void k_fas_check(const unsigned long long *__restrict__ slots, DevPoi
         p->total_cycles += cyc;
         p->last_cycles = cyc;
         p->last_residual = r;
+        p->stage_cycles[stage & 3] += cyc;
         if (r != r)
             p->nans += 1;
         else if (!fixed && r > tol)
