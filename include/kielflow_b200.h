@@ -132,6 +132,44 @@ int kf_rhs_eval(kf_ctx *ctx, double t);
  * may return before the GPU has finished. */
 int kf_rk4_steps(kf_ctx *ctx, int nsteps, double dt);
 
+/* ------------------------------------------------------------ the time loop
+ * kielflow.cpp:172-182: the input files hold the ion density on a linear
+ * scale; the state evolves s = ln n.  kf_set_state_linear sets the state
+ * from u' spectra and the spectrum Fn of n, forming s^ = r2c(log(c2r(Fn)))
+ * on the device. */
+int kf_set_state_linear(kf_ctx *ctx, const double *FUx, const double *FUy, const double *FUz,
+                        const double *Fn);
+
+/* The fields the reference's save_slice / save_all receive
+ * (kielflow.cpp:290-324): the u' spectra, Fn = r2c(exp(c2r(s^))) (linear
+ * density) and FPh = r2c(phi) with phi of the last stage solve.  Host arrays,
+ * Nc interleaved complex each; NULL entries skip. */
+int kf_get_output(kf_ctx *ctx, double *FUx, double *FUy, double *FUz, double *Fn, double *FPh);
+
+#define KF_OUT_SLICE 1  /* save_slice step  */
+#define KF_OUT_BACKUP 2 /* save_all backup  */
+typedef struct {
+    int step;       /* loop index: the state has advanced step + 1 RK4 steps  */
+    double t;       /* the reference's t_total at the output: t0 + step * dt  */
+                    /* (accumulated; it lags the state by one dt, as there)   */
+    int kind;       /* KF_OUT_SLICE | KF_OUT_BACKUP                           */
+    const double *FUx, *FUy, *FUz, *Fn, *FPh; /* as kf_get_output; valid     */
+                                              /* during the callback only     */
+} kf_output;
+typedef void (*kf_output_fn)(const kf_output *out, void *user);
+
+/* The time loop of kielflow.cpp:277-331: `iterations` RK4 steps of size dt;
+ * after step `step` a slice is due when the reference's counter i_output
+ * (counter.hpp: starts at 0, incremented after every step, reset at an output)
+ * has reached slice_every, a backup likewise with backup_every (0: never) --
+ * with 10 and 50, slices follow loop steps 10, 20, ... and backups 50, 100, ....
+ * The output fields are formed on the device and copied to pinned host memory
+ * on a side stream while the next steps run; fn is called from this thread,
+ * in step order, once an output's copy has finished (at most two are in
+ * flight).  Returns after the last step and the last callback. */
+int kf_run(kf_ctx *ctx, int iterations, double dt, double t0, int slice_every, int backup_every,
+           kf_output_fn fn, void *user);
+
 /* Batched form of kf_rk4_steps for independent contexts (a parameter sweep;
  * grids may differ): dts[i] is context i's step.  One host thread queues every
  * context's captured step on the context's own stream, step by step, so the

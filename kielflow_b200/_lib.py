@@ -78,6 +78,15 @@ class GradOut(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class Output(ctypes.Structure):
+    """kf_output (include/kielflow_b200.h)."""
+    _fields_ = [("step", ctypes.c_int), ("t", ctypes.c_double), ("kind", ctypes.c_int),
+                ("FUx", _D), ("FUy", _D), ("FUz", _D), ("Fn", _D), ("FPh", _D)]
+
+
+OUTPUT_FN = ctypes.CFUNCTYPE(None, ctypes.POINTER(Output), ctypes.c_void_p)
+KF_OUT_SLICE, KF_OUT_BACKUP = 1, 2
+
 KF_ADJ_STORE_PHI = 1
 KF_ADJ_J_ONLY = 2
 
@@ -91,7 +100,7 @@ EXPORTS = [
     "kf_get_state", "kf_set_sources", "kf_set_phi", "kf_get_phi", "kf_rhs_eval", "kf_rk4_steps",
     "kf_poisson_solve", "kf_diag", "kf_fft_r2c", "kf_fft_c2r", "kf_state_device_ptrs", "kf_launch_count",
     "kf_profile_enable", "kf_profile_read", "kf_profile_class_name", "kf_fft_r2c_noalloc", "kf_adjoint_run",
-    "kf_batch_rk4_steps",
+    "kf_batch_rk4_steps", "kf_set_state_linear", "kf_get_output", "kf_run",
 ]
 KCLASSES = 18
 
@@ -134,6 +143,10 @@ def load_library():
     L.kf_profile_class_name.argtypes = [ctypes.c_int]
     L.kf_profile_class_name.restype = ctypes.c_char_p
     L.kf_fft_r2c_noalloc.argtypes = [ctypes.c_int, vp, vp, vp]
+    L.kf_set_state_linear.argtypes = [vp, _D, _D, _D, _D]
+    L.kf_get_output.argtypes = [vp, _D, _D, _D, _D, _D]
+    L.kf_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                         OUTPUT_FN, ctypes.c_void_p]
     L.kf_batch_rk4_steps.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int, _D]
     L.kf_adjoint_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, _D,
                                  ctypes.POINTER(GradOut), _D, _D]
@@ -204,6 +217,37 @@ class Context:
             if a.shape != self.shape_c:
                 raise ValueError(f"spectral field must have shape {self.shape_c}")
         self._check(self.L.kf_set_state(self.h, *[a.ctypes.data_as(_D) for a in arrs]))
+
+    def set_state_linear(self, FUx, FUy, FUz, Fn):
+        """kf_set_state_linear: u' spectra and the spectrum of n (linear scale)."""
+        arrs = [np.ascontiguousarray(a, np.complex128) for a in (FUx, FUy, FUz, Fn)]
+        for a in arrs:
+            if a.shape != self.shape_c:
+                raise ValueError(f"spectral field must have shape {self.shape_c}")
+        self._check(self.L.kf_set_state_linear(self.h, *[a.ctypes.data_as(_D) for a in arrs]))
+
+    def get_output(self):
+        """kf_get_output: (FUx, FUy, FUz, Fn, FPh) as save_slice receives them."""
+        out = [np.empty(self.shape_c, np.complex128) for _ in range(5)]
+        self._check(self.L.kf_get_output(self.h, *[a.ctypes.data_as(_D) for a in out]))
+        return out
+
+    def run(self, iterations: int, dt: float, t0: float = 0.0, slice_every: int = 10, backup_every: int = 50,
+            callback=None):
+        """kf_run: the reference's time loop; callback(step, t, kind, fields) gets
+        copies of (FUx, FUy, FUz, Fn, FPh) at each output step."""
+        nc = int(np.prod(self.shape_c))
+        shape = self.shape_c
+
+        def fn(p, _user):
+            o = p.contents
+            fields = [np.ctypeslib.as_array(getattr(o, k), shape=(2 * nc,)).view(np.complex128).reshape(shape).copy()
+                      for k in ("FUx", "FUy", "FUz", "Fn", "FPh")]
+            if callback is not None:
+                callback(o.step, o.t, o.kind, fields)
+
+        cfn = OUTPUT_FN(fn)
+        self._check(self.L.kf_run(self.h, iterations, dt, t0, slice_every, backup_every, cfn, None))
 
     def get_state(self, out=None):
         out = out or [np.empty(self.shape_c, np.complex128) for _ in range(4)]

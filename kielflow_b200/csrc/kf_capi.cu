@@ -49,6 +49,7 @@ struct LevelBuf {
 constexpr int RBS = 256;  // reduction block size
 
 struct AdjState;  // discrete-adjoint buffers (allocated by the first kf_adjoint_run)
+struct OutState;  // output buffers of kf_run / kf_get_output (allocated on first use)
 
 }  // namespace
 
@@ -114,6 +115,7 @@ struct kf_ctx {
     // discrete adjoint: buffers, job-list offsets, and the "phi given" switch
     // under which a right-hand side uses c->phi as it stands (no solve)
     AdjState *adj = nullptr;
+    OutState *out = nullptr;
     bool phi_given = false;
     int stage_idx = 0;  // RK stage of the right-hand side being evaluated (0..3)
     // one RK4 step captured as a CUDA graph (FAS or no Poisson, profile off):
@@ -1304,6 +1306,7 @@ template <typename F> int guarded(kf_ctx *c, F f) {
 }  // namespace
 
 #include "kf_adjoint_host.cuh"
+#include "kf_driver.cuh"
 
 // Message of the last failure that has no context (kf_ctx_create and the
 // context-free entry points); kf_last_error(NULL) returns it.
@@ -1341,6 +1344,7 @@ int kf_ctx_destroy(kf_ctx *c) {
     if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
     if (c->st_body) cudaStreamDestroy(c->st_body);
     adj_release(c);
+    out_release(c);
     for (void *p : c->allocs) cudaFree(p);
     if (c->h_red) cudaFreeHost(c->h_red);
     if (c->h_max) cudaFreeHost(c->h_max);

@@ -117,6 +117,16 @@ __global__ void k_rk(typename C2<T>::type *__restrict__ y0, typename C2<T>::type
     }
 }
 
+// x <- exp(x) (fn 0) or log(x) (fn 1) in place, evaluated in FP64: the
+// density's linear <-> log scale (kielflow.cpp:172-182, 293-296)
+template <typename T>
+__global__ void k_explog(T *__restrict__ x, int fn, long N) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const double v = (double)x[i];
+    x[i] = (T)(fn == 0 ? exp(v) : log(v));
+}
+
 // FP64 <-> bulk precision conversion of interleaved complex / real arrays
 template <typename T>
 __global__ void k_from_f64(T *__restrict__ dst, const double *__restrict__ src, long M) {
