@@ -166,9 +166,37 @@ typedef void (*kf_output_fn)(const kf_output *out, void *user);
  * The output fields are formed on the device and copied to pinned host memory
  * on a side stream while the next steps run; fn is called from this thread,
  * in step order, once an output's copy has finished (at most two are in
- * flight).  Returns after the last step and the last callback. */
+ * flight).  With out_dir, the files of the reference's loop are written there
+ * as well: slice_NNNN.kfh (step, 4 digits at least) and backup_at_STEP.kfh,
+ * in the format of kf_save.  Returns after the last step and the last
+ * callback. */
 int kf_run(kf_ctx *ctx, int iterations, double dt, double t0, int slice_every, int backup_every,
-           kf_output_fn fn, void *user);
+           const char *out_dir, kf_output_fn fn, void *user);
+
+/* Files.  The reference writes HDF5 (IO.cpp:60-505, 1295-1340): root datasets
+ * version, date, path, time; group domain with type_/m_/l0_/N_/L_ + axis
+ * letter; group parameters ("mach number M", "damping ratio tau",
+ * "temperature ratio theta", "velocity diffusion mu", "magnetization beta");
+ * group data with Ux, Uy, Uz, ni (linear density), Ph in real space -- the
+ * whole grid in a backup (save_all), the plane z = 0 in a slice (save_slice,
+ * index N*(0 - l0)/L).  HDF5 is not available to this library, so the same
+ * hierarchy is written as a .kfh container: "KFH1", u32 entry count, then per
+ * entry u16 name length, name (the HDF5 path, "data/Ux"), u8 type (1 f64,
+ * 2 i32, 3 string, 4 i64), u8 rank, u64 dims[rank], little-endian payload.
+ * "velocity diffusion mu" holds diff_D, "magnetization beta" 0. */
+#define KF_FILE_SLICE 1
+#define KF_FILE_BACKUP 2
+typedef struct {
+    int n;            /* N_x (= N_y = N_z required)                     */
+    int kind;         /* KF_FILE_SLICE (2-D data) or KF_FILE_BACKUP     */
+    double L, l0, time, M, tau, theta, mu, beta;
+} kf_file_info;
+int kf_file_info_read(const char *path, kf_file_info *info);
+/* write the context's current state (and phi) as a slice or backup file */
+int kf_save(kf_ctx *ctx, const char *path, int kind, double t);
+/* load a backup file into the state and phi (load_field_imag + the ln
+ * transform of kielflow.cpp:156-182); the grid must match the context's */
+int kf_load(kf_ctx *ctx, const char *path, double *t_out);
 
 /* Batched form of kf_rk4_steps for independent contexts (a parameter sweep;
  * grids may differ): dts[i] is context i's step.  One host thread queues every

@@ -86,6 +86,27 @@ class Output(ctypes.Structure):
 
 OUTPUT_FN = ctypes.CFUNCTYPE(None, ctypes.POINTER(Output), ctypes.c_void_p)
 KF_OUT_SLICE, KF_OUT_BACKUP = 1, 2
+KF_FILE_SLICE, KF_FILE_BACKUP = 1, 2
+
+
+class FileInfo(ctypes.Structure):
+    """kf_file_info (include/kielflow_b200.h)."""
+    _fields_ = [("n", ctypes.c_int), ("kind", ctypes.c_int), ("L", ctypes.c_double), ("l0", ctypes.c_double),
+                ("time", ctypes.c_double), ("M", ctypes.c_double), ("tau", ctypes.c_double),
+                ("theta", ctypes.c_double), ("mu", ctypes.c_double), ("beta", ctypes.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+def file_info(path: str) -> dict:
+    """kf_file_info_read: grid, time and parameters of a .kfh file (no GPU needed)."""
+    L = load_library()
+    info = FileInfo()
+    rc = L.kf_file_info_read(path.encode(), ctypes.byref(info))
+    if rc:
+        raise KfError(rc, L.kf_last_error(None).decode())
+    return info.as_dict()
 
 KF_ADJ_STORE_PHI = 1
 KF_ADJ_J_ONLY = 2
@@ -100,7 +121,8 @@ EXPORTS = [
     "kf_get_state", "kf_set_sources", "kf_set_phi", "kf_get_phi", "kf_rhs_eval", "kf_rk4_steps",
     "kf_poisson_solve", "kf_diag", "kf_fft_r2c", "kf_fft_c2r", "kf_state_device_ptrs", "kf_launch_count",
     "kf_profile_enable", "kf_profile_read", "kf_profile_class_name", "kf_fft_r2c_noalloc", "kf_adjoint_run",
-    "kf_batch_rk4_steps", "kf_set_state_linear", "kf_get_output", "kf_run",
+    "kf_batch_rk4_steps", "kf_set_state_linear", "kf_get_output", "kf_run", "kf_save", "kf_load",
+    "kf_file_info_read",
 ]
 KCLASSES = 18
 
@@ -146,7 +168,10 @@ def load_library():
     L.kf_set_state_linear.argtypes = [vp, _D, _D, _D, _D]
     L.kf_get_output.argtypes = [vp, _D, _D, _D, _D, _D]
     L.kf_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
-                         OUTPUT_FN, ctypes.c_void_p]
+                         ctypes.c_char_p, OUTPUT_FN, ctypes.c_void_p]
+    L.kf_save.argtypes = [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_double]
+    L.kf_load.argtypes = [vp, ctypes.c_char_p, _D]
+    L.kf_file_info_read.argtypes = [ctypes.c_char_p, ctypes.c_void_p]
     L.kf_batch_rk4_steps.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int, _D]
     L.kf_adjoint_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, _D,
                                  ctypes.POINTER(GradOut), _D, _D]
@@ -233,9 +258,10 @@ class Context:
         return out
 
     def run(self, iterations: int, dt: float, t0: float = 0.0, slice_every: int = 10, backup_every: int = 50,
-            callback=None):
+            callback=None, out_dir: str | None = None):
         """kf_run: the reference's time loop; callback(step, t, kind, fields) gets
-        copies of (FUx, FUy, FUz, Fn, FPh) at each output step."""
+        copies of (FUx, FUy, FUz, Fn, FPh) at each output step; with out_dir the
+        slice / backup .kfh files are written there."""
         nc = int(np.prod(self.shape_c))
         shape = self.shape_c
 
@@ -247,7 +273,18 @@ class Context:
                 callback(o.step, o.t, o.kind, fields)
 
         cfn = OUTPUT_FN(fn)
-        self._check(self.L.kf_run(self.h, iterations, dt, t0, slice_every, backup_every, cfn, None))
+        self._check(self.L.kf_run(self.h, iterations, dt, t0, slice_every, backup_every,
+                                  None if out_dir is None else out_dir.encode(), cfn, None))
+
+    def save(self, path: str, kind: int = KF_FILE_BACKUP, t: float = 0.0):
+        """kf_save: the current state as a slice or backup .kfh file."""
+        self._check(self.L.kf_save(self.h, path.encode(), kind, t))
+
+    def load(self, path: str) -> float:
+        """kf_load: a backup .kfh file into the state and phi; returns its time."""
+        t = ctypes.c_double()
+        self._check(self.L.kf_load(self.h, path.encode(), ctypes.byref(t)))
+        return t.value
 
     def get_state(self, out=None):
         out = out or [np.empty(self.shape_c, np.complex128) for _ in range(4)]

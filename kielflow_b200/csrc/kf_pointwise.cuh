@@ -127,6 +127,25 @@ __global__ void k_explog(T *__restrict__ x, int fn, long N) {
     x[i] = (T)(fn == 0 ? exp(v) : log(v));
 }
 
+// The real-space fields of an output file (IO.cpp save_field_imag and
+// save_slice write iFFT of the spectra): u'_c, n = exp(s) from the c2r of the
+// state, and phi, as FP64; all points (k0 < 0, o[q][id]) or the plane z
+// index k0 only (o[q][j + n i]).
+template <typename T>
+__global__ void k_out_real(const T *__restrict__ ux, const T *__restrict__ uy, const T *__restrict__ uz,
+                           const T *__restrict__ s, const double *__restrict__ phi, double *__restrict__ o0,
+                           double *__restrict__ o1, double *__restrict__ o2, double *__restrict__ o3,
+                           double *__restrict__ o4, int n, int k0, long M) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= M) return;
+    const long src = k0 >= 0 ? i * n + k0 : i;
+    o0[i] = (double)ux[src];
+    o1[i] = (double)uy[src];
+    o2[i] = (double)uz[src];
+    o3[i] = exp((double)s[src]);
+    o4[i] = phi[src];
+}
+
 // FP64 <-> bulk precision conversion of interleaved complex / real arrays
 template <typename T>
 __global__ void k_from_f64(T *__restrict__ dst, const double *__restrict__ src, long M) {

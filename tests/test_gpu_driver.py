@@ -73,3 +73,60 @@ def test_run_cadence_and_fields(name, over):
             want = ref.get_output()
         for a, b in zip(fields, want):
             assert np.array_equal(a, b)
+
+
+def test_save_and_load_backup(tmp_path):
+    ctx, st, dt = setup()
+    p = str(tmp_path / "backup.kfh")
+    with ctx:
+        ctx.rk4(dt, 2)
+        s = ctx.get_state()
+        phi = ctx.get_phi()
+        ctx.save(p, kf.KF_FILE_BACKUP, 0.75)
+    f = kf.kfh.read(p)
+    assert f["domain/N_x"] == 32 and f["time"] == 0.75 and f["domain/type_z"] == 1
+    assert f["parameters/mach number M"] == C.WORKLOADS["fas128"]["M"]
+    for q, name in enumerate(("Ux", "Uy", "Uz")):
+        assert rel(f[f"data/{name}"], bind.c2r(s[q])) < TOL
+    assert rel(f["data/ni"], np.exp(bind.c2r(s[3]))) < TOL
+    assert np.array_equal(f["data/Ph"], phi)
+    info = kf.file_info(p)
+    assert info["kind"] == kf.KF_FILE_BACKUP and info["n"] == 32
+    ctx2, _, _ = setup()
+    with ctx2:
+        assert ctx2.load(p) == 0.75
+        s2 = ctx2.get_state()
+        for q in range(3):
+            assert rel(s2[q], bind.r2c(bind.c2r(s[q]))) < TOL
+        assert rel(s2[3], bind.r2c(np.log(np.exp(bind.c2r(s[3]))))) < TOL
+        assert np.array_equal(ctx2.get_phi(), phi)
+
+
+def test_slice_is_the_z0_plane_of_the_backup(tmp_path):
+    ctx, st, dt = setup()
+    with ctx:
+        ctx.rk4(dt, 1)
+        ctx.save(str(tmp_path / "s.kfh"), kf.KF_FILE_SLICE, 0.0)
+        ctx.save(str(tmp_path / "b.kfh"), kf.KF_FILE_BACKUP, 0.0)
+    s = kf.kfh.read(str(tmp_path / "s.kfh"))
+    b = kf.kfh.read(str(tmp_path / "b.kfh"))
+    for name in ("Ux", "Uy", "Uz", "ni", "Ph"):
+        assert s[f"data/{name}"].shape == (32, 32)
+        assert np.array_equal(s[f"data/{name}"], b[f"data/{name}"][:, :, 16])  # index_at(0) = N/2
+
+
+def test_run_writes_the_reference_files(tmp_path):
+    ctx, st, dt = setup()
+    with ctx:
+        ctx.run(12, dt, t0=0.0, slice_every=3, backup_every=6, out_dir=str(tmp_path))
+    names = sorted(p.name for p in tmp_path.iterdir())
+    assert names == ["backup_at_6.kfh", "slice_0003.kfh", "slice_0006.kfh", "slice_0009.kfh"]
+    ref, _, _ = setup()
+    with ref:
+        ref.rk4(dt, 7)
+        ref.save(str(tmp_path / "ref.kfh"), kf.KF_FILE_BACKUP, 0.0)
+    a = kf.kfh.read(str(tmp_path / "backup_at_6.kfh"))
+    b = kf.kfh.read(str(tmp_path / "ref.kfh"))
+    for name in ("Ux", "Uy", "Uz", "ni", "Ph"):
+        assert np.array_equal(a[f"data/{name}"], b[f"data/{name}"])
+    assert a["time"] == sum([dt] * 6)  # t_total accumulated over 6 loop steps
