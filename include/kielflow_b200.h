@@ -198,6 +198,20 @@ int kf_save(kf_ctx *ctx, const char *path, int kind, double t);
  * transform of kielflow.cpp:156-182); the grid must match the context's */
 int kf_load(kf_ctx *ctx, const char *path, double *t_out);
 
+/* The frontend's initial state (frontend.cpp:255-330, create_input_from_
+ * MGsolver and the filtering after it) on the context's equidistant grid:
+ * phi solves lap phi = e^phi - (n_background + n_d) from phi = 0 with the
+ * context's Poisson solver and its n_d (kf_set_sources), n = exp(-theta phi),
+ * both filtered by exp(-2000 k~^15) in k-space, u' = 0; the state takes
+ * s^ = r2c(log n) (the load of kielflow.cpp:172-182) and phi the filtered
+ * potential.  The reference solves with n_background = 0; on a periodic box
+ * that equation has a solution only if the dust charge is positive (the box
+ * integral gives sum e^phi = sum n_d), so for a negative grain pass 1, the
+ * uniform ion density the right-hand side's rho = e^s + n_d has at s = 0.
+ * (The reference's frontend builds stretched axis_CoSiSt grids, which this
+ * library does not support.) */
+int kf_frontend_state(kf_ctx *ctx, double n_background);
+
 /* Batched form of kf_rk4_steps for independent contexts (a parameter sweep;
  * grids may differ): dts[i] is context i's step.  One host thread queues every
  * context's captured step on the context's own stream, step by step, so the

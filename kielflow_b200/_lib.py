@@ -122,7 +122,7 @@ EXPORTS = [
     "kf_poisson_solve", "kf_diag", "kf_fft_r2c", "kf_fft_c2r", "kf_state_device_ptrs", "kf_launch_count",
     "kf_profile_enable", "kf_profile_read", "kf_profile_class_name", "kf_fft_r2c_noalloc", "kf_adjoint_run",
     "kf_batch_rk4_steps", "kf_set_state_linear", "kf_get_output", "kf_run", "kf_save", "kf_load",
-    "kf_file_info_read",
+    "kf_file_info_read", "kf_frontend_state",
 ]
 KCLASSES = 18
 
@@ -169,6 +169,7 @@ def load_library():
     L.kf_get_output.argtypes = [vp, _D, _D, _D, _D, _D]
     L.kf_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                          ctypes.c_char_p, OUTPUT_FN, ctypes.c_void_p]
+    L.kf_frontend_state.argtypes = [vp, ctypes.c_double]
     L.kf_save.argtypes = [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_double]
     L.kf_load.argtypes = [vp, ctypes.c_char_p, _D]
     L.kf_file_info_read.argtypes = [ctypes.c_char_p, ctypes.c_void_p]
@@ -275,6 +276,10 @@ class Context:
         cfn = OUTPUT_FN(fn)
         self._check(self.L.kf_run(self.h, iterations, dt, t0, slice_every, backup_every,
                                   None if out_dir is None else out_dir.encode(), cfn, None))
+
+    def frontend_state(self, n_background: float = 1.0):
+        """kf_frontend_state: the frontend's initial state from the context's n_d."""
+        self._check(self.L.kf_frontend_state(self.h, n_background))
 
     def save(self, path: str, kind: int = KF_FILE_BACKUP, t: float = 0.0):
         """kf_save: the current state as a slice or backup .kfh file."""

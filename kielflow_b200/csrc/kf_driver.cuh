@@ -317,6 +317,63 @@ int kf_run(kf_ctx *c, int iterations, double dt, double t0, int slice_every, int
     return guarded(c, [&] { run_loop(c, iterations, dt, t0, slice_every, backup_every, out_dir, fn, user); });
 }
 
+// frontend.cpp:255-330 (create_input_from_MGsolver and what follows) on the
+// context's grid: phi from 0 with rho = n_background + n_d (the reference:
+// n_background = 0), n = exp(-theta phi), both filtered by exp(-2000 k~^15)
+// in k-space, u' = 0; the state takes s^ = r2c(log n) as kielflow.cpp:172-182
+// does on loading the file.
+int kf_frontend_state(kf_ctx *c, double n_background) {
+    return guarded(c, [&] {
+        const long N = c->N, Nc = c->Nc;
+        CK(cudaMemsetAsync(c->phi, 0, 8 * N, c->st));
+        {
+            Launch L_(c, KC_MISC, 16. * N);
+            k_add_const<<<nblk(N, 256), 256, 0, c->st>>>(c->rho, c->nd, n_background, N);
+        }
+        if (poisson(c)) throw KfError{KF_ERR_NOT_CONVERGED, "frontend Poisson solve did not reach its tolerance"};
+        auto filter = [&]() {  // CX[0] *= PF
+            Launch L_(c, KC_MISC, (2. * c->cs + c->es) * Nc);
+            if (c->fp32)
+                k_filter<float><<<nblk(Nc, 256), 256, 0, c->st>>>((float2 *)c->CX[0], (const float *)c->PF, Nc);
+            else
+                k_filter<double><<<nblk(Nc, 256), 256, 0, c->st>>>((double2 *)c->CX[0], (const double *)c->PF, Nc);
+        };
+        {
+            Launch L_(c, KC_MISC, (8. + c->es) * N);
+            if (c->fp32)
+                k_boltzmann<float><<<nblk(N, 256), 256, 0, c->st>>>((float *)c->R[0], c->phi, c->cfg.theta, N);
+            else
+                k_boltzmann<double><<<nblk(N, 256), 256, 0, c->st>>>((double *)c->R[0], c->phi, c->cfg.theta, N);
+        }
+        c->r2c_fn(c);
+        filter();
+        c->c2r_fn(c);
+        explog(c, c->R[0], 1);
+        c->r2c_fn(c);
+        CK(cudaMemcpyAsync(c->Y[3], c->CX[0], c->cs * Nc, cudaMemcpyDeviceToDevice, c->st));
+        if (c->fp32) {
+            Launch L_(c, KC_MISC, 12. * N);
+            k_from_f64<float><<<nblk(N, 256), 256, 0, c->st>>>((float *)c->R[0], c->phi, N);
+        } else {
+            CK(cudaMemcpyAsync(c->R[0], c->phi, 8 * N, cudaMemcpyDeviceToDevice, c->st));
+        }
+        c->r2c_fn(c);
+        filter();
+        c->c2r_fn(c);
+        if (c->fp32) {
+            Launch L_(c, KC_MISC, 12. * N);
+            k_to_f64<float><<<nblk(N, 256), 256, 0, c->st>>>(c->phi, (const float *)c->R[0], N);
+        } else {
+            CK(cudaMemcpyAsync(c->phi, c->R[0], 8 * N, cudaMemcpyDeviceToDevice, c->st));
+        }
+        for (int q = 0; q < 3; ++q) CK(cudaMemsetAsync(c->Y[q], 0, c->cs * Nc, c->st));
+        copy_state(c, c->Ys, c->Y);
+        c->nhist = 0;
+        CK(cudaStreamSynchronize(c->st));
+        CK(cudaGetLastError());
+    });
+}
+
 int kf_save(kf_ctx *c, const char *path, int kind, double t) {
     return guarded(c, [&] {
         if (!path || (kind != KF_FILE_SLICE && kind != KF_FILE_BACKUP)) throw KfError{KF_ERR_ARG, "kf_save: path, kind"};

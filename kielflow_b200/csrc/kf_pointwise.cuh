@@ -146,6 +146,32 @@ __global__ void k_out_real(const T *__restrict__ ux, const T *__restrict__ uy, c
     o4[i] = phi[src];
 }
 
+// rho = n_background + n_d (the frontend's Poisson source)
+__global__ void k_add_const(double *__restrict__ out, const double *__restrict__ in, double a, long N) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) out[i] = a + in[i];
+}
+
+// frontend.cpp:245-248: the Boltzmann ion density n = exp(-theta phi)
+template <typename T>
+__global__ void k_boltzmann(T *__restrict__ out, const double *__restrict__ phi, double theta, long N) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) out[i] = (T)exp(-theta * phi[i]);
+}
+
+// X *= f elementwise over a half spectrum (dealiasing_undesignated with a
+// precomputed filter table, operations.hpp:20-46)
+template <typename T>
+__global__ void k_filter(typename C2<T>::type *__restrict__ X, const T *__restrict__ f, long Nc) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= Nc) return;
+    typename C2<T>::type x = X[i];
+    const T w = f[i];
+    x.x *= w;
+    x.y *= w;
+    X[i] = x;
+}
+
 // FP64 <-> bulk precision conversion of interleaved complex / real arrays
 template <typename T>
 __global__ void k_from_f64(T *__restrict__ dst, const double *__restrict__ src, long M) {

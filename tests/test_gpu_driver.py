@@ -7,6 +7,7 @@ import pytest
 
 import kielflow_b200 as kf
 from kielflow_b200 import configs as C
+from kielflow_b200 import inputs as I
 from oracle import bind
 
 pytestmark = pytest.mark.gpu
@@ -130,3 +131,35 @@ def test_run_writes_the_reference_files(tmp_path):
     for name in ("Ux", "Uy", "Uz", "ni", "Ph"):
         assert np.array_equal(a[f"data/{name}"], b[f"data/{name}"])
     assert a["time"] == sum([dt] * 6)  # t_total accumulated over 6 loop steps
+
+
+def oracle_for(cfg):
+    return bind.Oracle(bind.KfoConfig(*[getattr(cfg, f) for f, _ in bind.KfoConfig._fields_]))
+
+
+@pytest.mark.parametrize("mode", [kf.KF_PS_FAS, kf.KF_PS_CASCADIC])
+def test_frontend_state_vs_oracle(mode):
+    """frontend.cpp:255-330 restated with the oracle's Poisson solver and
+    phi-filter table: phi from 0 with rho = 1 + n_d (a grain of charge -0.5
+    in the uniform ion background), n = exp(-theta phi), both filtered,
+    s^ = r2c(log n)."""
+    w = C.WORKLOADS["fas128"]
+    st, _, mask, dt = C.make_inputs(w, 32)
+    nd = I.gauss_charge(32, C.L_BOX, -0.5, 0.5)
+    cfg = C.config_for(w, 32, poisson_mode=mode)
+    o = oracle_for(cfg)
+    phi = o.poisson(np.zeros((32, 32, 32)), 1.0 + nd)
+    _, _, PF = o.tables()
+    n_f = bind.c2r(bind.r2c(np.exp(-cfg.theta * phi)) * PF)
+    phi_f = bind.c2r(bind.r2c(phi) * PF)
+    with kf.Context(cfg) as ctx:
+        ctx.set_state(*st)
+        ctx.set_sources(nd, mask)
+        ctx.frontend_state(1.0)
+        got = ctx.get_state()
+        assert rel(ctx.get_phi(), phi_f) < TOL
+        assert rel(got[3], bind.r2c(np.log(n_f))) < TOL
+        for q in range(3):
+            assert not np.any(got[q])
+        ctx.rk4(dt, 1)  # the state is a valid start
+        assert np.isfinite(ctx.get_phi()).all()
