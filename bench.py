@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison arm")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--cpu-ref", default="", help=argparse.SUPPRESS)
+    ap.add_argument("--marks", default="100,500,2000", help="steps at which --workload precision compares")
     ap.add_argument("--adjoint-steps", type=int, default=200,
                     help="RK4 steps of the adjoint leg (128^3 FP64, checkpoints every 15); 0 skips it")
     return ap.parse_args()
@@ -448,8 +450,121 @@ def run_sweep_bench(args):
     return 0
 
 
+def cpu_reference_run(n: int, steps: int, workload: str):
+    """The reference's own Runge_kutta_O4 + rhs_standard + cascadic multigrid
+    (its sources compiled into oracle/_ref) for `steps` RK4 steps of the
+    workload's initial state at n^3, one thread; prints seconds as JSON.  Run
+    in a subprocess: the reference keeps one grid size per process."""
+    from kielflow_b200 import configs as C
+    from oracle import bind  # CPU baseline leg only
+    if not bind.ref_available():
+        print(json.dumps({"unavailable": "oracle/_ref not built"}))
+        return 0
+    w = C.WORKLOADS[workload]
+    st, nd, mask, dt = C.make_inputs(w, n)
+    with _QuietStdout():
+        R = bind.Reference(n, C.L_BOX, w["M"], w["tau"], C.THETA, poisson_mode=1)
+        R.set_real(0, nd)
+        R.set_real(1, mask)
+        R.set_state(st)
+        t0 = time.perf_counter()
+        R.rk4(dt, steps)
+        sec = time.perf_counter() - t0
+    print(json.dumps({"n": n, "steps": steps, "seconds": sec, "s_per_step": sec / steps}))
+    return 0
+
+
+def run_small(args):
+    """The smaller configurations: plain FP64 GPU steps/s at 32^3 (Jacobi to
+    1e-10) and 128^3 (FAS 4 levels 2+2), and the reference's CPU path on the
+    same inputs (subprocesses, one core), for the baseline table."""
+    import subprocess
+
+    import kielflow_b200 as kf
+    from kielflow_b200 import configs as C
+
+    out = {"workload": "small", "gpu": {}, "cpu_reference": {}}
+    for name, steps in (("jacobi32", 100), ("fas128", 20)):
+        w = C.WORKLOADS[name]
+        st, nd, mask, dt = C.make_inputs(w)
+        with kf.Context(C.config_for(w)) as ctx:
+            ctx.set_state(*st)
+            ctx.set_sources(nd, mask)
+            ctx.rk4(dt, 3)
+            ctx.synchronize()
+            t0 = time.perf_counter()
+            ctx.rk4(dt, steps)
+            ctx.synchronize()
+            sec = time.perf_counter() - t0
+        out["gpu"][name] = {"steps": steps, "seconds": sec, "steps_per_s": steps / sec,
+                            "timing": "host wall clock around a synchronised run"}
+    if not args.no_cpu:
+        for name, n, steps in (("jacobi32", 32, 100), ("fas128", 128, 2)):
+            r = subprocess.run([sys.executable, __file__, "--cpu-ref", f"{n},{steps},{name}"],
+                               capture_output=True, text=True, timeout=900)
+            line = [x for x in r.stdout.splitlines() if x.startswith("{")]
+            out["cpu_reference"][name] = json.loads(line[-1]) if line else {"unavailable": r.stderr[-300:]}
+        out["cpu_reference"]["note"] = ("the reference's own RK4 + rhs_standard + cascadic multigrid "
+                                        "(kielflow.cpp's solver plan), single thread")
+    print(json.dumps(out))
+    return 0
+
+
+def run_precision(args):
+    """FP32 bulk against plain FP64 on the 256^3 precision workload: relative
+    L2 and max-norm errors of n = exp(s), u' and phi after 100, 500 and 2000
+    steps of the same seeded run."""
+    import numpy as np
+
+    import kielflow_b200 as kf
+    from kielflow_b200 import configs as C
+
+    w = C.WORKLOADS["fp32bulk256"]
+    st, nd, mask, dt = C.make_inputs(w)
+    n = w["n"]
+    ctxs = {}
+    for p in (kf.KF_FP32_BULK, kf.KF_FP64):
+        c = kf.Context(C.config_for(w, precision=p))
+        c.set_state(*st)
+        c.set_sources(nd, mask)
+        ctxs[p] = c
+    marks = [int(x) for x in args.marks.split(",")]
+    done, rows = 0, []
+
+    def real(F):
+        return np.fft.irfftn(F, s=(n, n, n), axes=(0, 1, 2))
+
+    def errs(a, b):
+        d = a - b
+        return {"l2": float(np.sqrt((d * d).sum() / (b * b).sum())), "linf": float(np.abs(d).max() / np.abs(b).max())}
+
+    for m in marks:
+        for c in ctxs.values():
+            c.rk4(dt, m - done)
+        done = m
+        s32, s64 = ctxs[kf.KF_FP32_BULK].get_state(), ctxs[kf.KF_FP64].get_state()
+        row = {"step": m,
+               "n": errs(np.exp(real(s32[3])), np.exp(real(s64[3]))),
+               "u": errs(np.stack([real(x) for x in s32[:3]]), np.stack([real(x) for x in s64[:3]])),
+               "phi": errs(ctxs[kf.KF_FP32_BULK].get_phi(), ctxs[kf.KF_FP64].get_phi())}
+        rows.append(row)
+        print(json.dumps(row), file=sys.stderr, flush=True)
+    for c in ctxs.values():
+        c.close()
+    print(json.dumps({"workload": "precision: fp32bulk256 vs fp64_256, same seed", "dt": dt, "errors": rows,
+                      "note": "u is the perturbation u' (relative to its own size)"}))
+    return 0
+
+
 def main():
     args = parse()
+    if args.cpu_ref:
+        n, steps, name = args.cpu_ref.split(",")
+        return cpu_reference_run(int(n), int(steps), name)
+    if args.workload == "small":
+        return run_small(args)
+    if args.workload == "precision":
+        return run_precision(args)
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "sweep48":
