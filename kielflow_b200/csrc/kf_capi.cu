@@ -11,6 +11,7 @@
 //   F  forward z/y passes, then the forward x pass fused with the assembly
 //      K_q = -(lin_q + F_q)   (or P F_q with penalization)
 // RK4 (RKO4.cpp:50-241) combines four such evaluations with k_rk.
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -552,6 +553,8 @@ template <typename T, int N> struct Impl {
         const int big = 200 * 1024;
         CK(cudaFuncSetAttribute(k_axis_pass<T, N, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
         CK(cudaFuncSetAttribute(k_axis_pass<T, N, +1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+        CK(cudaFuncSetAttribute(k_axis_pipe<T, N, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+        CK(cudaFuncSetAttribute(k_axis_pipe<T, N, +1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
         CK(cudaFuncSetAttribute(k_z_c2r<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
         CK(cudaFuncSetAttribute(k_z_r2c<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
         CK(cudaFuncSetAttribute(k_xfwd_assemble<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
@@ -568,14 +571,32 @@ template <typename T, int N> struct Impl {
         }
         return (double)(u.size() + njobs) * c->Nc * sizeof(T2);
     }
+    // resident blocks per SM x SMs of the pipelined pass (its grid)
+    static int pipe_grid(int sign) {
+        static int g[2] = {0, 0};
+        int &v = g[sign > 0];
+        if (!v) {
+            int dev = 0, sms = 0, per = 0;
+            CK(cudaGetDevice(&dev));
+            CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            const size_t smem = 2 * (size_t)N * TC * sizeof(T2);
+            if (sign < 0)
+                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_axis_pipe<T, N, -1>, TC * P, smem));
+            else
+                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_axis_pipe<T, N, +1>, TC * P, smem));
+            v = (per > 0 ? per : 1) * sms;
+        }
+        return v;
+    }
     static void axis(kf_ctx *c, int off, int njobs, int ax, int sign) {
         const int ntiles = ax == 0 ? (N * NZC + TC - 1) / TC : N * ((NZC + TC - 1) / TC);
-        const size_t smem = (size_t)N * TC * sizeof(T2);
         Launch L_(c, sign > 0 ? KC_AXIS_INV : KC_AXIS_FWD, job_bytes(c, off, njobs));
+        const int total = njobs * ntiles, grid = std::min(total, pipe_grid(sign));
+        const size_t smem = 2 * (size_t)N * TC * sizeof(T2);
         if (sign < 0)
-            k_axis_pass<T, N, -1><<<njobs * ntiles, TC * P, smem, c->st>>>(c->dj + off, njobs, ax, geo(c), (const T2 *)c->tw);
+            k_axis_pipe<T, N, -1><<<grid, TC * P, smem, c->st>>>(c->dj + off, njobs, ax, geo(c), (const T2 *)c->tw, total);
         else
-            k_axis_pass<T, N, +1><<<njobs * ntiles, TC * P, smem, c->st>>>(c->dj + off, njobs, ax, geo(c), (const T2 *)c->tw);
+            k_axis_pipe<T, N, +1><<<grid, TC * P, smem, c->st>>>(c->dj + off, njobs, ax, geo(c), (const T2 *)c->tw, total);
     }
     static double z_bytes(kf_ctx *c, int off, int njobs, bool c2r) {
         std::vector<const void *> u;

@@ -158,15 +158,24 @@ template <int... Rs> struct Last;
 template <int R> struct Last<R> { static constexpr int value = R; };
 template <int R, int R2, int... Rest> struct Last<R, R2, Rest...> { static constexpr int value = Last<R2, Rest...>::value; };
 
+// Twiddle table W_N^m: in global memory (read through the read-only path) or
+// staged in shared memory by a persistent kernel.
+template <typename T2> __device__ __forceinline__ T2 tw_load(const T2 *__restrict__ tw, int m) { return __ldg(tw + m); }
+template <typename T2> struct SharedTw {
+    const T2 *p;
+};
+template <typename T2> __device__ __forceinline__ T2 tw_load(SharedTw<T2> tw, int m) { return tw.p[m]; }
+
 // Stages of one line.  v: E registers; sm: this line's shared-memory column
-// (element r at sm[r*stride]); tw: W_N table (global, read through L1).
+// (element r at sm[r*stride]); tw: W_N table (global, read through L1, or a
+// SharedTw).
 template <typename T2, int N, int P, int SIGN, int Ns, int R, int... Rest>
 struct Stages {
     static constexpr int E = N / P;
     static constexpr int NB = N / (P * R);
     static_assert(NB * P * R == N, "radix does not tile the line");
-    template <typename A>
-    __device__ __forceinline__ static void run(T2 *v, T2 *sm, A addr, int p, const T2 *__restrict__ tw) {
+    template <typename A, typename TW>
+    __device__ __forceinline__ static void run(T2 *v, T2 *sm, A addr, int p, TW tw) {
 #pragma unroll
         for (int b = 0; b < NB; ++b) {
             const int j = p + b * P;
@@ -175,7 +184,7 @@ struct Stages {
 #pragma unroll
                 for (int t = 1; t < R; ++t) {
                     const int m = (t * k * (N / (Ns * R))) % N;
-                    T2 w = __ldg(tw + m);
+                    T2 w = tw_load(tw, m);
                     if (SIGN > 0) w.y = -w.y;
                     v[b * R + t] = cmul(v[b * R + t], w);
                 }
@@ -204,8 +213,8 @@ struct Stages {
     }
 };
 
-template <typename T2, int N, int P, int SIGN, int... Rs, typename A>
-__device__ __forceinline__ void fft_line(T2 *v, T2 *sm, A addr, int p, const T2 *__restrict__ tw) {
+template <typename T2, int N, int P, int SIGN, int... Rs, typename A, typename TW>
+__device__ __forceinline__ void fft_line(T2 *v, T2 *sm, A addr, int p, TW tw) {
     Stages<T2, N, P, SIGN, 1, Rs...>::run(v, sm, addr, p, tw);
 }
 
@@ -218,15 +227,15 @@ __device__ __forceinline__ int reg_row(int p, int q) {
 
 // Per-length launch plans: threads per line P and the radix sequence.
 template <int N> struct Plan;
-template <> struct Plan<16> { static constexpr int P = 4; template <typename T2, int S, typename A> __device__ static void fft(T2 *v, T2 *sm, A a, int p, const T2 *tw) { fft_line<T2, 16, 4, S, 4, 4>(v, sm, a, p, tw); } static constexpr int R1 = 4, RL = 4; };
-template <> struct Plan<32> { static constexpr int P = 4; template <typename T2, int S, typename A> __device__ static void fft(T2 *v, T2 *sm, A a, int p, const T2 *tw) { fft_line<T2, 32, 4, S, 8, 4>(v, sm, a, p, tw); } static constexpr int R1 = 8, RL = 4; };
-template <> struct Plan<64> { static constexpr int P = 8; template <typename T2, int S, typename A> __device__ static void fft(T2 *v, T2 *sm, A a, int p, const T2 *tw) { fft_line<T2, 64, 8, S, 8, 8>(v, sm, a, p, tw); } static constexpr int R1 = 8, RL = 8; };
-template <> struct Plan<96> { static constexpr int P = 8; template <typename T2, int S, typename A> __device__ static void fft(T2 *v, T2 *sm, A a, int p, const T2 *tw) { fft_line<T2, 96, 8, S, 6, 4, 4>(v, sm, a, p, tw); } static constexpr int R1 = 6, RL = 4; };
-template <> struct Plan<128> { static constexpr int P = 8; template <typename T2, int S, typename A> __device__ static void fft(T2 *v, T2 *sm, A a, int p, const T2 *tw) { fft_line<T2, 128, 8, S, 16, 8>(v, sm, a, p, tw); } static constexpr int R1 = 16, RL = 8; };
+template <> struct Plan<16> { static constexpr int P = 4; template <typename T2, int S, typename A, typename TW> __device__ static void fft(T2 *v, T2 *sm, A a, int p, TW tw) { fft_line<T2, 16, 4, S, 4, 4>(v, sm, a, p, tw); } static constexpr int R1 = 4, RL = 4; };
+template <> struct Plan<32> { static constexpr int P = 4; template <typename T2, int S, typename A, typename TW> __device__ static void fft(T2 *v, T2 *sm, A a, int p, TW tw) { fft_line<T2, 32, 4, S, 8, 4>(v, sm, a, p, tw); } static constexpr int R1 = 8, RL = 4; };
+template <> struct Plan<64> { static constexpr int P = 8; template <typename T2, int S, typename A, typename TW> __device__ static void fft(T2 *v, T2 *sm, A a, int p, TW tw) { fft_line<T2, 64, 8, S, 8, 8>(v, sm, a, p, tw); } static constexpr int R1 = 8, RL = 8; };
+template <> struct Plan<96> { static constexpr int P = 8; template <typename T2, int S, typename A, typename TW> __device__ static void fft(T2 *v, T2 *sm, A a, int p, TW tw) { fft_line<T2, 96, 8, S, 6, 4, 4>(v, sm, a, p, tw); } static constexpr int R1 = 6, RL = 4; };
+template <> struct Plan<128> { static constexpr int P = 8; template <typename T2, int S, typename A, typename TW> __device__ static void fft(T2 *v, T2 *sm, A a, int p, TW tw) { fft_line<T2, 128, 8, S, 16, 8>(v, sm, a, p, tw); } static constexpr int R1 = 16, RL = 8; };
 #ifdef KF_PLAN256_P32
-template <> struct Plan<256> { static constexpr int P = 32; template <typename T2, int S, typename A> __device__ static void fft(T2 *v, T2 *sm, A a, int p, const T2 *tw) { fft_line<T2, 256, 32, S, 8, 8, 4>(v, sm, a, p, tw); } static constexpr int R1 = 8, RL = 4; };
+template <> struct Plan<256> { static constexpr int P = 32; template <typename T2, int S, typename A, typename TW> __device__ static void fft(T2 *v, T2 *sm, A a, int p, TW tw) { fft_line<T2, 256, 32, S, 8, 8, 4>(v, sm, a, p, tw); } static constexpr int R1 = 8, RL = 4; };
 #else
-template <> struct Plan<256> { static constexpr int P = 16; template <typename T2, int S, typename A> __device__ static void fft(T2 *v, T2 *sm, A a, int p, const T2 *tw) { fft_line<T2, 256, 16, S, 16, 16>(v, sm, a, p, tw); } static constexpr int R1 = 16, RL = 16; };
+template <> struct Plan<256> { static constexpr int P = 16; template <typename T2, int S, typename A, typename TW> __device__ static void fft(T2 *v, T2 *sm, A a, int p, TW tw) { fft_line<T2, 256, 16, S, 16, 16>(v, sm, a, p, tw); } static constexpr int R1 = 16, RL = 16; };
 #endif
 
 }  // namespace kf

@@ -91,6 +91,120 @@ k_axis_pass(const AxisJob *__restrict__ jobs, int njobs, int axis, Geo<T> g,
     }
 }
 
+// ------------------------------------------------- pipelined x / y pass
+// The x / y pass as a persistent kernel: each block walks tiles t, t + grid,
+// ... and while tile t is transformed in registers, the loads of the next
+// tile are in flight as cp.async copies into a staging buffer (shared memory
+// beside the exchange buffer).  Every thread stages exactly the elements it
+// later reads, so the staging buffer needs no barrier; the exchange buffer
+// keeps the FFT's own.  Same tiles, multipliers, transforms and stores as
+// k_axis_pass, so the same results.
+__device__ __forceinline__ void cp_async_copy(void *smem, const float2 *g) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async_copy(void *smem, const double2 *g) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+template <typename T> struct AxisTile {
+    typedef typename C2<T>::type T2;
+    const T2 *in;
+    T2 *out;
+    long base, rstride;
+    int jj, kk, mul;
+    bool valid;
+};
+
+template <typename T, int N>
+__device__ __forceinline__ AxisTile<T> axis_tile(const AxisJob *__restrict__ jobs, int njobs, int axis, int t,
+                                                 int c, int n, int nzc) {
+    typedef typename C2<T>::type T2;
+    constexpr int TC = Tile<T>::TC;
+    AxisTile<T> G;
+    const int job = t % njobs, tile = t / njobs;
+    const AxisJob J = jobs[job];
+    G.in = static_cast<const T2 *>(J.in);
+    G.out = static_cast<T2 *>(J.out);
+    G.mul = J.mul;
+    G.jj = 0;
+    G.kk = 0;
+    if (axis == 0) {
+        const int col = tile * TC + c;
+        G.valid = col < n * nzc;
+        G.base = col;
+        G.rstride = (long)n * nzc;
+        G.jj = col / nzc;
+        G.kk = col - G.jj * nzc;
+    } else {
+        const int tpp = (nzc + TC - 1) / TC;
+        const int plane = tile / tpp;
+        G.kk = (tile - plane * tpp) * TC + c;
+        G.valid = G.kk < nzc;
+        G.base = (long)plane * n * nzc + G.kk;
+        G.rstride = nzc;
+    }
+    return G;
+}
+
+template <typename T, int N, int SIGN>
+__global__ void __launch_bounds__(Tile<T>::TC * Plan<N>::P)
+k_axis_pipe(const AxisJob *__restrict__ jobs, int njobs, int axis, Geo<T> g,
+            const typename C2<T>::type *__restrict__ tw, int total) {
+    typedef typename C2<T>::type T2;
+    constexpr int TC = Tile<T>::TC, P = Plan<N>::P, E = N / P;
+    extern __shared__ __align__(16) unsigned char kf_smem[];
+    T2 *sm = reinterpret_cast<T2 *>(kf_smem);  // exchange [N][TC]
+    T2 *stg = sm + N * TC;                      // staging  [N][TC]
+    const int c = threadIdx.x % TC, p = threadIdx.x / TC;
+    int t = blockIdx.x;
+    if (t >= total) return;
+    auto prefetch = [&](const AxisTile<T> &G) {
+#pragma unroll
+        for (int q = 0; q < E; ++q) {
+            const int row = reg_row<N, P, Plan<N>::R1>(p, q);
+            T2 *dst = stg + row * TC + c;
+            if (G.valid)
+                cp_async_copy(dst, G.in + G.base + row * G.rstride);
+            else
+                *dst = mk<T2>((T)0, (T)0);
+        }
+        cp_async_commit();
+    };
+    AxisTile<T> cur = axis_tile<T, N>(jobs, njobs, axis, t, c, g.n, g.nzc);
+    prefetch(cur);
+    for (; t < total; t += gridDim.x) {
+        const int tn = t + gridDim.x;
+        AxisTile<T> nxt = cur;
+        if (tn < total) nxt = axis_tile<T, N>(jobs, njobs, axis, tn, c, g.n, g.nzc);
+        cp_async_wait_all();
+        T2 v[E];
+#pragma unroll
+        for (int q = 0; q < E; ++q) {
+            const int row = reg_row<N, P, Plan<N>::R1>(p, q);
+            T2 x = stg[row * TC + c];
+            if (cur.mul == MUL_P || cur.mul == MUL_P_IK) {
+                if (!dealias_keep(g.q2, g.thr, row, cur.jj, cur.kk)) x = mk<T2>((T)0, (T)0);
+            }
+            if (cur.mul == MUL_P_IK || cur.mul == MUL_IK) x = mul_ik(x, g.kv[row]);
+            v[q] = x;
+        }
+        if (tn < total) prefetch(nxt);
+        Plan<N>::template fft<T2, SIGN>(v, sm + c, StrideAddr{TC}, p, tw);
+        if (cur.valid) {
+#pragma unroll
+            for (int q = 0; q < E; ++q) {
+                const int row = reg_row<N, P, Plan<N>::RL>(p, q);
+                cur.out[cur.base + row * cur.rstride] = v[q];
+            }
+        }
+        cur = nxt;
+    }
+}
+
 // --------------------------------------------------------------- z c2r pass
 // LZ line pairs per block; thread = p + P*l.  Half rows are staged in shared
 // memory, multiplied, extended by Hermitian symmetry (the imaginary parts of
