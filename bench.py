@@ -565,6 +565,10 @@ def main():
         return run_small(args)
     if args.workload == "precision":
         return run_precision(args)
+    if args.workload == "adjoint":  # the adjoint leg alone (profiling runs)
+        import torch
+        print(json.dumps({"workload": "adjoint", "adjoint": adjoint_leg(args.adjoint_steps, torch.cuda.Stream())}))
+        return 0
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "sweep48":

@@ -54,7 +54,7 @@ struct ProdVjpArgs {
 };
 
 template <int BS>
-__global__ void __launch_bounds__(BS) k_prod_vjp(ProdVjpArgs a) {
+__global__ void __launch_bounds__(BS, 3) k_prod_vjp(ProdVjpArgs a) {
     __shared__ double sh[4 * BS];
     double acc[4] = {0., 0., 0., 0.};
     const bool pen = a.terms & T_PENALIZATION, adv = a.terms & T_ADVECTION, cont = a.terms & T_CONTINUITY;
@@ -107,7 +107,7 @@ struct VjpAsmArgs {
 };
 
 template <int BS>
-__global__ void __launch_bounds__(BS) k_vjp_assemble(VjpAsmArgs a, Geo<double> g) {
+__global__ void __launch_bounds__(BS, 3) k_vjp_assemble(VjpAsmArgs a, Geo<double> g) {
     __shared__ double sh[4 * BS];
     double acc[4] = {0., 0., 0., 0.};
     const long Nc = (long)g.n * g.n * g.nzc;

@@ -25,9 +25,6 @@ def test_library_exports_every_declared_symbol():
     lib = _lib.load_library()
     for sym in declared_symbols():
         assert hasattr(lib, sym), sym
-    # the CUDA kernels are in the library (sm_100a cubin)
-    data = open(_lib.library_path(), "rb").read()
-    assert b"k_axis_pass" in data and b"k_z_c2r" in data
 
 
 def test_context_creation_fails_loudly_without_a_b200():
