@@ -327,9 +327,7 @@ def run_kf(args):
     with torch.cuda.stream(stream):
         e0.record(stream)
         for _ in range(args.e2e_steps):
-            ctx32.set_state(*host)
-            ctx32.rk4(dt, 1)
-            ctx32.get_state(host)
+            ctx32.step_host(host, dt, 1)  # interface_ode_solver::solve on host arrays
         e1.record(stream)
     stream.synchronize()
     ms_e2e = max_over_ranks(e0.elapsed_time(e1))

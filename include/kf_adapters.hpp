@@ -89,9 +89,8 @@ class kf_gpu_rk4 : public interface_ode_solver {
 public:
     kf_gpu_rk4(kf_gpu_rhs &rhs, double dt = 0.01) : ctx_(rhs.context()), dt_(dt) {}
     void solve(field_imag &FUx, field_imag &FUy, field_imag &FUz, field_imag &Fni) {
-        kf_adapt::check(ctx_, kf_set_state(ctx_, &FUx.val[0][0], &FUy.val[0][0], &FUz.val[0][0], &Fni.val[0][0]));
-        kf_adapt::check(ctx_, kf_rk4_steps(ctx_, 1, dt_));
-        kf_adapt::check(ctx_, kf_get_state(ctx_, &FUx.val[0][0], &FUy.val[0][0], &FUz.val[0][0], &Fni.val[0][0]));
+        kf_adapt::check(ctx_, kf_step_host(ctx_, 1, dt_, &FUx.val[0][0], &FUy.val[0][0], &FUz.val[0][0],
+                                           &Fni.val[0][0]));
     }
 
 private:

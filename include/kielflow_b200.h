@@ -212,6 +212,15 @@ int kf_load(kf_ctx *ctx, const char *path, double *t_out);
  * library does not support.) */
 int kf_frontend_state(kf_ctx *ctx, double n_background);
 
+/* interface_ode_solver::solve on host arrays, in place (the reference's call:
+ * RKO4.cpp:50-241 on field_imag data): set the state from the four arrays,
+ * advance nsteps steps, write the result back; returns when the result is
+ * in the arrays.  With the captured step, u' is uploaded on a second stream
+ * while stage 1 solves its Poisson problem (which needs s only), so most of
+ * the upload is hidden; page-locked host arrays are needed for the overlap
+ * (pageable ones work, without it). */
+int kf_step_host(kf_ctx *ctx, int nsteps, double dt, double *FUx, double *FUy, double *FUz, double *Fni);
+
 /* Batched form of kf_rk4_steps for independent contexts (a parameter sweep;
  * grids may differ): dts[i] is context i's step.  One host thread queues every
  * context's captured step on the context's own stream, step by step, so the

@@ -122,7 +122,7 @@ EXPORTS = [
     "kf_poisson_solve", "kf_diag", "kf_fft_r2c", "kf_fft_c2r", "kf_state_device_ptrs", "kf_launch_count",
     "kf_profile_enable", "kf_profile_read", "kf_profile_class_name", "kf_fft_r2c_noalloc", "kf_adjoint_run",
     "kf_batch_rk4_steps", "kf_set_state_linear", "kf_get_output", "kf_run", "kf_save", "kf_load",
-    "kf_file_info_read", "kf_frontend_state",
+    "kf_file_info_read", "kf_frontend_state", "kf_step_host",
 ]
 KCLASSES = 18
 
@@ -170,6 +170,7 @@ def load_library():
     L.kf_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                          ctypes.c_char_p, OUTPUT_FN, ctypes.c_void_p]
     L.kf_frontend_state.argtypes = [vp, ctypes.c_double]
+    L.kf_step_host.argtypes = [vp, ctypes.c_int, ctypes.c_double, _D, _D, _D, _D]
     L.kf_save.argtypes = [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_double]
     L.kf_load.argtypes = [vp, ctypes.c_char_p, _D]
     L.kf_file_info_read.argtypes = [ctypes.c_char_p, ctypes.c_void_p]
@@ -314,6 +315,14 @@ class Context:
     # ---- the hot path --------------------------------------------------
     def rhs(self, t: float = 0.0):
         self._check(self.L.kf_rhs_eval(self.h, t))
+
+    def step_host(self, arrays, dt: float, nsteps: int = 1):
+        """kf_step_host: advance the state held in four host arrays (complex128,
+        C-contiguous, updated in place)."""
+        for a in arrays:
+            if a.shape != self.shape_c or a.dtype != np.complex128 or not a.flags["C_CONTIGUOUS"]:
+                raise ValueError(f"state arrays must be C-contiguous complex128 {self.shape_c}")
+        self._check(self.L.kf_step_host(self.h, nsteps, dt, *[a.ctypes.data_as(_D) for a in arrays]))
 
     def rk4(self, dt: float, nsteps: int = 1):
         self._check(self.L.kf_rk4_steps(self.h, nsteps, dt))

@@ -127,6 +127,13 @@ struct kf_ctx {
     DevPois *dpois = nullptr;
     DevPois hpois{};  // last values read back
     cudaGraphExec_t step_graph = nullptr;
+    // the same step whose stage 1 waits for ev_u (the u' upload of kf_step_host)
+    // after its Poisson solve, before the first use of u'
+    cudaGraphExec_t step_graph_wait = nullptr;
+    bool capture_wait_u = false;
+    cudaStream_t st_copy = nullptr;
+    cudaEvent_t ev_u = nullptr;
+    double *stage64b = nullptr;  // FP32-bulk staging of the copy stream
     double step_dt = 0.;
     long long step_kernels = 0, cycle_kernels = 0;
     int jV_x = 0, jV_y = 0, zV = 0, zW = 0, nWz = 0, nWf = 0, jW_y = 0, jW_x = 0, zS = 0, jS_y = 0, jS_x = 0;
@@ -673,6 +680,8 @@ template <typename T, int N> struct Impl {
             }
         }
         // B
+        if (c->capturing && c->capture_wait_u && c->stage_idx == 0)
+            CK(cudaStreamWaitEvent(c->st, c->ev_u, cudaEventWaitExternal));
         if (Tm & T_E_INT) {
             if (c->fp32) {
                 Launch L_(c, KC_MISC, (double)c->N * (8 + sizeof(T)));
@@ -1213,13 +1222,23 @@ bool graph_path(kf_ctx *c) {
 }
 
 // Capture one RK4 step (the sequence of rk4_step) with device-side stage
-// times, warm starts and convergence loops.
-void build_step_graph(kf_ctx *c, double dt) {
-    if (c->step_graph && c->step_dt == dt) return;
-    if (c->step_graph) {
+// times, warm starts and convergence loops; with wait_u, stage 1 waits for
+// ev_u after its Poisson solve.
+void capture_step(kf_ctx *c, double dt, bool wait_u, cudaGraphExec_t *out);
+
+void build_step_graph(kf_ctx *c, double dt, bool with_wait = false) {
+    if (c->step_graph && c->step_dt != dt) {
         cudaGraphExecDestroy(c->step_graph);
         c->step_graph = nullptr;
+        if (c->step_graph_wait) cudaGraphExecDestroy(c->step_graph_wait);
+        c->step_graph_wait = nullptr;
     }
+    if (!c->step_graph) capture_step(c, dt, false, &c->step_graph);
+    if (with_wait && !c->step_graph_wait) capture_step(c, dt, true, &c->step_graph_wait);
+    c->step_dt = dt;
+}
+
+void capture_step(kf_ctx *c, double dt, bool wait_u, cudaGraphExec_t *out) {
     const double xs[4] = {0., 0.5 * dt, 0.5 * dt, 1.0 * dt};
     const double cdt[4] = {0.5 * dt, 0.5 * dt, 1.0 * dt, dt / 6.};
     const int mode[4] = {0, 1, 1, 2};
@@ -1228,6 +1247,7 @@ void build_step_graph(kf_ctx *c, double dt) {
     const long long l0 = c->launches;
     c->cycle_kernels = 0;
     c->capturing = true;
+    c->capture_wait_u = wait_u;
     CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
     try {
         for (int i = 0; i < 4; ++i) {
@@ -1249,19 +1269,20 @@ void build_step_graph(kf_ctx *c, double dt) {
         cudaStreamEndCapture(c->st, &g);
         if (g) cudaGraphDestroy(g);
         c->capturing = false;
+        c->capture_wait_u = false;
         c->launches = l0;
         throw;
     }
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(c->st, &g);
     c->capturing = false;
+    c->capture_wait_u = false;
     CK(e);
-    e = cudaGraphInstantiate(&c->step_graph, g, 0);
+    e = cudaGraphInstantiate(out, g, 0);
     cudaGraphDestroy(g);
     CK(e);
     c->step_kernels = c->launches - l0 - (pois ? 4 * c->cycle_kernels : 0);
     c->launches = l0;
-    c->step_dt = dt;
 }
 
 // nsteps replays of the step graph; the host's time and warm-start record is
@@ -1308,6 +1329,42 @@ void rk4_steps_graph(kf_ctx *c, int nsteps, double dt) {
     graph_begin(c, dt);
     for (int s = 0; s < nsteps; ++s) graph_step(c);
     graph_end(c);
+}
+
+// interface_ode_solver::solve with the state in host arrays, in place: the
+// upload of s goes first on the compute stream; u' is uploaded on a copy
+// stream while stage 1's Poisson solve runs (the captured step of the first
+// step waits for it just before it needs u'); the result is copied back.
+void step_host(kf_ctx *c, int nsteps, double dt, double *const *host) {
+    if (!c->st_copy) {
+        CK(cudaStreamCreateWithFlags(&c->st_copy, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&c->ev_u, cudaEventDisableTiming));
+        if (c->fp32) c->stage64b = dalloc<double>(c, 16 * (size_t)c->Nc);
+    }
+    build_step_graph(c, dt, true);
+    put_bulk(c, c->Y[3], host[3], 2 * c->Nc);
+    CK(cudaMemcpyAsync(c->Ys[3], c->Y[3], c->cs * c->Nc, cudaMemcpyDeviceToDevice, c->st));
+    for (int q = 0; q < 3; ++q) {
+        if (!c->fp32) {
+            CK(cudaMemcpyAsync(c->Y[q], host[q], 16 * c->Nc, cudaMemcpyHostToDevice, c->st_copy));
+        } else {
+            CK(cudaMemcpyAsync(c->stage64b, host[q], 16 * c->Nc, cudaMemcpyHostToDevice, c->st_copy));
+            const long M = 2 * c->Nc;
+            Launch L_(c, KC_MISC, 12. * M);
+            k_from_f64<float><<<nblk(M, 256), 256, 0, c->st_copy>>>((float *)c->Y[q], c->stage64b, M);
+        }
+        CK(cudaMemcpyAsync(c->Ys[q], c->Y[q], c->cs * c->Nc, cudaMemcpyDeviceToDevice, c->st_copy));
+    }
+    CK(cudaEventRecord(c->ev_u, c->st_copy));
+    c->nhist = 0;  // as kf_set_state
+    DevTime ht{c->t, c->t_stage, c->tau_a, c->tau_b, c->nhist, 0, 0, 0};
+    CK(cudaMemcpyAsync(c->dtime, &ht, sizeof(DevTime), cudaMemcpyHostToDevice, c->st));
+    CK(cudaGraphLaunch(c->step_graph_wait, c->st));
+    c->launches += c->step_kernels;
+    for (int s = 1; s < nsteps; ++s) graph_step(c);
+    graph_end(c);
+    for (int q = 0; q < 4; ++q) get_bulk(c, host[q], c->Y[q], 2 * c->Nc);
+    CK(cudaStreamSynchronize(c->st));
 }
 
 template <typename F> int guarded(kf_ctx *c, F f) {
@@ -1363,6 +1420,9 @@ int kf_ctx_destroy(kf_ctx *c) {
     for (auto e : c->evfree) cudaEventDestroy(e);
     if (c->vgraph) cudaGraphExecDestroy(c->vgraph);
     if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+    if (c->step_graph_wait) cudaGraphExecDestroy(c->step_graph_wait);
+    if (c->ev_u) cudaEventDestroy(c->ev_u);
+    if (c->st_copy) cudaStreamDestroy(c->st_copy);
     if (c->st_body) cudaStreamDestroy(c->st_body);
     adj_release(c);
     out_release(c);
@@ -1445,6 +1505,24 @@ int kf_rhs_eval(kf_ctx *c, double t) {
         c->rhs_fn(c);
         copy_state(c, c->Y, c->K);
         copy_state(c, c->Ys, c->K);
+        CK(cudaStreamSynchronize(c->st));
+    });
+}
+
+int kf_step_host(kf_ctx *c, int nsteps, double dt, double *ux, double *uy, double *uz, double *s) {
+    return guarded(c, [&] {
+        if (!ux || !uy || !uz || !s) throw KfError{KF_ERR_ARG, "null state array"};
+        if (nsteps < 0) throw KfError{KF_ERR_ARG, "nsteps < 0"};
+        double *host[4] = {ux, uy, uz, s};
+        if (nsteps > 0 && graph_path(c)) {
+            step_host(c, nsteps, dt, host);
+            return;
+        }
+        for (int q = 0; q < 4; ++q) put_bulk(c, c->Y[q], host[q], 2 * c->Nc);
+        copy_state(c, c->Ys, c->Y);
+        c->nhist = 0;
+        for (int k = 0; k < nsteps; ++k) rk4_step(c, dt, nullptr, nullptr, nullptr);
+        for (int q = 0; q < 4; ++q) get_bulk(c, host[q], c->Y[q], 2 * c->Nc);
         CK(cudaStreamSynchronize(c->st));
     });
 }

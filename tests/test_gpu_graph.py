@@ -60,3 +60,27 @@ def test_graph_step_in_pieces():
     for a, b in zip(out[0][0], out[1][0]):
         assert np.array_equal(a, b)
     assert np.array_equal(out[0][1], out[1][1])
+
+
+@pytest.mark.parametrize("name,nsteps", [("fas128", 1), ("fas128", 3), ("fp32bulk256", 2), ("jacobi32", 2)])
+def test_step_host_matches_set_step_get(name, nsteps):
+    """kf_step_host (u' uploaded while stage 1 solves its Poisson problem)
+    against kf_set_state + kf_rk4_steps + kf_get_state: identical results."""
+    w = C.WORKLOADS[name]
+    st, nd, mask, dt = C.make_inputs(w, 32)
+    out = []
+    for host_call in (True, False):
+        with kf.Context(C.config_for(w, 32)) as ctx:
+            ctx.set_sources(nd, mask)
+            arrays = [np.ascontiguousarray(x).copy() for x in st]
+            for _ in range(2):  # twice: the second call starts from the first's phi
+                if host_call:
+                    ctx.step_host(arrays, dt, nsteps)
+                else:
+                    ctx.set_state(*arrays)
+                    ctx.rk4(dt, nsteps)
+                    arrays = ctx.get_state()
+            out.append((arrays, ctx.get_phi()))
+    for a, b in zip(out[0][0], out[1][0]):
+        assert np.array_equal(a, b)
+    assert np.array_equal(out[0][1], out[1][1])
