@@ -40,7 +40,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="kf", choices=["kf", "reference"])
     ap.add_argument("--workload", default="fp32bulk256")
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=8)
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison arm")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--cpu-ref", default="", help=argparse.SUPPRESS)
@@ -334,8 +334,23 @@ def run_kf(args):
     bytes_io = 4 * int(np.prod(shape_c)) * 16
     e2e = None
     if args.e2e_steps > 0:
+        # this box's page-locked copy bandwidth, for reading the number
+        hb = torch.empty(bytes_io // 8, dtype=torch.float64, pin_memory=True)
+        db = torch.empty(bytes_io // 8, dtype=torch.float64, device="cuda")
+        c0, c1, c2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        with torch.cuda.stream(stream):
+            c0.record(stream)
+            db.copy_(hb, non_blocking=True)
+            c1.record(stream)
+            hb.copy_(db, non_blocking=True)
+            c2.record(stream)
+        stream.synchronize()
         e2e = {"value": ws * args.e2e_steps / (ms_e2e / 1000.0), "unit": UNIT, "h2d_bytes_per_step": bytes_io,
-               "d2h_bytes_per_step": bytes_io}
+               "d2h_bytes_per_step": bytes_io, "steps": args.e2e_steps,
+               "call": "kf_step_host (interface_ode_solver::solve on page-locked host arrays)",
+               "link_h2d_GBps": bytes_io / (c0.elapsed_time(c1) * 1e6),
+               "link_d2h_GBps": bytes_io / (c1.elapsed_time(c2) * 1e6)}
+        del hb, db
     ctx32.close()
     del ctx32
 

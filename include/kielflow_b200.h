@@ -252,7 +252,7 @@ long long kf_launch_count(const kf_ctx *ctx);
 /* Kernel profile: when enabled, every launch is bracketed by CUDA events on the
  * context's stream and its algorithmic bytes (distinct inputs + outputs) are
  * recorded per kernel class; enabling or disabling resets the totals.
- * Classes 0..17; kf_profile_class_name gives the kernel name of each. */
+ * Classes 0..18; kf_profile_class_name gives the kernel name of each. */
 int kf_profile_enable(kf_ctx *ctx, int on);
 int kf_profile_read(kf_ctx *ctx, int cls, double *ms, long long *launches, double *bytes);
 const char *kf_profile_class_name(int cls);

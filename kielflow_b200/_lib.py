@@ -124,7 +124,7 @@ EXPORTS = [
     "kf_batch_rk4_steps", "kf_set_state_linear", "kf_get_output", "kf_run", "kf_save", "kf_load",
     "kf_file_info_read", "kf_frontend_state", "kf_step_host",
 ]
-KCLASSES = 18
+KCLASSES = 19
 
 _lib = None
 

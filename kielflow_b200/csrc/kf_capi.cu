@@ -154,13 +154,15 @@ inline int nblk(long work, int bs) { return (int)((work + bs - 1) / bs); }
 // Kernel classes for the profile (kf_profile_read); names in kf_profile_class_name.
 enum KCls { KC_AXIS_INV, KC_AXIS_FWD, KC_Z_C2R, KC_Z_R2C, KC_XASM, KC_PROD, KC_LIN, KC_RHO, KC_RK,
             KC_JACOBI, KC_RBGS, KC_RESID, KC_TRANSFER, KC_COARSE, KC_REDUCE, KC_MISC, KC_ADJ_PW, KC_ADJ_MG,
+            KC_MG_COARSE,
             KC_N };
 const char *const kKClsName[KC_N] = {"k_axis_pass(inverse)", "k_axis_pass(forward)", "k_z_c2r", "k_z_r2c",
                                      "k_xfwd_assemble", "k_products", "k_lin", "k_rho", "k_rk", "k_jacobi",
                                      "k_rbgs", "k_residual", "k_restrict/k_fas_rhs/k_prolong/k_inject",
                                      "k_coarse_solve", "k_reduce_final", "conversion/diagnostics",
                                      "adjoint pointwise (k_prod_vjp/k_vjp_assemble/k_adj_stage/...)",
-                                     "adjoint Poisson (linear multigrid)"};
+                                     "adjoint Poisson (linear multigrid)",
+                                     "FAS levels below the finest (k_rbgs/k_residual/transfers)"};
 
 void prof_flush(kf_ctx *c) {
     if (c->recs.empty()) return;
@@ -335,31 +337,31 @@ void vcycle(kf_ctx *c, int l) {
                                                                    c->d_sweeps);
         return;
     }
-    smooth(c, L, L.phi, L.rho, nullptr, cf.mg_pre, KC_RBGS);
+    smooth(c, L, L.phi, L.rho, nullptr, cf.mg_pre, l == 0 ? KC_RBGS : KC_MG_COARSE);
     {
-        Launch L_(c, KC_RESID, 24. * N);
+        Launch L_(c, l == 0 ? KC_RESID : KC_MG_COARSE, 24. * N);
         k_residual<true><<<mg_grid(n, n), mg_block(), 0, c->st>>>(L.phi, L.rho, L.lev(), L.r);
     }
     LevelBuf &Lc = c->lv[l + 1];
     const long Nc3 = (long)Lc.n * Lc.n * Lc.n;
     {
-        Launch L_(c, KC_TRANSFER, 8. * N + 32. * Nc3);
+        Launch L_(c, l == 0 ? KC_TRANSFER : KC_MG_COARSE, 8. * N + 32. * Nc3);
         k_restrict<<<mg_grid(Lc.n, Lc.n), mg_block(), 0, c->st>>>(L.r, L.phi, n, Lc.r, Lc.phi, Lc.phi0);
     }
     {
-        Launch L_(c, KC_TRANSFER, 24. * Nc3);
+        Launch L_(c, l == 0 ? KC_TRANSFER : KC_MG_COARSE, 24. * Nc3);
         k_fas_rhs<<<mg_grid(Lc.n, Lc.n), mg_block(), 0, c->st>>>(Lc.phi, Lc.r, Lc.lev(), Lc.rho);
     }
     vcycle(c, l + 1);
     {
-        Launch L_(c, KC_TRANSFER, 24. * Nc3);
+        Launch L_(c, l == 0 ? KC_TRANSFER : KC_MG_COARSE, 24. * Nc3);
         k_correction<<<mg_grid(Lc.n, Lc.n), mg_block(), 0, c->st>>>(Lc.phi, Lc.phi0, Lc.n);
     }
     {
-        Launch L_(c, KC_TRANSFER, 16. * N + 8. * Nc3);
+        Launch L_(c, l == 0 ? KC_TRANSFER : KC_MG_COARSE, 16. * N + 8. * Nc3);
         k_prolong_add<<<mg_grid(Lc.n, Lc.n), mg_block(), 0, c->st>>>(L.phi, Lc.phi0, nullptr, L.gam, n);
     }
-    smooth(c, L, L.phi, L.rho, nullptr, cf.mg_post, KC_RBGS);
+    smooth(c, L, L.phi, L.rho, nullptr, cf.mg_post, l == 0 ? KC_RBGS : KC_MG_COARSE);
     CK(cudaGetLastError());
 }
 
