@@ -284,6 +284,7 @@ def run_kf(args):
         ctx.set_stream(stream.cuda_stream)
         ctx.set_state(*st)
         ctx.set_sources(nd, mask)
+        tune = ctx.autotune()  # radix plan and smoother shape, timed on this context
         ctx.rk4(dt, args.warmup)
         ctx.synchronize()
         barrier()
@@ -311,6 +312,7 @@ def run_kf(args):
             ctx.rk4(dt, max(1, min(args.steps, 3)))
             prof = ctx.profile_read()
             ctx.profile(False)
+        ctx.tune = tune
         return ctx, ms, launches, prof, clk, d, phi
 
     ctx32, ms32, launches, prof, clk, d32, phi32 = timed_arm(w["precision"], profile=True, clocks=True)
@@ -351,18 +353,22 @@ def run_kf(args):
                "link_h2d_GBps": bytes_io / (c0.elapsed_time(c1) * 1e6),
                "link_d2h_GBps": bytes_io / (c1.elapsed_time(c2) * 1e6)}
         del hb, db
+    tune32 = ctx32.tune
     ctx32.close()
     del ctx32
 
     fp64 = None
     if not args.no_fp64 and w["precision"] != kf.KF_FP64:
         ctx64, ms64, _, _, _, d64, phi64 = timed_arm(kf.KF_FP64)
+        tune64 = ctx64.tune
         ctx64.close()
         err = float(np.abs(phi32 - phi64).max() / np.abs(phi64).max())
         fp64 = {"value": ws * args.steps / (ms64 / 1000.0), "ms_per_step": ms64 / args.steps,
                 "phi_rel_err_fp32_vs_fp64": max_over_ranks(err),
                 "charge_fp32": d32.charge, "charge_fp64": d64.charge,
-                "kinetic_fp32": d32.kinetic, "kinetic_fp64": d64.kinetic}
+                "kinetic_fp32": d32.kinetic, "kinetic_fp64": d64.kinetic,
+                "tuning": {"fft_radices": tune64["fft_radices"][tune64["fft_plan"]],
+                           "rbgs_rows": tune64["rbgs_rows"]}}
 
     adj = adjoint_leg(args.adjoint_steps, stream) if args.adjoint_steps > 0 else None
 
@@ -400,7 +406,9 @@ def run_kf(args):
                                f"Q {w['Q']}, sigma {w['sigma']}, FAS 4 levels 2+2 to 1e-10, penalization, "
                                f"diffusion 1e-3, SV > 0.6 k_max",
                    "n": w["n"], "dt": dt, "l2": "inputs larger than L2 (state + work buffers > 2 GB)",
-                   "parallelism": f"replicas x{ws}"},
+                   "parallelism": f"replicas x{ws}",
+                   "tuning": {"fft_radices": tune32["fft_radices"][tune32["fft_plan"]],
+                              "rbgs_rows": tune32["rbgs_rows"]}},
         "gpu_launches": launches,
         "roofline": roofline,
         "cpu_baseline": cpu,
@@ -435,13 +443,14 @@ def run_sweep_bench(args):
     mine = [inst[i] for i in kdist.partition([x.n for x in inst], ws)[rank]]
     if ws > 1:
         torch.distributed.barrier()
-    wall_c, _, dg = run_sweep(mine, steps=args.steps, mode="batched", warmup=args.warmup)
+    tunings = {}
+    wall_c, _, dg = run_sweep(mine, steps=args.steps, mode="batched", warmup=args.warmup, tunings=tunings)
     wall_c = kdist.max_over_ranks(wall_c, device="cuda")
     wall_s = wall_t = None
     if not args.no_fp64:  # the sequential reference run (skipped with --no-fp64 to save time)
-        wall_s, _, _ = run_sweep(mine, steps=args.steps, mode="sequential", warmup=args.warmup)
+        wall_s, _, _ = run_sweep(mine, steps=args.steps, mode="sequential", warmup=args.warmup, tune=tunings)
         wall_s = kdist.max_over_ranks(wall_s, device="cuda")
-        wall_t, _, _ = run_sweep(mine, steps=args.steps, mode="threads", warmup=args.warmup)
+        wall_t, _, _ = run_sweep(mine, steps=args.steps, mode="threads", warmup=args.warmup, tune=tunings)
         wall_t = kdist.max_over_ranks(wall_t, device="cuda")
     if rank == 0:
         total = len(inst) * args.steps
@@ -453,7 +462,9 @@ def run_sweep_bench(args):
                                       "Q ~ U[-50,-5] (seed 0); FP32 bulk, FP64 FAS Poisson",
                           "timing": "host wall clock around fully synchronised runs; warm-up steps "
                                     "(graph capture) outside", "batched": "kf_batch_rk4_steps",
-                          "sequential": "kf_rk4_steps per instance, one after another"},
+                          "sequential": "kf_rk4_steps per instance, one after another",
+                          "tuning": {str(n): {"fft_radices": t["fft_radices"][t["fft_plan"]],
+                                              "rbgs_rows": t["rbgs_rows"]} for n, t in sorted(tunings.items())}},
                "sequential_value": (total / wall_s) if wall_s else None,
                "threads_value": (total / wall_t) if wall_t else None,
                "batched_over_sequential": (wall_s / wall_c) if wall_s else None}

@@ -230,6 +230,33 @@ int kf_step_host(kf_ctx *ctx, int nsteps, double dt, double *FUx, double *FUy, d
  * in kf_last_error(that context) and kf_last_error(NULL). */
 int kf_batch_rk4_steps(kf_ctx *const *ctxs, int nctx, int nsteps, const double *dts);
 
+/* Kernel variants of a context (no reference counterpart: the reference's
+ * FFTW plans are chosen by FFTW_MEASURE inside fftw_plan_dft_*, OP_FFT.cpp).
+ * fft_plan: radix plan of every transform kernel, 0 or 1 (two factorisations
+ * of each supported n into radix stages, with different threads per line);
+ * rbgs_rows: rows per block of the red-black smoother, 4, 8 or 16.  Results
+ * do not depend on rbgs_rows (same arithmetic per point) and agree between
+ * the fft plans to rounding. */
+typedef struct kf_tune_out {
+    int fft_plan;          /* chosen radix plan */
+    int rbgs_rows;         /* chosen rows per smoother block */
+    int fft_radices[2][4]; /* radix stages of plans 0 and 1 (0 = unused) */
+    int fft_threads[2];    /* threads per transformed line of plans 0 and 1 */
+    double fft_ms[2];      /* one right-hand side without its Poisson solve, per plan */
+    double rbgs_ms[3];     /* one finest-level smoothing sweep with 4, 8, 16 rows */
+} kf_tune_out;
+
+/* Time the variants on the context's own buffers (reps timed calls each,
+ * reps <= 0: 5), keep the fastest of each kind and drop the context's captured
+ * graphs so they are rebuilt with the choices.  The state, the potential and
+ * the time are unchanged (the right-hand side runs with the potential held,
+ * the smoother sweeps a copy of it).  out may be NULL. */
+int kf_autotune(kf_ctx *ctx, int reps, kf_tune_out *out);
+
+/* Set the variants directly (the values kf_autotune reports; e.g. one tuning
+ * applied to every instance of a sweep).  KF_ERR_ARG for other values. */
+int kf_set_tuning(kf_ctx *ctx, int fft_plan, int rbgs_rows);
+
 /* interface_poisson_solver::solve (interface_poisson_solver.hpp:18): phi_io is
  * the initial guess and the result, rho is read only; host arrays, n^3 doubles. */
 int kf_poisson_solve(kf_ctx *ctx, double *phi_io, const double *rho);

@@ -25,7 +25,7 @@ from ._lib import (  # noqa: F401
     KF_FP32_BULK, KF_FP64, KF_PS_CASCADIC, KF_PS_FAS, KF_PS_JACOBI_REF, KF_PS_JACOBI_RES, KF_T_ADVECTION,
     KF_T_CONTINUITY, KF_T_DIFFUSION, KF_T_DISSIPATION, KF_T_E_EXT, KF_T_E_INT, KF_T_PENALIZATION,
     KF_T_POISSON, KF_T_PRESSURE, KF_T_SHIPPED, KF_T_SVISCOSITY, KF_T_ALL, KF_ADJ_J_ONLY, KF_ADJ_STORE_PHI, Config,
-    Context, GradOut, KfError, batch_rk4, file_info, load_library, library_path, KF_FILE_SLICE, KF_FILE_BACKUP,
+    Context, GradOut, TuneOut, KfError, batch_rk4, file_info, load_library, library_path, KF_FILE_SLICE, KF_FILE_BACKUP,
     KF_OUT_SLICE, KF_OUT_BACKUP,
 )
 from .interfaces import Grid, Parameters, PoissonSolver, RhsStandard, RungeKuttaO4  # noqa: F401

@@ -78,6 +78,17 @@ class GradOut(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class TuneOut(ctypes.Structure):
+    """kf_tune_out (include/kielflow_b200.h)."""
+    _fields_ = [("fft_plan", ctypes.c_int), ("rbgs_rows", ctypes.c_int), ("fft_radices", (ctypes.c_int * 4) * 2),
+                ("fft_threads", ctypes.c_int * 2), ("fft_ms", ctypes.c_double * 2), ("rbgs_ms", ctypes.c_double * 3)]
+
+    def as_dict(self):
+        return {"fft_plan": self.fft_plan, "rbgs_rows": self.rbgs_rows,
+                "fft_radices": [[r for r in row if r] for row in self.fft_radices],
+                "fft_threads": list(self.fft_threads), "fft_ms": list(self.fft_ms), "rbgs_ms": list(self.rbgs_ms)}
+
+
 class Output(ctypes.Structure):
     """kf_output (include/kielflow_b200.h)."""
     _fields_ = [("step", ctypes.c_int), ("t", ctypes.c_double), ("kind", ctypes.c_int),
@@ -122,7 +133,7 @@ EXPORTS = [
     "kf_poisson_solve", "kf_diag", "kf_fft_r2c", "kf_fft_c2r", "kf_state_device_ptrs", "kf_launch_count",
     "kf_profile_enable", "kf_profile_read", "kf_profile_class_name", "kf_fft_r2c_noalloc", "kf_adjoint_run",
     "kf_batch_rk4_steps", "kf_set_state_linear", "kf_get_output", "kf_run", "kf_save", "kf_load",
-    "kf_file_info_read", "kf_frontend_state", "kf_step_host",
+    "kf_file_info_read", "kf_frontend_state", "kf_step_host", "kf_autotune", "kf_set_tuning",
 ]
 KCLASSES = 19
 
@@ -175,6 +186,8 @@ def load_library():
     L.kf_load.argtypes = [vp, ctypes.c_char_p, _D]
     L.kf_file_info_read.argtypes = [ctypes.c_char_p, ctypes.c_void_p]
     L.kf_batch_rk4_steps.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int, _D]
+    L.kf_autotune.argtypes = [vp, ctypes.c_int, ctypes.POINTER(TuneOut)]
+    L.kf_set_tuning.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     L.kf_adjoint_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, _D,
                                  ctypes.POINTER(GradOut), _D, _D]
     _lib = L
@@ -323,6 +336,17 @@ class Context:
             if a.shape != self.shape_c or a.dtype != np.complex128 or not a.flags["C_CONTIGUOUS"]:
                 raise ValueError(f"state arrays must be C-contiguous complex128 {self.shape_c}")
         self._check(self.L.kf_step_host(self.h, nsteps, dt, *[a.ctypes.data_as(_D) for a in arrays]))
+
+    def autotune(self, reps: int = 5) -> dict:
+        """kf_autotune: time the transform plans and smoother shapes on this
+        context's buffers, keep the fastest; returns the choices and timings."""
+        o = TuneOut()
+        self._check(self.L.kf_autotune(self.h, reps, ctypes.byref(o)))
+        return o.as_dict()
+
+    def set_tuning(self, fft_plan: int, rbgs_rows: int):
+        """kf_set_tuning: select the transform plan (0, 1) and smoother rows (4, 8, 16)."""
+        self._check(self.L.kf_set_tuning(self.h, fft_plan, rbgs_rows))
 
     def rk4(self, dt: float, nsteps: int = 1):
         self._check(self.L.kf_rk4_steps(self.h, nsteps, dt))

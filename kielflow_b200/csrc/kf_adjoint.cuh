@@ -279,10 +279,11 @@ __global__ void __launch_bounds__(BS) k_dot_w(const double *__restrict__ w, cons
 // forward solver: the point equation A - D psi - c psi = 0 (A = 2 sum w psi_nb + b)
 // is linear, so the "Newton step" is the exact point solve psi = A / (D + c).
 
-__global__ void __launch_bounds__(256) k_rbgs_lin(double *__restrict__ phi, const double *__restrict__ rho,
-                                                  const double *__restrict__ cl, Lev L, int color) {
+template <int BY = 8>
+__global__ void __launch_bounds__(32 * BY) k_rbgs_lin(double *__restrict__ phi, const double *__restrict__ rho,
+                                                      const double *__restrict__ cl, Lev L, int color) {
     const int n = L.n;
-    const int k2 = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, i = blockIdx.z;
+    const int k2 = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * BY + threadIdx.y, i = blockIdx.z;
     if (2 * k2 >= n || j >= n) return;
     const int k = 2 * k2 + ((i + j + color) & 1);
     double A, D;

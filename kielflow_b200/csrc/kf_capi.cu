@@ -118,6 +118,8 @@ struct kf_ctx {
     AdjState *adj = nullptr;
     OutState *out = nullptr;
     bool phi_given = false;
+    int fftv = 0;     // radix-plan variant of the transform kernels (kf_autotune)
+    int rbgs_by = 8;  // rows per block of the red-black smoother (kf_autotune)
     int stage_idx = 0;  // RK stage of the right-hand side being evaluated (0..3)
     // one RK4 step captured as a CUDA graph (FAS or no Poisson, profile off):
     // time / warm-start history and solve statistics live on the device
@@ -315,13 +317,26 @@ int jacobi_solve(kf_ctx *c, const LevelBuf &L, double *phi, double *tmp, const d
 void smooth(kf_ctx *c, LevelBuf &L, double *phi, const double *rho, const double *cc, int sweeps, int cls) {
     const int n = L.n;
     const long N = (long)n * n * n;
+    const int by = c->rbgs_by;
+    const dim3 g((n / 2 + 31) / 32, (n + by - 1) / by, n), b(32, by);
     for (int s = 0; s < sweeps; ++s)
         for (int color = 0; color < 2; ++color) {
             Launch L_(c, cls, 16. * N);
-            if (cc)
-                k_rbgs_lin<<<mg_grid(n / 2, n), mg_block(), 0, c->st>>>(phi, rho, cc, L.lev(), color);
-            else
-                k_rbgs<<<mg_grid(n / 2, n), mg_block(), 0, c->st>>>(phi, rho, L.lev(), color);
+            if (cc) {
+                if (by == 4)
+                    k_rbgs_lin<4><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color);
+                else if (by == 16)
+                    k_rbgs_lin<16><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color);
+                else
+                    k_rbgs_lin<8><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color);
+            } else {
+                if (by == 4)
+                    k_rbgs<4><<<g, b, 0, c->st>>>(phi, rho, L.lev(), color);
+                else if (by == 16)
+                    k_rbgs<16><<<g, b, 0, c->st>>>(phi, rho, L.lev(), color);
+                else
+                    k_rbgs<8><<<g, b, 0, c->st>>>(phi, rho, L.lev(), color);
+            }
         }
 }
 
@@ -552,7 +567,8 @@ void poisson_captured(kf_ctx *c) {
 // ------------------------------------------------------------------ per-(T, N) implementation
 template <typename T, int N> struct Impl {
     typedef typename C2<T>::type T2;
-    static constexpr int TC = Tile<T>::TC, P = Plan<N>::P, LZ = ZTile<T>::LZ, NZC = N / 2 + 1;
+    static constexpr int TC = Tile<T>::TC, LZ = ZTile<T>::LZ, NZC = N / 2 + 1;
+    template <int V> static constexpr int PV = PlanV<N, V>::P;
 
     static Geo<T> geo(kf_ctx *c) { return Geo<T>{c->n, c->nzc, (const T *)c->kv, c->q2, dealias_threshold()}; }
 
@@ -562,12 +578,17 @@ template <typename T, int N> struct Impl {
         const int big = 200 * 1024;
         CK(cudaFuncSetAttribute(k_axis_pass<T, N, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
         CK(cudaFuncSetAttribute(k_axis_pass<T, N, +1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-        CK(cudaFuncSetAttribute(k_axis_pipe<T, N, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-        CK(cudaFuncSetAttribute(k_axis_pipe<T, N, +1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-        CK(cudaFuncSetAttribute(k_z_c2r<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-        CK(cudaFuncSetAttribute(k_z_r2c<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-        CK(cudaFuncSetAttribute(k_xfwd_assemble<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+        set_attrs_v<0>(big);
+        set_attrs_v<1>(big);
         done = true;
+    }
+
+    template <int V> static void set_attrs_v(int big) {
+        CK(cudaFuncSetAttribute(k_axis_pipe<T, N, -1, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+        CK(cudaFuncSetAttribute(k_axis_pipe<T, N, +1, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+        CK(cudaFuncSetAttribute(k_z_c2r<T, N, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+        CK(cudaFuncSetAttribute(k_z_r2c<T, N, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+        CK(cudaFuncSetAttribute(k_xfwd_assemble<T, N, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     }
 
     static double job_bytes(kf_ctx *c, int off, int njobs) {
@@ -581,7 +602,7 @@ template <typename T, int N> struct Impl {
         return (double)(u.size() + njobs) * c->Nc * sizeof(T2);
     }
     // resident blocks per SM x SMs of the pipelined pass (its grid)
-    static int pipe_grid(int sign) {
+    template <int V> static int pipe_grid(int sign) {
         static int g[2] = {0, 0};
         int &v = g[sign > 0];
         if (!v) {
@@ -590,22 +611,30 @@ template <typename T, int N> struct Impl {
             CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
             const size_t smem = 2 * (size_t)N * TC * sizeof(T2);
             if (sign < 0)
-                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_axis_pipe<T, N, -1>, TC * P, smem));
+                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_axis_pipe<T, N, -1, V>, TC * PV<V>, smem));
             else
-                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_axis_pipe<T, N, +1>, TC * P, smem));
+                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_axis_pipe<T, N, +1, V>, TC * PV<V>, smem));
             v = (per > 0 ? per : 1) * sms;
         }
         return v;
     }
-    static void axis(kf_ctx *c, int off, int njobs, int ax, int sign) {
+    template <int V> static void axis_v(kf_ctx *c, int off, int njobs, int ax, int sign) {
         const int ntiles = ax == 0 ? (N * NZC + TC - 1) / TC : N * ((NZC + TC - 1) / TC);
-        Launch L_(c, sign > 0 ? KC_AXIS_INV : KC_AXIS_FWD, job_bytes(c, off, njobs));
-        const int total = njobs * ntiles, grid = std::min(total, pipe_grid(sign));
+        const int total = njobs * ntiles, grid = std::min(total, pipe_grid<V>(sign));
         const size_t smem = 2 * (size_t)N * TC * sizeof(T2);
         if (sign < 0)
-            k_axis_pipe<T, N, -1><<<grid, TC * P, smem, c->st>>>(c->dj + off, njobs, ax, geo(c), (const T2 *)c->tw, total);
+            k_axis_pipe<T, N, -1, V><<<grid, TC * PV<V>, smem, c->st>>>(c->dj + off, njobs, ax, geo(c),
+                                                                      (const T2 *)c->tw, total);
         else
-            k_axis_pipe<T, N, +1><<<grid, TC * P, smem, c->st>>>(c->dj + off, njobs, ax, geo(c), (const T2 *)c->tw, total);
+            k_axis_pipe<T, N, +1, V><<<grid, TC * PV<V>, smem, c->st>>>(c->dj + off, njobs, ax, geo(c),
+                                                                      (const T2 *)c->tw, total);
+    }
+    static void axis(kf_ctx *c, int off, int njobs, int ax, int sign) {
+        Launch L_(c, sign > 0 ? KC_AXIS_INV : KC_AXIS_FWD, job_bytes(c, off, njobs));
+        if (c->fftv)
+            axis_v<1>(c, off, njobs, ax, sign);
+        else
+            axis_v<0>(c, off, njobs, ax, sign);
     }
     static double z_bytes(kf_ctx *c, int off, int njobs, bool c2r) {
         std::vector<const void *> u;
@@ -630,15 +659,23 @@ template <typename T, int N> struct Impl {
         const size_t smem = (size_t)(2 * LZ * NZC > LZ * PadLen<N>::value ? 2 * LZ * NZC : LZ * PadLen<N>::value) *
                             sizeof(T2);
         Launch L_(c, KC_Z_C2R, z_bytes(c, off, njobs, true));
-        k_z_c2r<T, N><<<njobs * ntiles, LZ * P, smem, c->st>>>(c->dz + off, njobs, nrows, geo(c), (const T2 *)c->tw,
-                                                             (T)(scale < 0. ? 1. / ((double)N * N * N) : scale));
+        const T sc = (T)(scale < 0. ? 1. / ((double)N * N * N) : scale);
+        if (c->fftv)
+            k_z_c2r<T, N, 1><<<njobs * ntiles, LZ * PV<1>, smem, c->st>>>(c->dz + off, njobs, nrows, geo(c),
+                                                                        (const T2 *)c->tw, sc);
+        else
+            k_z_c2r<T, N, 0><<<njobs * ntiles, LZ * PV<0>, smem, c->st>>>(c->dz + off, njobs, nrows, geo(c),
+                                                                        (const T2 *)c->tw, sc);
     }
     static void zr2c(kf_ctx *c, int off, int njobs) {
         const int nrows = N * N;
         const int ntiles = (nrows + LZ - 1) / LZ;
         const size_t smem = (size_t)(LZ * PadLen<N>::value) * sizeof(T2);
         Launch L_(c, KC_Z_R2C, z_bytes(c, off, njobs, false));
-        k_z_r2c<T, N><<<njobs * ntiles, LZ * P, smem, c->st>>>(c->dz + off, njobs, nrows, (const T2 *)c->tw);
+        if (c->fftv)
+            k_z_r2c<T, N, 1><<<njobs * ntiles, LZ * PV<1>, smem, c->st>>>(c->dz + off, njobs, nrows, (const T2 *)c->tw);
+        else
+            k_z_r2c<T, N, 0><<<njobs * ntiles, LZ * PV<0>, smem, c->st>>>(c->dz + off, njobs, nrows, (const T2 *)c->tw);
     }
     static RhsArgs<T> rargs(kf_ctx *c) {
         RhsArgs<T> a;
@@ -731,8 +768,12 @@ template <typename T, int N> struct Impl {
         {
             const double cb = (double)c->Nc * sizeof(T2), rb = (double)c->Nc * sizeof(T);
             Launch L_(c, KC_XASM, pen ? 8 * cb : 8 * cb + 4 * cb + ((Tm & T_E_INT) ? cb : 0.) + 2 * rb);
-            k_xfwd_assemble<T, N><<<ntiles, TC * P, (size_t)N * TC * sizeof(T2), c->st>>>(c->dj + c->jF_x, geo(c),
-                                                                                         rargs(c), (const T2 *)c->tw);
+            if (c->fftv)
+                k_xfwd_assemble<T, N, 1><<<ntiles, TC * PV<1>, (size_t)N * TC * sizeof(T2), c->st>>>(
+                    c->dj + c->jF_x, geo(c), rargs(c), (const T2 *)c->tw);
+            else
+                k_xfwd_assemble<T, N, 0><<<ntiles, TC * PV<0>, (size_t)N * TC * sizeof(T2), c->st>>>(
+                    c->dj + c->jF_x, geo(c), rargs(c), (const T2 *)c->tw);
         }
         CK(cudaGetLastError());
     }
@@ -828,6 +869,27 @@ template <typename T> struct Dispatch {
         }
     }
 };
+
+// radix stages and threads per line of the two transform plans of length n
+template <int NN> void plan_info_n(int rad[2][4], int thr[2]) {
+    for (int i = 0; i < 4; ++i) {
+        rad[0][i] = PlanV<NN, 0>::radix[i];
+        rad[1][i] = PlanV<NN, 1>::radix[i];
+    }
+    thr[0] = PlanV<NN, 0>::P;
+    thr[1] = PlanV<NN, 1>::P;
+}
+void plan_info(int n, int rad[2][4], int thr[2]) {
+    switch (n) {
+        case 16: plan_info_n<16>(rad, thr); break;
+        case 32: plan_info_n<32>(rad, thr); break;
+        case 64: plan_info_n<64>(rad, thr); break;
+        case 96: plan_info_n<96>(rad, thr); break;
+        case 128: plan_info_n<128>(rad, thr); break;
+        case 256: plan_info_n<256>(rad, thr); break;
+        default: break;
+    }
+}
 
 // FP64 sums of the charge density e^s - e^phi + n_d and the kinetic energy
 // density 0.5 e^s |M e_x + u'|^2 (block partials in slots 0 and 1).
@@ -1388,6 +1450,110 @@ template <typename F> int guarded(kf_ctx *c, F f) {
 #include "kf_adjoint_host.cuh"
 #include "kf_driver.cuh"
 
+namespace {
+
+// Captured graphs hold the kernel variants they were captured with; dropped
+// when the variants change and rebuilt by their next use.
+void drop_graphs(kf_ctx *c) {
+    CK(cudaStreamSynchronize(c->st));
+    if (c->vgraph) cudaGraphExecDestroy(c->vgraph);
+    c->vgraph = nullptr;
+    if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+    c->step_graph = nullptr;
+    if (c->step_graph_wait) cudaGraphExecDestroy(c->step_graph_wait);
+    c->step_graph_wait = nullptr;
+    if (c->adj && c->adj->graph) {
+        cudaGraphExecDestroy(c->adj->graph);
+        c->adj->graph = nullptr;
+    }
+}
+
+// milliseconds per call of f: two untimed calls, then reps calls between
+// CUDA events on the context's stream
+template <typename F> double time_candidate(kf_ctx *c, int reps, F f) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    float ms = 0.f;
+    cudaError_t e = cudaSuccess;
+    try {
+        f();
+        f();
+        CK(cudaEventRecord(a, c->st));
+        for (int r = 0; r < reps; ++r) f();
+        CK(cudaEventRecord(b, c->st));
+        CK(cudaEventSynchronize(b));
+        e = cudaEventElapsedTime(&ms, a, b);
+    } catch (...) {
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        throw;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    CK(e);
+    return (double)ms / reps;
+}
+
+void autotune(kf_ctx *c, int reps, kf_tune_out *o) {
+    if (c->capturing) throw KfError{KF_ERR_ARG, "kf_autotune during a capture"};
+    kf_tune_out r{};
+    plan_info(c->n, r.fft_radices, r.fft_threads);
+    // transform plans: the right-hand side with the potential held writes
+    // only scratch arrays and K (the stage derivative, consumed within a step)
+    const bool pg = c->phi_given;
+    const int si = c->stage_idx, fv = c->fftv, by = c->rbgs_by;
+    c->phi_given = true;
+    c->stage_idx = 0;
+    try {
+        for (int v = 0; v < 2; ++v) {
+            c->fftv = v;
+            copy_state(c, c->Ys, c->Y);
+            r.fft_ms[v] = time_candidate(c, reps, [&] { c->rhs_fn(c); });
+        }
+    } catch (...) {
+        c->phi_given = pg;
+        c->stage_idx = si;
+        c->fftv = fv;
+        throw;
+    }
+    c->phi_given = pg;
+    c->stage_idx = si;
+    r.fft_plan = r.fft_ms[1] < r.fft_ms[0] ? 1 : 0;
+    // smoother shapes: sweeps of a copy of the finest-level potential
+    const int rows[3] = {4, 8, 16};
+    r.rbgs_rows = by;
+    if (c->rho && !c->lv.empty()) {
+        LevelBuf &L0 = c->lv[0];
+        double *tmp = nullptr;
+        CK(cudaMalloc(&tmp, 8 * (size_t)c->N));
+        try {
+            CK(cudaMemcpyAsync(tmp, c->phi, 8 * (size_t)c->N, cudaMemcpyDeviceToDevice, c->st));
+            int best = -1;
+            for (int k = 0; k < 3; ++k) {
+                c->rbgs_by = rows[k];
+                r.rbgs_ms[k] = time_candidate(c, reps, [&] { smooth(c, L0, tmp, c->rho, nullptr, 1, KC_RBGS); });
+                if (best < 0 || r.rbgs_ms[k] < r.rbgs_ms[best]) best = k;
+            }
+            r.rbgs_rows = rows[best];
+        } catch (...) {
+            c->rbgs_by = by;
+            c->fftv = fv;
+            cudaStreamSynchronize(c->st);
+            cudaFree(tmp);
+            throw;
+        }
+        CK(cudaStreamSynchronize(c->st));
+        CK(cudaFree(tmp));
+    }
+    c->fftv = r.fft_plan;
+    c->rbgs_by = r.rbgs_rows;
+    drop_graphs(c);
+    if (o) *o = r;
+}
+
+}  // namespace
+
 // Message of the last failure that has no context (kf_ctx_create and the
 // context-free entry points); kf_last_error(NULL) returns it.
 std::string &kf_global_error() {
@@ -1539,6 +1705,22 @@ int kf_rk4_steps(kf_ctx *c, int nsteps, double dt) {
         }
         for (int s = 0; s < nsteps; ++s) rk4_step(c, dt, nullptr, nullptr, nullptr);
         CK(cudaGetLastError());
+    });
+}
+
+int kf_autotune(kf_ctx *c, int reps, kf_tune_out *out) {
+    return guarded(c, [&] { autotune(c, reps > 0 ? reps : 5, out); });
+}
+
+int kf_set_tuning(kf_ctx *c, int fft_plan, int rbgs_rows) {
+    return guarded(c, [&] {
+        if ((fft_plan != 0 && fft_plan != 1) || (rbgs_rows != 4 && rbgs_rows != 8 && rbgs_rows != 16))
+            throw KfError{KF_ERR_ARG, "kf_set_tuning: fft_plan 0 or 1, rbgs_rows 4, 8 or 16"};
+        if (c->capturing) throw KfError{KF_ERR_ARG, "kf_set_tuning during a capture"};
+        const bool changed = fft_plan != c->fftv || rbgs_rows != c->rbgs_by;
+        c->fftv = fft_plan;
+        c->rbgs_by = rbgs_rows;
+        if (changed) drop_graphs(c);
     });
 }
 

@@ -226,16 +226,33 @@ __device__ __forceinline__ int reg_row(int p, int q) {
 }
 
 // Per-length launch plans: threads per line P and the radix sequence.
-template <int N> struct Plan;
-template <> struct Plan<16> { static constexpr int P = 4; template <typename T2, int S, typename A, typename TW> __device__ static void fft(T2 *v, T2 *sm, A a, int p, TW tw) { fft_line<T2, 16, 4, S, 4, 4>(v, sm, a, p, tw); } static constexpr int R1 = 4, RL = 4; };
-template <> struct Plan<32> { static constexpr int P = 4; template <typename T2, int S, typename A, typename TW> __device__ static void fft(T2 *v, T2 *sm, A a, int p, TW tw) { fft_line<T2, 32, 4, S, 8, 4>(v, sm, a, p, tw); } static constexpr int R1 = 8, RL = 4; };
-template <> struct Plan<64> { static constexpr int P = 8; template <typename T2, int S, typename A, typename TW> __device__ static void fft(T2 *v, T2 *sm, A a, int p, TW tw) { fft_line<T2, 64, 8, S, 8, 8>(v, sm, a, p, tw); } static constexpr int R1 = 8, RL = 8; };
-template <> struct Plan<96> { static constexpr int P = 8; template <typename T2, int S, typename A, typename TW> __device__ static void fft(T2 *v, T2 *sm, A a, int p, TW tw) { fft_line<T2, 96, 8, S, 6, 4, 4>(v, sm, a, p, tw); } static constexpr int R1 = 6, RL = 4; };
-template <> struct Plan<128> { static constexpr int P = 8; template <typename T2, int S, typename A, typename TW> __device__ static void fft(T2 *v, T2 *sm, A a, int p, TW tw) { fft_line<T2, 128, 8, S, 16, 8>(v, sm, a, p, tw); } static constexpr int R1 = 16, RL = 8; };
-#ifdef KF_PLAN256_P32
-template <> struct Plan<256> { static constexpr int P = 32; template <typename T2, int S, typename A, typename TW> __device__ static void fft(T2 *v, T2 *sm, A a, int p, TW tw) { fft_line<T2, 256, 32, S, 8, 8, 4>(v, sm, a, p, tw); } static constexpr int R1 = 8, RL = 4; };
-#else
-template <> struct Plan<256> { static constexpr int P = 16; template <typename T2, int S, typename A, typename TW> __device__ static void fft(T2 *v, T2 *sm, A a, int p, TW tw) { fft_line<T2, 256, 16, S, 16, 16>(v, sm, a, p, tw); } static constexpr int R1 = 16, RL = 16; };
-#endif
+// Variant 0 is the default; variant 1 an alternative the autotuner can pick
+// (kf_autotune): a different radix order and, where it allows, more threads
+// per line with fewer registers each.
+#define KF_PLAN(NN, V, PP, R1_, RL_, ...)                                                                   \
+    template <> struct PlanV<NN, V> {                                                                       \
+        static constexpr int P = PP;                                                                        \
+        template <typename T2, int S, typename A, typename TW>                                              \
+        __device__ static void fft(T2 *v, T2 *sm, A a, int p, TW tw) {                                      \
+            fft_line<T2, NN, PP, S, __VA_ARGS__>(v, sm, a, p, tw);                                          \
+        }                                                                                                   \
+        static constexpr int R1 = R1_, RL = RL_;                                                            \
+        static constexpr int radix[4] = {__VA_ARGS__};                                                      \
+    };
+template <int N, int V> struct PlanV;
+KF_PLAN(16, 0, 4, 4, 4, 4, 4)
+KF_PLAN(16, 1, 4, 4, 4, 4, 4)
+KF_PLAN(32, 0, 4, 8, 4, 8, 4)
+KF_PLAN(32, 1, 4, 4, 8, 4, 8)
+KF_PLAN(64, 0, 8, 8, 8, 8, 8)
+KF_PLAN(64, 1, 16, 4, 4, 4, 4, 4)
+KF_PLAN(96, 0, 8, 6, 4, 6, 4, 4)
+KF_PLAN(96, 1, 8, 4, 6, 4, 4, 6)
+KF_PLAN(128, 0, 8, 16, 8, 16, 8)
+KF_PLAN(128, 1, 16, 8, 4, 8, 4, 4)
+KF_PLAN(256, 0, 16, 16, 16, 16, 16)
+KF_PLAN(256, 1, 32, 8, 4, 8, 8, 4)
+#undef KF_PLAN
+template <int N> using Plan = PlanV<N, 0>;
 
 }  // namespace kf

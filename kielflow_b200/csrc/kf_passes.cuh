@@ -150,12 +150,12 @@ __device__ __forceinline__ AxisTile<T> axis_tile(const AxisJob *__restrict__ job
     return G;
 }
 
-template <typename T, int N, int SIGN>
-__global__ void __launch_bounds__(Tile<T>::TC * Plan<N>::P)
+template <typename T, int N, int SIGN, int V = 0>
+__global__ void __launch_bounds__(Tile<T>::TC * PlanV<N, V>::P)
 k_axis_pipe(const AxisJob *__restrict__ jobs, int njobs, int axis, Geo<T> g,
             const typename C2<T>::type *__restrict__ tw, int total) {
     typedef typename C2<T>::type T2;
-    constexpr int TC = Tile<T>::TC, P = Plan<N>::P, E = N / P;
+    constexpr int TC = Tile<T>::TC, P = PlanV<N, V>::P, E = N / P;
     extern __shared__ __align__(16) unsigned char kf_smem[];
     T2 *sm = reinterpret_cast<T2 *>(kf_smem);  // exchange [N][TC]
     T2 *stg = sm + N * TC;                      // staging  [N][TC]
@@ -165,7 +165,7 @@ k_axis_pipe(const AxisJob *__restrict__ jobs, int njobs, int axis, Geo<T> g,
     auto prefetch = [&](const AxisTile<T> &G) {
 #pragma unroll
         for (int q = 0; q < E; ++q) {
-            const int row = reg_row<N, P, Plan<N>::R1>(p, q);
+            const int row = reg_row<N, P, PlanV<N, V>::R1>(p, q);
             T2 *dst = stg + row * TC + c;
             if (G.valid)
                 cp_async_copy(dst, G.in + G.base + row * G.rstride);
@@ -184,7 +184,7 @@ k_axis_pipe(const AxisJob *__restrict__ jobs, int njobs, int axis, Geo<T> g,
         T2 v[E];
 #pragma unroll
         for (int q = 0; q < E; ++q) {
-            const int row = reg_row<N, P, Plan<N>::R1>(p, q);
+            const int row = reg_row<N, P, PlanV<N, V>::R1>(p, q);
             T2 x = stg[row * TC + c];
             if (cur.mul == MUL_P || cur.mul == MUL_P_IK) {
                 if (!dealias_keep(g.q2, g.thr, row, cur.jj, cur.kk)) x = mk<T2>((T)0, (T)0);
@@ -193,11 +193,11 @@ k_axis_pipe(const AxisJob *__restrict__ jobs, int njobs, int axis, Geo<T> g,
             v[q] = x;
         }
         if (tn < total) prefetch(nxt);
-        Plan<N>::template fft<T2, SIGN>(v, sm + c, StrideAddr{TC}, p, tw);
+        PlanV<N, V>::template fft<T2, SIGN>(v, sm + c, StrideAddr{TC}, p, tw);
         if (cur.valid) {
 #pragma unroll
             for (int q = 0; q < E; ++q) {
-                const int row = reg_row<N, P, Plan<N>::RL>(p, q);
+                const int row = reg_row<N, P, PlanV<N, V>::RL>(p, q);
                 cur.out[cur.base + row * cur.rstride] = v[q];
             }
         }
@@ -213,12 +213,12 @@ k_axis_pipe(const AxisJob *__restrict__ jobs, int njobs, int axis, Geo<T> g,
 // `scale` (the 1/N of OP_iFFT.cpp:59-61).
 template <typename T> struct ZTile { static constexpr int LZ = 8; };
 
-template <typename T, int N>
-__global__ void __launch_bounds__(ZTile<T>::LZ * Plan<N>::P)
+template <typename T, int N, int V = 0>
+__global__ void __launch_bounds__(ZTile<T>::LZ * PlanV<N, V>::P)
 k_z_c2r(const ZJob *__restrict__ jobs, int njobs, int nrows, Geo<T> g,
         const typename C2<T>::type *__restrict__ tw, T scale) {
     typedef typename C2<T>::type T2;
-    constexpr int LZ = ZTile<T>::LZ, P = Plan<N>::P, E = N / P, NZC = N / 2 + 1;
+    constexpr int LZ = ZTile<T>::LZ, P = PlanV<N, V>::P, E = N / P, NZC = N / 2 + 1;
     constexpr int LS = PadLen<N>::value;  // padded line of the exchange buffer
     extern __shared__ __align__(16) unsigned char kf_smem[];
     T2 *half = reinterpret_cast<T2 *>(kf_smem);  // [2][LZ][NZC], staging of the half spectra
@@ -251,7 +251,7 @@ k_z_c2r(const ZJob *__restrict__ jobs, int njobs, int nrows, Geo<T> g,
     T2 v[E];
 #pragma unroll
     for (int q = 0; q < E; ++q) {
-        const int k = reg_row<N, P, Plan<N>::R1>(p, q);
+        const int k = reg_row<N, P, PlanV<N, V>::R1>(p, q);
         T2 a, b;
         if (k < NZC) {
             a = hA[k];
@@ -265,14 +265,14 @@ k_z_c2r(const ZJob *__restrict__ jobs, int njobs, int nrows, Geo<T> g,
         v[q] = mk<T2>(a.x - b.y, a.y + b.x);  // A + iB
     }
     __syncthreads();  // staging consumed: the exchange buffer may overwrite it
-    Plan<N>::template fft<T2, +1>(v, xch + l * LS, PadAddr{}, p, tw);
+    PlanV<N, V>::template fft<T2, +1>(v, xch + l * LS, PadAddr{}, p, tw);
     const int r = r0 + l;
     if (r < nrows) {
         T *oA = static_cast<T *>(J.outA) + (long)r * N;
         T *oB = J.outB ? static_cast<T *>(J.outB) + (long)r * N : nullptr;
 #pragma unroll
         for (int q = 0; q < E; ++q) {
-            const int z = reg_row<N, P, Plan<N>::RL>(p, q);
+            const int z = reg_row<N, P, PlanV<N, V>::RL>(p, q);
             oA[z] = v[q].x * scale;
             if (oB) oB[z] = v[q].y * scale;
         }
@@ -280,12 +280,12 @@ k_z_c2r(const ZJob *__restrict__ jobs, int njobs, int nrows, Geo<T> g,
 }
 
 // --------------------------------------------------------------- z r2c pass
-template <typename T, int N>
-__global__ void __launch_bounds__(ZTile<T>::LZ * Plan<N>::P)
+template <typename T, int N, int V = 0>
+__global__ void __launch_bounds__(ZTile<T>::LZ * PlanV<N, V>::P)
 k_z_r2c(const ZJob *__restrict__ jobs, int njobs, int nrows,
         const typename C2<T>::type *__restrict__ tw) {
     typedef typename C2<T>::type T2;
-    constexpr int LZ = ZTile<T>::LZ, P = Plan<N>::P, E = N / P, NZC = N / 2 + 1;
+    constexpr int LZ = ZTile<T>::LZ, P = PlanV<N, V>::P, E = N / P, NZC = N / 2 + 1;
     constexpr int LS = PadLen<N>::value;
     extern __shared__ __align__(16) unsigned char kf_smem[];
     T2 *xch = reinterpret_cast<T2 *>(kf_smem);  // [LZ][LS], padded lines
@@ -299,7 +299,7 @@ k_z_r2c(const ZJob *__restrict__ jobs, int njobs, int nrows,
     T2 v[E];
 #pragma unroll
     for (int q = 0; q < E; ++q) {
-        const int z = reg_row<N, P, Plan<N>::R1>(p, q);
+        const int z = reg_row<N, P, PlanV<N, V>::R1>(p, q);
         T a = (T)0, b = (T)0;
         if (r < nrows) {
             a = iA[(long)r * N + z];
@@ -309,10 +309,10 @@ k_z_r2c(const ZJob *__restrict__ jobs, int njobs, int nrows,
     }
     T2 *line = xch + l * LS;
     const PadAddr pa;
-    Plan<N>::template fft<T2, -1>(v, line, pa, p, tw);
+    PlanV<N, V>::template fft<T2, -1>(v, line, pa, p, tw);
     __syncthreads();
 #pragma unroll
-    for (int q = 0; q < E; ++q) line[pa(reg_row<N, P, Plan<N>::RL>(p, q))] = v[q];
+    for (int q = 0; q < E; ++q) line[pa(reg_row<N, P, PlanV<N, V>::RL>(p, q))] = v[q];
     __syncthreads();
     for (int idx = threadIdx.x; idx < LZ * NZC; idx += blockDim.x) {
         const int ll = idx / NZC, k = idx - ll * NZC;
@@ -411,12 +411,12 @@ __device__ __forceinline__ typename C2<T>::type lin_term(const RhsArgs<T> &a, co
 //   penalization on : K_q = P(k) F_q              (the 2/3 filter after the
 //                     physical-space penalization, rhs_standard.cpp:491-532)
 // gridDim.x = number of column tiles; jobs[q].in = y-passed field, .out = K_q.
-template <typename T, int N>
-__global__ void __launch_bounds__(Tile<T>::TC * Plan<N>::P)
+template <typename T, int N, int V = 0>
+__global__ void __launch_bounds__(Tile<T>::TC * PlanV<N, V>::P)
 k_xfwd_assemble(const AxisJob *__restrict__ jobs, Geo<T> g, RhsArgs<T> a,
                 const typename C2<T>::type *__restrict__ tw) {
     typedef typename C2<T>::type T2;
-    constexpr int TC = Tile<T>::TC, P = Plan<N>::P, E = N / P;
+    constexpr int TC = Tile<T>::TC, P = PlanV<N, V>::P, E = N / P;
     extern __shared__ __align__(16) unsigned char kf_smem[];
     T2 *sm = reinterpret_cast<T2 *>(kf_smem);
     const int tile = blockIdx.x;
@@ -433,14 +433,14 @@ k_xfwd_assemble(const AxisJob *__restrict__ jobs, Geo<T> g, RhsArgs<T> a,
         T2 v[E];
 #pragma unroll
         for (int e = 0; e < E; ++e) {
-            const int row = reg_row<N, P, Plan<N>::R1>(p, e);
+            const int row = reg_row<N, P, PlanV<N, V>::R1>(p, e);
             v[e] = valid ? in[col + row * rstride] : mk<T2>((T)0, (T)0);
         }
-        Plan<N>::template fft<T2, -1>(v, sm + c, StrideAddr{TC}, p, tw);
+        PlanV<N, V>::template fft<T2, -1>(v, sm + c, StrideAddr{TC}, p, tw);
         if (valid) {
 #pragma unroll
             for (int e = 0; e < E; ++e) {
-                const int i = reg_row<N, P, Plan<N>::RL>(p, e);
+                const int i = reg_row<N, P, PlanV<N, V>::RL>(p, e);
                 const long idx = col + i * rstride;
                 T2 F = v[e];
                 T2 K;

@@ -43,7 +43,7 @@ def workload_of(inst: Instance) -> dict:
 
 
 def run_sweep(instances, steps: int, mode: str = "batched", precision=None, warmup: int = 1,
-              max_threads: int = 64):
+              max_threads: int = 64, tune=True, tunings: dict | None = None):
     """Advance every instance `steps` RK4 steps on the current GPU.
 
     Each instance is its own context (device memory, tables, CUDA stream,
@@ -54,8 +54,13 @@ def run_sweep(instances, steps: int, mode: str = "batched", precision=None, warm
       "threads"    -- a pool of host threads, one kf_rk4_steps call each
                       (the C calls release the GIL);
       "sequential" -- one instance after another (the baseline).
-    `warmup` steps per instance run first, outside the timed region (graph
-    capture, first-touch of the buffers).  Returns (wall seconds of the timed
+    With `tune`, the first instance of each grid size is autotuned
+    (kf_autotune: transform radix plan, smoother block shape) and its choice
+    is given to every instance of that size; `tune` may instead be such a
+    result per size ({n: {"fft_plan": p, "rbgs_rows": r}}, e.g. the `tunings`
+    of an earlier run) to apply without timing.  `tunings`, when a dict,
+    receives {n: the choice used}.  `warmup` steps per instance run first, outside
+    the timed region (graph capture, first-touch of the buffers).  Returns (wall seconds of the timed
     steps, [final state per instance], [diag per instance]).
     """
     import threading
@@ -72,6 +77,15 @@ def run_sweep(instances, steps: int, mode: str = "batched", precision=None, warm
         ctx.set_sources(nd, mask)
         ctxs.append(ctx)
         dts.append(dt)
+    if tune:
+        chosen = dict(tune) if isinstance(tune, dict) else {}
+        for inst, ctx in zip(instances, ctxs):
+            if inst.n not in chosen:
+                chosen[inst.n] = ctx.autotune()
+            else:
+                ctx.set_tuning(chosen[inst.n]["fft_plan"], chosen[inst.n]["rbgs_rows"])
+        if tunings is not None:
+            tunings.update(chosen)
     if warmup > 0:
         for ctx, dt in zip(ctxs, dts):
             ctx.rk4(dt, warmup)
