@@ -403,9 +403,12 @@ def run_kf(args):
         if w["precision"] == kf.KF_FP32_BULK else "f64",
         "data": "synthetic (seeded noise, Gaussian dust; seed = rank)",
         "config": {"workload": f"{args.workload}: {w['n']}^3 box 2*pi*4, M {w['M']}, nu {w['tau']}, "
-                               f"Q {w['Q']}, sigma {w['sigma']}, FAS 4 levels 2+2 to 1e-10, penalization, "
+                               f"Q {w['Q']}, sigma {w['sigma']}, FAS {C.config_for(w).mg_levels} levels 2+2 to 1e-10 "
+                               f"(at most {C.config_for(w).max_cycles} V-cycles per solve), penalization, "
                                f"diffusion 1e-3, SV > 0.6 k_max",
                    "n": w["n"], "dt": dt, "l2": "inputs larger than L2 (state + work buffers > 2 GB)",
+                   "axes": (f"axis_CoSiSt m {w['stretch']:.6g} (sine-stretched, chain-rule derivatives)"
+                            if w.get("stretch") else "axis_CoEqSt"),
                    "parallelism": f"replicas x{ws}",
                    "tuning": {"fft_radices": tune32["fft_radices"][tune32["fft_plan"]],
                               "rbgs_rows": tune32["rbgs_rows"]}},

@@ -30,13 +30,24 @@ inline void check(kf_ctx *c, int rc) {
 }
 
 /* kf_config for a cubic reference grid and parameters (the shipped physics by
- * default: rhs_standard.hpp:22-30 term set, SV amplitude 0.5, theta from params) */
+ * default: rhs_standard.hpp:22-30 term set, SV amplitude 0.5, theta from params).
+ * The three axes must be alike: axis_CoEqSt (type_id 1) or axis_CoSiSt
+ * (type_id 3, its m becomes stretch_m); axis_CoHySt has no dS and cannot take
+ * derivatives in the reference either (axis_base.cpp:17-23). */
 template <typename Grid, typename Params>
 kf_config config_from(const Grid &g, const Params &p, int poisson_mode, int terms = KF_T_SHIPPED) {
     if (g.Nx != g.Ny || g.Nx != g.Nz) throw std::runtime_error("kielflow_b200: cubic grids only");
+    const auto *ax = g.x_axis;
+    for (const auto *a : {g.y_axis, g.z_axis})
+        if (a->type_id != ax->type_id || a->L != ax->L || a->l0 != ax->l0 || (ax->type_id == 3 && a->m != ax->m))
+            throw std::runtime_error("kielflow_b200: the three axes must be alike");
+    if (ax->type_id != 1 && ax->type_id != 3)
+        throw std::runtime_error("kielflow_b200: axis_CoEqSt or axis_CoSiSt axes only");
+    if (ax->l0 != -0.5 * ax->L) throw std::runtime_error("kielflow_b200: the box must be centred (l0 = -L/2)");
     kf_config c = {};
     c.n = g.Nx;
-    c.L = g.x_axis->L;
+    c.L = ax->L;
+    c.stretch_m = ax->type_id == 3 ? ax->m : 0.;
     c.M = p.M;
     c.tau = p.tau;
     c.theta = p.theta;

@@ -82,6 +82,14 @@ typedef struct {
     int phi_extrap;    /* 1: start each Poisson solve at a new time from the linear  */
                        /*    extrapolation of the last two solutions in time         */
     int precision;     /* KF_FP64 or KF_FP32_BULK                                    */
+    double stretch_m;  /* 0: axis_CoEqSt(-L/2, L, n) axes.  > 0: axis_CoSiSt(-L/2, L,  */
+                       /* n, stretch_m) on all three axes (x = S(l0 + L i/n),        */
+                       /* S(x) = x - m sin(2 pi x/L), axis_SiSt.cpp; the frontend's  */
+                       /* grid uses m = L (1 - 0.3)/(2 pi), frontend.cpp:285-287);   */
+                       /* 2 pi m / L < 1.  Derivatives then take the chain-rule path */
+                       /* of OP_partial_derivative.cpp:104-136 and the Poisson       */
+                       /* stencils the stretched spacings (H_create).  Not with      */
+                       /* kf_adjoint_run.                                           */
 } kf_config;
 
 typedef struct kf_ctx kf_ctx;
@@ -190,6 +198,8 @@ typedef struct {
     int n;            /* N_x (= N_y = N_z required)                     */
     int kind;         /* KF_FILE_SLICE (2-D data) or KF_FILE_BACKUP     */
     double L, l0, time, M, tau, theta, mu, beta;
+    int type;         /* domain/type_x: 1 axis_CoEqSt, 3 axis_CoSiSt    */
+    double m;         /* domain/m_x (the stretching parameter)          */
 } kf_file_info;
 int kf_file_info_read(const char *path, kf_file_info *info);
 /* write the context's current state (and phi) as a slice or backup file */

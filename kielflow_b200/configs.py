@@ -21,6 +21,7 @@ DIFF_D = 1e-3
 PEN_ETA = -1e-3
 MASK_RADIUS = 0.5
 CFL = 0.2
+STRETCH_FRONTEND = L_BOX * (1.0 - 0.3) / (2.0 * math.pi)  # frontend.cpp:285-287
 
 WORKLOADS = {
     # plain FP64, nonlinear Jacobi to residual 1e-10, no spectral viscosity
@@ -38,6 +39,14 @@ WORKLOADS = {
     # adjoint workload geometry (forward part)
     "adj128": dict(n=128, M=0.9, tau=0.1, Q=-20.0, sigma=0.5, steps=200, sv=True,
                    poisson_mode=KF_PS_FAS, precision=KF_FP64),
+    # the fp32bulk256 physics on the reference frontend's sine-stretched grid
+    # (axis_CoSiSt, m = L (1 - 0.3) / (2 pi): 0.3 h cells at the grain).  The
+    # cells' aspect ratios reach 1.7/0.3, so the point smoother of the FAS
+    # cycle converges slowly there (about 0.75 per V-cycle against 0.07 on the
+    # equidistant grid): a higher cycle cap per solve
+    "stretch256": dict(n=256, M=1.0, tau=0.05, Q=-50.0, sigma=0.3, steps=2000, sv=True,
+                       poisson_mode=KF_PS_FAS, precision=KF_FP32_BULK, stretch=STRETCH_FRONTEND,
+                       max_cycles=600),
 }
 
 
@@ -59,7 +68,8 @@ def config_for(w: dict, n: int | None = None, precision: int | None = None, **ov
     kw = dict(tau=w["tau"], theta=THETA, diff_D=DIFF_D, sv_eps=0.5, sv_cut=0.6 if w["sv"] else 0.0,
               pen_eta=PEN_ETA, terms=terms, poisson_mode=w["poisson_mode"], nlj_max_it=100000,
               nlj_limit=0.5e-5, res_tol=1e-10, mg_levels=levels, mg_pre=2, mg_post=2, coarse_tol=1e-13,
-              max_cycles=100, phi_extrap=1, precision=w["precision"] if precision is None else precision)
+              max_cycles=w.get("max_cycles", 100), phi_extrap=1, precision=w["precision"] if precision is None else precision,
+              stretch_m=w.get("stretch", 0.0))
     kw.update(over)
     return Config.make(n, L_BOX, w["M"], **kw)
 
@@ -83,8 +93,9 @@ def make_inputs(w: dict, n: int | None = None, seed: int = 0):
     """(state, n_d, mask, dt) of a workload, from the seeded generator."""
     from . import inputs as I
     n = n or w["n"]
+    m = w.get("stretch", 0.0)
     st = I.initial_state(n, seed=seed)
-    nd = I.gauss_charge(n, L_BOX, w["Q"], w["sigma"])
-    mask = I.sphere_mask(n, L_BOX, MASK_RADIUS)
-    dt = I.cfl_dt(st, n, L_BOX, w["M"], CFL)
+    nd = I.gauss_charge(n, L_BOX, w["Q"], w["sigma"], m)
+    mask = I.sphere_mask(n, L_BOX, MASK_RADIUS, m)
+    dt = I.cfl_dt(st, n, L_BOX, w["M"], CFL, m)
     return st, nd, mask, dt

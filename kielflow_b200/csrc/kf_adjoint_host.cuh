@@ -623,5 +623,8 @@ void adj_run(kf_ctx *c, int nsteps, double dt, int E, int flags, const double *w
 
 extern "C" int kf_adjoint_run(kf_ctx *c, int nsteps, double dt, int ckpt_every, int flags, const double *w,
                               kf_grad_out *out, double *dJ_dn0, double *lam0) {
-    return guarded(c, [&] { adj_run(c, nsteps, dt, ckpt_every, flags, w, out, dJ_dn0, lam0); });
+    return guarded(c, [&] {
+        if (c->stretched) throw KfError{KF_ERR_ARG, "the discrete adjoint needs equidistant axes (stretch_m = 0)"};
+        adj_run(c, nsteps, dt, ckpt_every, flags, w, out, dJ_dn0, lam0);
+    });
 }

@@ -24,6 +24,7 @@
 #include "kf_passes.cuh"
 #include "kf_pointwise.cuh"
 #include "kf_poisson.cuh"
+#include "kf_stretch.cuh"
 
 using namespace kf;
 
@@ -91,6 +92,14 @@ struct kf_ctx {
     int jA_x = 0, jA_y = 0, zA = 0, zB = 0, jB_y = 0, jB_x = 0, jD_x = 0, nD_x = 0, jD_y = 0, nD_y = 0;
     int zD = 0, nzD = 0, zF = 0, jF_y = 0, jF_x = 0, jT_x = 0, jT_y = 0, zT = 0, jTf_y = 0, jTf_x = 0;
     int jG_x = 0, jG_y = 0, zG = 0;
+    // sine-stretched axes: the chain-rule right-hand side's buffers, metric
+    // tables and job lists (allocated only when cfg.stretch_m != 0)
+    bool stretched = false;
+    void *SX[15] = {};
+    void *met = nullptr;    // filtered 1/dS per index (bulk precision)
+    double *vol = nullptr;  // dS per index (cell widths / h) for the diagnostics
+    int jS_Dx = 0, jS_Dy = 0, zS_D = 0, zS_F = 0, jS_Fy = 0, jS_Fx = 0, jS_Gx = 0, jS_Gy = 0, zS_G = 0;
+    int zS_I = 0, jS_Iy = 0, jS_Ix = 0, jS_Kx = 0, jS_Ky = 0, zS_K = 0, zS_Kf = 0, jS_Kfy = 0, jS_Kfx = 0;
     // Jacobi state carried between sweeps and solves (solver_poisson_jacobi_nlin.hpp:66-95)
     double norm_max = 0., norm_sum = 0., norm_max_old = -1., norm_sum_old = -1.;
     double sup = 0., inf = 0., omega = 1.;
@@ -221,7 +230,62 @@ double k_val_at(int i, int n, double L) {  // axis_EqSt.cpp:57-61
     double pi = acos(-1.);
     return ((i <= n / 2) ? (2. * pi * i / L) : (2. * pi * (i - n) / L));
 }
-double val_at(int i, int n, double L) { return -0.5 * L + i * (L / n); }  // axis_EqSt.cpp:52-55
+// Position of index i (-1 <= i <= n) on the box axis [-L/2, L/2):
+// axis_CoEqSt for m == 0 (axis_EqSt.cpp:52-55), else axis_CoSiSt with the
+// periodic extension of its val_at (axis_SiSt.cpp:93-116) and
+// S(x) = x - m sin(2 pi x / L) (:153-157).
+double val_at(int i, int n, double L, double m = 0.) {
+    if (m == 0.) return -0.5 * L + i * (L / n);
+    int shift = 0;
+    if (i < 0) {
+        do {
+            shift += 1;
+        } while (i + shift * n < 0);
+    }
+    if (i >= n) {
+        do {
+            shift -= 1;
+        } while (i + shift * n >= n - 1);
+    }
+    const double pi = acos(-1.);
+    const double x = -0.5 * L + L * double(i + shift * n) / (n);
+    return (x - m * sin(2. * pi * x / L)) - shift * L;
+}
+// dS/dx of the stretched axis at index i (axis_SiSt.cpp:158-164)
+double dS_at(int i, int n, double L, double m) {
+    const double pi = acos(-1.);
+    const double x = -0.5 * L + (L / n) * i;
+    return 1. - (2. * pi * m / L) * cos(2. * pi * x / L);
+}
+// 1/dS of each index after the 2/3 filter: OP_partial_derivative.cpp:60-80
+// forms it on the whole grid (FFT, OP_dealiasing, inverse FFT); the field
+// depends on one index only, so that is one 1-D DFT pair along the axis with
+// the filter of the (k, 0, 0) line, done here in long double.
+std::vector<double> metric_table(int n, double L, double m, double thr) {
+    std::vector<double> f(n), q2(n), out(n);
+    const double kmax = k_val_at(n / 2, n, L);
+    for (int i = 0; i < n; ++i) {
+        f[i] = 1. / dS_at(i, n, L, m);
+        q2[i] = pow(k_val_at(i, n, L) / kmax, 2.);
+    }
+    const long double twopi = 6.283185307179586476925286766559005768L;
+    std::vector<long double> acc(n, 0.L);
+    for (int kk = 0; kk < n; ++kk) {
+        if (!(q2[kk] + q2[0] + q2[0] < thr)) continue;
+        long double Fr = 0.L, Fi = 0.L;
+        for (int i = 0; i < n; ++i) {
+            const long double a = twopi * (long double)((long)kk * i % n) / n;
+            Fr += f[i] * cosl(a);
+            Fi -= f[i] * sinl(a);
+        }
+        for (int i = 0; i < n; ++i) {
+            const long double a = twopi * (long double)((long)kk * i % n) / n;
+            acc[i] += Fr * cosl(a) - Fi * sinl(a);
+        }
+    }
+    for (int i = 0; i < n; ++i) out[i] = (double)(acc[i] / n);
+    return out;
+}
 
 // ------------------------------------------------------------------ Poisson driver
 void reduce_read(kf_ctx *c, int nb) {
@@ -691,8 +755,9 @@ template <typename T, int N> struct Impl {
         return a;
     }
 
-    // one right-hand-side evaluation: Ys -> K
-    static void rhs(kf_ctx *c) {
+    // rounds A (P s, d_x s, d_y s and s_d = c2r(P s)), the Poisson solve and
+    // B (phi^ = r2c(phi)), shared by both right-hand sides
+    static void rounds_AB(kf_ctx *c) {
         const int Tm = c->cfg.terms;
         const bool pen = Tm & T_PENALIZATION;
         const bool pois = (Tm & T_POISSON) && (Tm & T_E_INT);
@@ -730,6 +795,13 @@ template <typename T, int N> struct Impl {
             axis(c, c->jB_y, 1, 1, -1);
             axis(c, c->jB_x, 1, 0, -1);
         }
+    }
+
+    // one right-hand-side evaluation: Ys -> K
+    static void rhs(kf_ctx *c) {
+        const int Tm = c->cfg.terms;
+        const bool pen = Tm & T_PENALIZATION;
+        rounds_AB(c);
         // C
         if (pen) {
             Launch L_(c, KC_LIN, (double)c->Nc * (9 * sizeof(T2) + 2 * sizeof(T)));
@@ -774,6 +846,112 @@ template <typename T, int N> struct Impl {
             else
                 k_xfwd_assemble<T, N, 0><<<ntiles, TC * PV<0>, (size_t)N * TC * sizeof(T2), c->st>>>(
                     c->dj + c->jF_x, geo(c), rargs(c), (const T2 *)c->tw);
+        }
+        CK(cudaGetLastError());
+    }
+
+    // The right-hand side on sine-stretched axes: every derivative takes the
+    // chain-rule path D_d F = r2c(m_d c2r(P i k_d F)) of
+    // OP_partial_derivative.cpp:104-136, so the derivative terms that
+    // rhs() folds into k-space become transform pairs:
+    //   C' linear parts, F1                 D' raw derivatives (15 c2r)
+    //   E' times the metric                 F' their r2c (15)
+    //   G' c2r(P D_d u'_c), c2r(P D_d s)    H' products (rhs_standard.cpp:323-436)
+    //   I' r2c of the products              J' assembly
+    //   K' penalization of the finished right-hand side, then the 2/3 filter
+    static void rhs_stretched(kf_ctx *c) {
+        const int Tm = c->cfg.terms;
+        const bool pen = Tm & T_PENALIZATION;
+        const long Nc = c->Nc, Nr = c->N;
+        const double cb = (double)Nc * sizeof(T2), rb = (double)Nr * sizeof(T);
+        rounds_AB(c);
+        {  // C'
+            Launch L_(c, KC_LIN, 4 * cb + 6 * cb + 2 * rb);
+            k_sl_lin<T><<<nblk(Nc, 256), 256, 0, c->st>>>(rargs(c), geo(c), (T2 *)c->LIN[0], (T2 *)c->LIN[1],
+                                                            (T2 *)c->LIN[2], (T2 *)c->LIN[3], (T2 *)c->CX[10]);
+        }
+        // D'
+        axis(c, c->jS_Dx, 8, 0, +1);
+        axis(c, c->jS_Dy, 12, 1, +1);
+        zc2r(c, c->zS_D, 10);
+        {  // E'
+            ScaleArgs<T> sa;
+            for (int j = 0; j < 15; ++j) sa.f[j] = (T *)c->R[4 + j];
+            sa.met = (const T *)c->met;
+            sa.n = c->n;
+            sa.N = Nr;
+            Launch L_(c, KC_PROD, 30. * rb);
+            k_sl_scale<T><<<nblk(Nr, 256), 256, 0, c->st>>>(sa);
+        }
+        // F'
+        zr2c(c, c->zS_F, 8);
+        axis(c, c->jS_Fy, 15, 1, -1);
+        axis(c, c->jS_Fx, 15, 0, -1);
+        const bool prod = Tm & (T_ADVECTION | T_CONTINUITY);
+        if (prod) {
+            // G'
+            axis(c, c->jS_Gx, 12, 0, +1);
+            axis(c, c->jS_Gy, 12, 1, +1);
+            zc2r(c, c->zS_G, 6);
+            {  // H'
+                ProdArgs<T> pa{};
+                for (int q = 0; q < 3; ++q) {
+                    pa.U[q] = (const T *)c->R[1 + q];
+                    pa.ds[q] = (const T *)c->R[13 + q];
+                    for (int d = 0; d < 3; ++d) pa.dU[q][d] = (const T *)c->R[4 + 3 * q + d];
+                }
+                for (int q = 0; q < 4; ++q) pa.out[q] = (T *)c->R[20 + q];
+                pa.M = (T)c->cfg.M;
+                pa.terms = Tm & (T_ADVECTION | T_CONTINUITY);
+                pa.N = Nr;
+                Launch L_(c, KC_PROD, 19. * rb);
+                k_products<T><<<nblk(Nr, 256), 256, 0, c->st>>>(pa);
+            }
+            // I'
+            zr2c(c, c->zS_I, 2);
+            axis(c, c->jS_Iy, 4, 1, -1);
+            axis(c, c->jS_Ix, 4, 0, -1);
+        }
+        {  // J'
+            AsmArgs<T> aa;
+            for (int q = 0; q < 4; ++q) {
+                aa.lin[q] = (const T2 *)c->LIN[q];
+                aa.pr[q] = prod ? (const T2 *)c->SX[8 + q] : nullptr;
+                aa.K[q] = (T2 *)c->K[q];
+            }
+            for (int j = 0; j < 15; ++j) aa.dn[j] = (const T2 *)c->CY[j];
+            aa.M = (T)c->cfg.M;
+            aa.terms = Tm;
+            aa.Nc = Nc;
+            Launch L_(c, KC_XASM, 27 * cb);
+            k_sl_assemble<T><<<nblk(Nc, 256), 256, 0, c->st>>>(aa);
+        }
+        if (pen) {  // K'
+            axis(c, c->jS_Kx, 4, 0, +1);
+            axis(c, c->jS_Ky, 4, 1, +1);
+            zc2r(c, c->zS_K, 2);
+            {
+                ProdArgs<T> pa{};
+                for (int q = 0; q < 3; ++q) pa.U[q] = (const T *)c->R[1 + q];
+                for (int q = 0; q < 4; ++q) {
+                    pa.rl[q] = (const T *)c->R[20 + q];
+                    pa.out[q] = (T *)c->R[20 + q];
+                }
+                pa.sd = (const T *)c->R[0];
+                pa.H = (const T *)c->H;
+                pa.M = (T)c->cfg.M;
+                pa.eta = (T)c->cfg.pen_eta;
+                pa.terms = T_PENALIZATION;
+                pa.N = Nr;
+                Launch L_(c, KC_PROD, 13. * rb);
+                k_products<T><<<nblk(Nr, 256), 256, 0, c->st>>>(pa);
+            }
+            zr2c(c, c->zS_Kf, 2);
+            axis(c, c->jS_Kfy, 4, 1, -1);
+            axis(c, c->jS_Kfx, 4, 0, -1);
+            Launch L_(c, KC_MISC, 8 * cb);
+            k_sl_dealias4<T><<<nblk(Nc, 256), 256, 0, c->st>>>(geo(c), (T2 *)c->K[0], (T2 *)c->K[1],
+                                                                 (T2 *)c->K[2], (T2 *)c->K[3]);
         }
         CK(cudaGetLastError());
     }
@@ -851,7 +1029,7 @@ template <typename T> struct Dispatch {
 #define KF_CASE(NN)                                    \
     case NN:                                           \
         Impl<T, NN>::set_attrs();                      \
-        c->rhs_fn = &Impl<T, NN>::rhs;                 \
+        c->rhs_fn = c->stretched ? &Impl<T, NN>::rhs_stretched : &Impl<T, NN>::rhs; \
         c->r2c_fn = &Impl<T, NN>::r2c;                 \
         c->c2r_fn = &Impl<T, NN>::c2r;                 \
         c->inv_state_fn = &Impl<T, NN>::inv_state;     \
@@ -897,14 +1075,18 @@ template <typename T>
 __global__ void __launch_bounds__(RBS) k_diag_sums(const T *__restrict__ s, const T *__restrict__ ux,
                                                    const T *__restrict__ uy, const T *__restrict__ uz,
                                                    const double *__restrict__ phi, const double *__restrict__ nd,
-                                                   double M, long N, double *__restrict__ partial) {
+                                                   double M, long N, double *__restrict__ partial,
+                                                   const double *__restrict__ vol, int n) {
     __shared__ double sh[2 * RBS];
     double ch = 0., kin = 0.;
     for (long i = (long)blockIdx.x * RBS + threadIdx.x; i < N; i += (long)gridDim.x * RBS) {
+        // cell volume / h^3: 1, or dS(x) dS(y) dS(z) on stretched axes
+        double w = 1.;
+        if (vol) w = vol[i / ((long)n * n)] * vol[(i / n) % n] * vol[i % n];
         const double n_i = exp((double)s[i]);
-        ch += n_i - exp(phi[i]) + nd[i];
+        ch += w * (n_i - exp(phi[i]) + nd[i]);
         const double vx = M + (double)ux[i], vy = (double)uy[i], vz = (double)uz[i];
-        kin += 0.5 * n_i * (vx * vx + vy * vy + vz * vz);
+        kin += w * (0.5 * n_i * (vx * vx + vy * vy + vz * vz));
     }
     sh[threadIdx.x] = kin;
     sh[RBS + threadIdx.x] = ch;
@@ -993,6 +1175,20 @@ void build_tables(kf_ctx *c) {
         CK(cudaMemcpy(c->PF, PF.data(), 8 * c->Nc, cudaMemcpyHostToDevice));
         CK(cudaMemcpy(c->tw, tw.data(), 16 * n, cudaMemcpyHostToDevice));
     }
+    if (c->stretched) {
+        const std::vector<double> met = metric_table(n, L, c->cfg.stretch_m, dealias_threshold());
+        std::vector<double> vol(n);
+        for (int i = 0; i < n; ++i) vol[i] = dS_at(i, n, L, c->cfg.stretch_m);
+        c->met = dalloc<void>(c, c->es * n);
+        c->vol = dalloc<double>(c, 8 * n);
+        if (c->fp32) {
+            std::vector<float> mf(met.begin(), met.end());
+            CK(cudaMemcpy(c->met, mf.data(), 4 * n, cudaMemcpyHostToDevice));
+        } else {
+            CK(cudaMemcpy(c->met, met.data(), 8 * n, cudaMemcpyHostToDevice));
+        }
+        CK(cudaMemcpy(c->vol, vol.data(), 8 * n, cudaMemcpyHostToDevice));
+    }
 }
 
 void build_levels(kf_ctx *c) {
@@ -1014,7 +1210,8 @@ void build_levels(kf_ctx *c) {
         L.n = n;
         const double Lb = cf.L;
         std::vector<double> H(n + 1), dd(n), dp(n), dm(n), ip(n), im(n), gam(n, 0.);
-        for (int i = 0; i < n + 1; ++i) H[i] = val_at(i, n, Lb) - val_at(i - 1, n, Lb);  // H_create (:112-126)
+        const double sm = cf.stretch_m;
+        for (int i = 0; i < n + 1; ++i) H[i] = val_at(i, n, Lb, sm) - val_at(i - 1, n, Lb, sm);  // H_create (:112-126)
         for (int i = 0; i < n; ++i) {
             dd[i] = 2. / (H[i + 1] * H[i]);
             dp[i] = H[i + 1] * (H[i + 1] + H[i]);
@@ -1023,7 +1220,7 @@ void build_levels(kf_ctx *c) {
             im[i] = 2. / dm[i];
         }
         for (int m = 1; m < n; m += 2) {  // OP_hto2h gamma on this (fine) axis
-            const double x1 = val_at(m - 1, n, Lb), x2 = val_at(m + 1, n, Lb), x = val_at(m, n, Lb);
+            const double x1 = val_at(m - 1, n, Lb, sm), x2 = val_at(m + 1, n, Lb, sm), x = val_at(m, n, Lb, sm);
             gam[m] = (x - x1) / (x2 - x1);
         }
         L.dd = dalloc<double>(c, 8 * n);
@@ -1127,6 +1324,75 @@ void build_jobs(kf_ctx *c) {
     c->zG = (int)Z.size();
     zj(CY[0], MUL_NONE, CY[1], MUL_NONE, R[20], R[21]);
     zj(CY[2], MUL_NONE, CY[3], MUL_NONE, R[22], R[23]);
+    if (c->stretched) {
+        void **SX = c->SX;
+        // D': raw derivatives c2r(P i k_d F) of u'_c (R[4+3c+d], with U_c in
+        // R[1+c]), of s (R[13+d]; its x and y passes are round A's) and of F1
+        // (in CX[10]; R[16+d])
+        c->jS_Dx = (int)J.size();
+        for (int q = 0; q < 3; ++q) {
+            aj(c->Ys[q], CX[2 + 2 * q], MUL_P);
+            aj(c->Ys[q], CX[3 + 2 * q], MUL_P_IK);
+        }
+        aj(CX[10], CX[8], MUL_P);
+        aj(CX[10], CX[9], MUL_P_IK);
+        c->jS_Dy = (int)J.size();
+        for (int q = 0; q < 3; ++q) {
+            aj(CX[2 + 2 * q], CY[3 + 3 * q], MUL_NONE);
+            aj(CX[2 + 2 * q], CY[4 + 3 * q], MUL_IK);
+            aj(CX[3 + 2 * q], CY[5 + 3 * q], MUL_NONE);
+        }
+        aj(CX[8], CY[12], MUL_NONE);
+        aj(CX[8], CY[13], MUL_IK);
+        aj(CX[9], CY[14], MUL_NONE);
+        c->zS_D = (int)Z.size();
+        for (int q = 0; q < 3; ++q) {
+            zj(CY[3 + 3 * q], MUL_NONE, CY[3 + 3 * q], MUL_IK, R[1 + q], R[4 + 3 * q + 2]);
+            zj(CY[4 + 3 * q], MUL_NONE, CY[5 + 3 * q], MUL_NONE, R[4 + 3 * q + 1], R[4 + 3 * q + 0]);
+        }
+        zj(CY[1], MUL_NONE, CY[2], MUL_NONE, R[14], R[13]);
+        zj(CY[0], MUL_IK, nullptr, 0, R[15], nullptr);
+        zj(CY[14], MUL_NONE, CY[13], MUL_NONE, R[16], R[17]);
+        zj(CY[12], MUL_IK, nullptr, 0, R[18], nullptr);
+        // F': r2c of the 15 scaled derivatives R[4..18] -> CY[0..14]
+        c->zS_F = (int)Z.size();
+        for (int j = 0; j < 14; j += 2) zj(R[4 + j], 0, R[5 + j], 0, CY[j], CY[j + 1]);
+        zj(R[18], 0, nullptr, 0, CY[14], nullptr);
+        c->jS_Fy = (int)J.size();
+        for (int j = 0; j < 15; ++j) aj(CY[j], SX[j], MUL_NONE);
+        c->jS_Fx = (int)J.size();
+        for (int j = 0; j < 15; ++j) aj(SX[j], CY[j], MUL_NONE);
+        // G': c2r(P D_d u'_c), c2r(P D_d s) -> R[4..15] (the products' operands)
+        c->jS_Gx = (int)J.size();
+        for (int j = 0; j < 12; ++j) aj(CY[j], SX[j], MUL_P);
+        c->jS_Gy = (int)J.size();
+        for (int j = 0; j < 12; ++j) aj(SX[j], CX[j], MUL_NONE);
+        c->zS_G = (int)Z.size();
+        for (int j = 0; j < 12; j += 2) zj(CX[j], MUL_NONE, CX[j + 1], MUL_NONE, R[4 + j], R[5 + j]);
+        // I': r2c of the products R[20..23] -> SX[8..11]
+        c->zS_I = (int)Z.size();
+        zj(R[20], 0, R[21], 0, SX[0], SX[1]);
+        zj(R[22], 0, R[23], 0, SX[2], SX[3]);
+        c->jS_Iy = (int)J.size();
+        for (int q = 0; q < 4; ++q) aj(SX[q], SX[4 + q], MUL_NONE);
+        c->jS_Ix = (int)J.size();
+        for (int q = 0; q < 4; ++q) aj(SX[4 + q], SX[8 + q], MUL_NONE);
+        // K': penalization, K -> R[20..23] -> K
+        c->jS_Kx = (int)J.size();
+        for (int q = 0; q < 4; ++q) aj(c->K[q], SX[q], MUL_NONE);
+        c->jS_Ky = (int)J.size();
+        for (int q = 0; q < 4; ++q) aj(SX[q], SX[4 + q], MUL_NONE);
+        c->zS_K = (int)Z.size();
+        zj(SX[4], MUL_NONE, SX[5], MUL_NONE, R[20], R[21]);
+        zj(SX[6], MUL_NONE, SX[7], MUL_NONE, R[22], R[23]);
+        c->zS_Kf = (int)Z.size();
+        zj(R[20], 0, R[21], 0, SX[0], SX[1]);
+        zj(R[22], 0, R[23], 0, SX[2], SX[3]);
+        c->jS_Kfy = (int)J.size();
+        for (int q = 0; q < 4; ++q) aj(SX[q], SX[4 + q], MUL_NONE);
+        c->jS_Kfx = (int)J.size();
+        for (int q = 0; q < 4; ++q) aj(SX[4 + q], c->K[q], MUL_NONE);
+    }
     c->hj = J;
     c->hz = Z;
     c->dj = dalloc<AxisJob>(c, sizeof(AxisJob) * J.size());
@@ -1147,6 +1413,9 @@ void create(kf_ctx *c) {
     if (cf.precision != KF_FP64 && cf.precision != KF_FP32_BULK) throw KfError{KF_ERR_ARG, "precision"};
     if (cf.pen_eta > 0.) throw KfError{KF_ERR_ARG, "penalization damping must be <= 0 (effect_penalization.cpp:7-12)"};
     if (!(cf.L > 0.) || !(cf.theta != 0.)) throw KfError{KF_ERR_ARG, "L > 0 and theta != 0 required"};
+    if (!(cf.stretch_m >= 0.) || !(2. * acos(-1.) * cf.stretch_m < cf.L))
+        throw KfError{KF_ERR_ARG, "stretch_m must satisfy 0 <= 2 pi m < L (a monotone axis_CoSiSt map)"};
+    c->stretched = cf.stretch_m != 0.;
     c->fp32 = cf.precision == KF_FP32_BULK;
     c->es = c->fp32 ? 4 : 8;
     c->cs = 2 * c->es;
@@ -1170,6 +1439,8 @@ void create(kf_ctx *c) {
     for (int i = 0; i < 12; ++i) c->CX[i] = dalloc<void>(c, cb);
     for (int i = 0; i < 16; ++i) c->CY[i] = dalloc<void>(c, cb);
     for (int i = 0; i < 24; ++i) c->R[i] = dalloc<void>(c, rb);
+    if (c->stretched)
+        for (int i = 0; i < 15; ++i) c->SX[i] = dalloc<void>(c, cb);
     c->phihat = dalloc<void>(c, cb);
     c->phi = dalloc<double>(c, 8 * c->N);
     c->rho = dalloc<double>(c, 8 * c->N);
@@ -1787,11 +2058,11 @@ int kf_diag(kf_ctx *c, kf_diag_out *out) {
         if (c->fp32)
             k_diag_sums<float><<<nb, RBS, 0, c->st>>>((const float *)c->R[23], (const float *)c->R[20],
                                                      (const float *)c->R[21], (const float *)c->R[22], c->phi, c->nd,
-                                                     c->cfg.M, c->N, c->partial);
+                                                     c->cfg.M, c->N, c->partial, c->vol, c->n);
         else
             k_diag_sums<double><<<nb, RBS, 0, c->st>>>((const double *)c->R[23], (const double *)c->R[20],
                                                       (const double *)c->R[21], (const double *)c->R[22], c->phi,
-                                                      c->nd, c->cfg.M, c->N, c->partial);
+                                                      c->nd, c->cfg.M, c->N, c->partial, c->vol, c->n);
         k_diag_final<<<1, 32, 0, c->st>>>(c->partial, nb, c->red);
         c->launches++;
         CK(cudaGetLastError());

@@ -150,8 +150,8 @@ void write_file(kf_ctx *c, const std::string &path, double t, bool plane, double
     F.str("path", self_path());
     for (const char *ax : {"x", "y", "z"}) {
         const std::string a(ax);
-        F.i32("domain/type_" + a, 1);  // axis_CoEqSt
-        F.f64("domain/m_" + a, 0.);
+        F.i32("domain/type_" + a, c->stretched ? 3 : 1);  // axis_CoSiSt : axis_CoEqSt
+        F.f64("domain/m_" + a, cf.stretch_m);
         F.f64("domain/l0_" + a, -0.5 * cf.L);
         F.i32("domain/N_" + a, c->n);
         F.f64("domain/L_" + a, cf.L);
@@ -419,6 +419,11 @@ int kf_file_info_read(const char *path, kf_file_info *info) {
     }
     r.n = n;
     r.kind = ux->dims.size() == 2 ? KF_FILE_SLICE : KF_FILE_BACKUP;
+    int32_t type = 1;
+    r.m = 0.;
+    F.get_i32("domain/type_x", type);
+    r.type = type;
+    F.get_f64("domain/m_x", r.m);
     *info = r;
     return KF_OK;
 }
@@ -430,10 +435,13 @@ int kf_load(kf_ctx *c, const char *path, double *t_out) {
         std::string err;
         if (!F.read(path, err)) throw KfError{KF_ERR_ARG, err};
         for (const char *ax : {"x", "y", "z"}) {
-            int32_t n = 0;
-            double L = 0.;
+            int32_t n = 0, type = 1;
+            double L = 0., m = 0.;
+            F.get_i32(std::string("domain/type_") + ax, type);
+            F.get_f64(std::string("domain/m_") + ax, m);
             if (!F.get_i32(std::string("domain/N_") + ax, n) || !F.get_f64(std::string("domain/L_") + ax, L) ||
-                n != c->n || std::fabs(L - c->cfg.L) > 1e-12 * c->cfg.L)
+                n != c->n || std::fabs(L - c->cfg.L) > 1e-12 * c->cfg.L || type != (c->stretched ? 3 : 1) ||
+                std::fabs(m - c->cfg.stretch_m) > 1e-12 * c->cfg.L)
                 throw KfError{KF_ERR_ARG, std::string(path) + ": grid differs from the context's"};
         }
         const char *names[5] = {"Ux", "Uy", "Uz", "ni", "Ph"};

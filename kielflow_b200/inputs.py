@@ -32,10 +32,38 @@ L_DEFAULT = 2.0 * math.pi * 4.0
 _MASK64 = (1 << 64) - 1
 
 
-def axis_values(n: int, L: float) -> np.ndarray:
-    """``axis_CoEqSt::val_at(i) = l0 + i*(L/N)`` for i < n, l0 = -L/2."""
+def val_at(i: int, n: int, L: float, m: float = 0.0) -> float:
+    """Position of index i (-1 <= i <= n): ``axis_CoEqSt::val_at`` = l0 + i*(L/N)
+    for m == 0, else ``axis_CoSiSt::val_at`` (axis_SiSt.cpp:93-116), the
+    periodic extension of S(l0 + L i/N) with S(x) = x - m sin(2 pi x/L)."""
     l0 = -0.5 * L
-    return np.array([l0 + i * (L / n) for i in range(n)], dtype=np.float64)
+    if m == 0.0:
+        return l0 + i * (L / n)
+    shift = 0
+    if i < 0:
+        while True:
+            shift += 1
+            if not i + shift * n < 0:
+                break
+    if i >= n:
+        while True:
+            shift -= 1
+            if not i + shift * n >= n - 1:
+                break
+    pi = math.acos(-1.0)
+    x = l0 + L * float(i + shift * n) / n
+    return (x - m * math.sin(2.0 * pi * x / L)) - shift * L
+
+
+def axis_values(n: int, L: float, m: float = 0.0) -> np.ndarray:
+    """val_at(i) for i < n (axis_CoEqSt, or axis_CoSiSt for m > 0)."""
+    return np.array([val_at(i, n, L, m) for i in range(n)], dtype=np.float64)
+
+
+def frontend_stretch(L: float) -> float:
+    """The stretching the reference's frontend uses, m = L (1 - 0.3) / (2 pi)
+    (frontend.cpp:285-287): cells at the box centre are 0.3 h wide."""
+    return L * (1.0 - 0.3) / (2.0 * math.acos(-1.0))
 
 
 def k_values(n: int, L: float) -> np.ndarray:
@@ -118,27 +146,28 @@ def initial_state(n: int, seed: int = 0, amp: float = 1e-3, kmax: int = 4):
     return Hu[0], Hu[1], Hu[2], Fs
 
 
-def gauss_charge(n: int, L: float, Q: float, sigma: float) -> np.ndarray:
+def gauss_charge(n: int, L: float, Q: float, sigma: float, m: float = 0.0) -> np.ndarray:
     """``fkt3d_Gauss(Q, sigma, sigma, sigma)`` sampled on the grid
     (masks.hpp:351-366, filled as field_real::fill, field_real.cpp:78-95)."""
     pi = math.acos(-1.0)
     A = Q / (math.pow(math.sqrt(pi), 3.0) * sigma * sigma * sigma)
-    x = axis_values(n, L)
+    x = axis_values(n, L, m)
     X = (x / sigma) ** 2
     e = -X[:, None, None] - X[None, :, None] - X[None, None, :]
     return A * np.exp(e)
 
 
-def sphere_mask(n: int, L: float, radius: float) -> np.ndarray:
-    x = axis_values(n, L)
+def sphere_mask(n: int, L: float, radius: float, m: float = 0.0) -> np.ndarray:
+    x = axis_values(n, L, m)
     r2 = x[:, None, None] ** 2 + x[None, :, None] ** 2 + x[None, None, :] ** 2
     return (r2 < radius * radius).astype(np.float64)
 
 
-def cfl_dt(state, n: int, L: float, M: float, cfl: float = 0.2) -> float:
-    """dt = cfl * h / max(|M + u'_x|, |u'_y|, |u'_z|) from the initial state,
-    then held fixed (the reference's RK4 keeps dt_ fixed, RKO4.cpp:41-47)."""
-    h = L / n
+def cfl_dt(state, n: int, L: float, M: float, cfl: float = 0.2, m: float = 0.0) -> float:
+    """dt = cfl * h_min / max(|M + u'_x|, |u'_y|, |u'_z|) from the initial
+    state, then held fixed (the reference's RK4 keeps dt_ fixed,
+    RKO4.cpp:41-47); h_min = h (1 - 2 pi m / L) on a stretched axis."""
+    h = L / n * (1.0 - 2.0 * math.acos(-1.0) * m / L)
     ux = np.fft.irfftn(state[0], s=(n, n, n), axes=(0, 1, 2))
     uy = np.fft.irfftn(state[1], s=(n, n, n), axes=(0, 1, 2))
     uz = np.fft.irfftn(state[2], s=(n, n, n), axes=(0, 1, 2))

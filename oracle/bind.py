@@ -44,7 +44,7 @@ class KfoConfig(ctypes.Structure):
         ("terms", ctypes.c_int), ("poisson_mode", ctypes.c_int), ("nlj_max_it", ctypes.c_int),
         ("nlj_limit", ctypes.c_double), ("res_tol", ctypes.c_double), ("mg_levels", ctypes.c_int),
         ("mg_pre", ctypes.c_int), ("mg_post", ctypes.c_int), ("coarse_tol", ctypes.c_double),
-        ("max_cycles", ctypes.c_int), ("phi_extrap", ctypes.c_int),
+        ("max_cycles", ctypes.c_int), ("phi_extrap", ctypes.c_int), ("stretch_m", ctypes.c_double),
     ]
 
 
@@ -87,6 +87,9 @@ def lib():
         L.kfo_set_phi.argtypes = [ctypes.c_void_p, _D]
         L.kfo_get_phi.argtypes = [ctypes.c_void_p, _D]
         L.kfo_rhs.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        L.kfo_positions.argtypes = [ctypes.c_void_p, _D]
+        L.kfo_metric.argtypes = [ctypes.c_void_p, _D]
+        L.kfo_deriv.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D]
         L.kfo_rk4.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
         L.kfo_poisson.argtypes = [ctypes.c_void_p, _D, _D]
         L.kfo_poisson_stats_get.argtypes = [ctypes.c_void_p, ctypes.POINTER(KfoStats)]
@@ -112,7 +115,13 @@ def ref():
         R = ctypes.CDLL(REF_SO)
         R.kfref_create.restype = ctypes.c_void_p
         R.kfref_create.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
-                                   ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_double]
+                                   ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                   ctypes.c_double]
+        R.kfref_positions.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, _D]
+        R.kfref_deriv_m.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, _D, _D]
+        R.kfref_mg_solve_m.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, _D, _D]
+        R.kfref_gauss_m.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_double, _D]
         R.kfref_destroy.argtypes = [ctypes.c_void_p]
         R.kfref_last_error.restype = ctypes.c_char_p
         R.kfref_set_state.argtypes = [ctypes.c_void_p, _D, _D, _D, _D]
@@ -139,10 +148,10 @@ def ref():
 def config(n, L, M, tau=0.1, theta=30.0, diff_D=0.0, sv_eps=0.5, sv_cut=0.0, pen_eta=0.0,
            terms=KFO_SHIPPED, poisson_mode=PS_JACOBI_REF, nlj_max_it=80, nlj_limit=0.5e-5,
            res_tol=1e-10, mg_levels=4, mg_pre=2, mg_post=2, coarse_tol=1e-13, max_cycles=50,
-           phi_extrap=0):
+           phi_extrap=0, stretch_m=0.0):
     return KfoConfig(n, L, M, tau, theta, diff_D, sv_eps, sv_cut, pen_eta, terms, poisson_mode,
                      nlj_max_it, nlj_limit, res_tol, mg_levels, mg_pre, mg_post, coarse_tol,
-                     max_cycles, phi_extrap)
+                     max_cycles, phi_extrap, stretch_m)
 
 
 class Oracle:
@@ -219,6 +228,25 @@ class Oracle:
         self.L.kfo_tables(self.h, _p(P), _p(SV), _p(PF))
         return P, SV, PF
 
+    def positions(self):
+        """val_at(i) for i = -1 .. n."""
+        out = np.zeros(self.n + 2)
+        self.L.kfo_positions(self.h, _p(out))
+        return out
+
+    def deriv(self, d, F):
+        """OP_partial_derivative along axis d of a half spectrum."""
+        F = np.ascontiguousarray(F, np.complex128)
+        out = np.zeros(self.shape_c, np.complex128)
+        self.L.kfo_deriv(self.h, d, F.ctypes.data_as(_D), out.ctypes.data_as(_D))
+        return out
+
+    def metric(self):
+        """The filtered 1/dS of the derivative along one axis (n values)."""
+        out = np.zeros(self.n)
+        self.L.kfo_metric(self.h, _p(out))
+        return out
+
 
 def r2c(x: np.ndarray) -> np.ndarray:
     n = x.shape[0]
@@ -251,10 +279,10 @@ class Reference:
     (compiled from its sources) on one grid."""
 
     def __init__(self, n, L, M, tau=0.1, theta=30.0, poisson_mode=1, nlj_max_it=80,
-                 nlj_limit=0.5e-5):
+                 nlj_limit=0.5e-5, m=0.0):
         self.R = ref()
         self.n = n
-        self.h = self.R.kfref_create(n, L, M, tau, theta, poisson_mode, nlj_max_it, nlj_limit)
+        self.h = self.R.kfref_create(n, L, M, tau, theta, poisson_mode, nlj_max_it, nlj_limit, m)
         if not self.h:
             raise RuntimeError(self.R.kfref_last_error().decode())
         self.shape_c = (n, n, n // 2 + 1)

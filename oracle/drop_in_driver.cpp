@@ -9,7 +9,8 @@
  *      rhs_standard and Runge_kutta_O4;
  *   2. with kf_gpu_rhs / kf_gpu_rk4 from include/kf_adapters.hpp in their place,
  *      the loop body unchanged.
- * Usage: drop_in_driver <dir> <n> <M> <tau> <theta> <dt> <nsteps>; <dir> holds
+ * Usage: drop_in_driver <dir> <n> <M> <tau> <theta> <dt> <nsteps> [m]; with m
+ * the axes are axis_CoSiSt(-L/2, L, n, m) (the frontend's grid); <dir> holds
  * state.bin (4 half spectra, interleaved doubles), nd.bin, mask.bin (n^3
  * doubles); writes ref_state.bin and gpu_state.bin.
  */
@@ -20,6 +21,7 @@
 
 #include "RKO4.hpp"
 #include "axis_EqSt.hpp"
+#include "axis_SiSt.hpp"
 #include "field.hpp"
 #include "grid.hpp"
 #include "interface_ODE_solver.hpp"
@@ -50,8 +52,8 @@ static bool write_bin(const std::string &p, const double *src, size_t count) {
 }
 
 int main(int argc, char **argv) {
-    if (argc != 8) {
-        std::fprintf(stderr, "usage: %s dir n M tau theta dt nsteps\n", argv[0]);
+    if (argc != 8 && argc != 9) {
+        std::fprintf(stderr, "usage: %s dir n M tau theta dt nsteps [m]\n", argv[0]);
         return 2;
     }
     const std::string dir = argv[1];
@@ -60,7 +62,10 @@ int main(int argc, char **argv) {
     const double dt = std::atof(argv[6]);
     const int nsteps = std::atoi(argv[7]);
     const double L = 2. * acos(-1.) * 4.;
-    axis_CoEqSt ax(-0.5 * L, L, n);
+    const double m = argc == 9 ? std::atof(argv[8]) : 0.;
+    axis_CoEqSt axe(-0.5 * L, L, n);
+    axis_CoSiSt axs(-0.5 * L, L, n, m);
+    const axis &ax = m != 0. ? static_cast<const axis &>(axs) : static_cast<const axis &>(axe);
     grid Omega(ax, ax, ax);
     parameters Params(M, tau, theta, 0., 0.);
     field_imag FUx(Omega), FUy(Omega), FUz(Omega), Fni(Omega);

@@ -37,11 +37,39 @@ namespace {
 
 typedef std::vector<double> vec;
 
-/* axis_CoEqSt (axis_EqSt.cpp:52-61) */
+/* axis_CoEqSt (axis_EqSt.cpp:52-61) and, with m > 0, axis_CoSiSt: the
+ * periodic sine-stretched axis x = S(l0 + L i/N), S(x) = x - m sin(2 pi x/L)
+ * (axis_SiSt.cpp:93-116 val_at, :153-164 S and dS; k_val_at :120-124 is the
+ * equidistant one). */
 struct axis_eq {
     double l0, L;
     int N;
-    double val_at(int i) const { return l0 + i * (L / N); }
+    double m = 0.;
+    double S(double x) const {
+        const double pi = acos(-1.);
+        return x - m * sin(2. * pi * x / L);
+    }
+    double val_at(int index) const {
+        if (m == 0.) return l0 + index * (L / N);
+        int shift = 0;
+        if (index < 0) {
+            do {
+                shift += 1;
+            } while (index + shift * N < 0);
+        }
+        if (index >= N) {
+            do {
+                shift -= 1;
+            } while (index + shift * N >= N - 1);
+        }
+        double x = l0 + L * double(index + shift * N) / (N);
+        return S(x) - shift * L;
+    }
+    double dS(int index) const {
+        const double pi = acos(-1.);
+        double x = l0 + (L / N) * index;
+        return 1. - (2. * pi * m / L) * cos(2. * pi * x / L);
+    }
     double k_val_at(int i) const {
         double pi = acos(-1.);
         return ((i <= N / 2) ? (2. * pi * i / L) : (2. * pi * (i - N) / L));
@@ -76,11 +104,12 @@ struct level {
     vec H;                  /* H[i] = val_at(i) - val_at(i-1), i = 0..n */
     vec dd, den_p, den_m;   /* 2/(H[i+1]H[i]), H[i+1](H[i+1]+H[i]), H[i](H[i+1]+H[i]) */
     vec inv_p, inv_m;       /* 2/den_p, 2/den_m: stencil weights of the FAS cycle      */
-    void init(int n_, double L) {
+    void init(int n_, double L, double m) {
         n = n_;
         ax.l0 = -0.5 * L;
         ax.L = L;
         ax.N = n_;
+        ax.m = m;
         H.resize(n + 1);
         for (int i = 0; i < n + 1; ++i) H[i] = ax.val_at(i) - ax.val_at(i - 1);
         dd.resize(n);
@@ -151,6 +180,8 @@ struct kfo_ctx {
     vec kv;                    /* k_val_at(i) */
     vec P, SV, PF, K2;         /* dealias mask, SV table, phi filter, |k|^2  (Nc) */
     vec FU[3], Fs;             /* state (interleaved complex) */
+    bool stretched = false;    /* axis_CoSiSt: derivatives take the chain-rule path */
+    vec dsv[3];                /* filtered 1/dS per direction (N), OP_partial_derivative.cpp:60-80 */
     vec Phi, nd, mask;         /* real fields */
     /* Jacobi solver state that persists across calls (solver_poisson_jacobi_nlin.hpp:66-95) */
     double norm_max = 0., norm_sum = 0., norm_max_old = -1., norm_sum_old = -1.;
@@ -188,7 +219,9 @@ void dealias(const kfo_ctx *c, vec &F) {
     }
 }
 
-/* OP_partial_derivative::operator(), uniform-grid branch (OP_partial_derivative.cpp:111-119) */
+/* OP_partial_derivative::operator() (OP_partial_derivative.cpp:104-136): i k
+ * times the input; on a stretched axis, then dealiased, taken to physical
+ * space, multiplied by the filtered 1/dS of the direction and transformed back. */
 void deriv(const kfo_ctx *c, int dir, const vec &in, vec &out) {
     out.resize(2 * c->Nc);
     const int n = c->n, nzc = c->nzc;
@@ -202,6 +235,13 @@ void deriv(const kfo_ctx *c, int dir, const vec &in, vec &out) {
                 out[2 * ijk] = -kk * in[2 * ijk + 1];
                 out[2 * ijk + 1] = kk * tmp;
             }
+    if (!c->stretched) return;
+    dealias(c, out);
+    vec t;
+    c2r(c, out, t);
+    const vec &d = c->dsv[dir];
+    for (size_t i = 0; i < c->N; ++i) t[i] = t[i] * d[i];
+    r2c(c, t, out);
 }
 
 void add(vec &a, const vec &b) {
@@ -298,9 +338,9 @@ void inject(int nf, int step, const vec &in, vec &out) {
 
 /* OP_hto2h: trilinear prolongation in z, then y, then x passes
  * (field_interpolation.cpp:56-147), on the axis of the fine level. */
-void prolong(int nc, double L, const vec &in, vec &out) {
+void prolong(int nc, double L, double m, const vec &in, vec &out) {
     int nf = 2 * nc;
-    axis_eq ax{-0.5 * L, L, nf};
+    axis_eq ax{-0.5 * L, L, nf, m};
     out.assign((size_t)nf * nf * nf, 0.);
     auto id = [nf](int i, int j, int k) { return (size_t)k + nf * ((size_t)j + (size_t)i * nf); };
     auto w = [nf](int i) { return i < 0 ? i + nf : (i > nf - 1 ? i - nf : i); };
@@ -439,7 +479,7 @@ void fas_vcycle(kfo_ctx *c, int l, vec &phi, const vec &rho) {
     fas_vcycle(c, l + 1, phic, rhoc);
     for (size_t q = 0; q < phic.size(); ++q) phic[q] = phic[q] - phic0[q];
     vec e;
-    prolong(Lc.n, cf.L, phic, e);
+    prolong(Lc.n, cf.L, cf.stretch_m, phic, e);
     for (size_t q = 0; q < phi.size(); ++q) phi[q] += e[q];
     for (int s = 0; s < cf.mg_post; ++s) rbgs_sweep(L, phi, rho);
 }
@@ -458,13 +498,13 @@ void cascadic_solve(kfo_ctx *c, vec &phi, const vec &rho) {
             inject(ncur, 8, cur, nxt);
             ncur /= 8;
         } else {
-            prolong(ncur, c->cfg.L, cur, nxt);
+            prolong(ncur, c->cfg.L, c->cfg.stretch_m, cur, nxt);
             ncur *= 2;
         }
         vec rho_n;
         inject(n, n / ncur, rho, rho_n); /* repeated injection == one strided injection */
         level L;
-        L.init(ncur, c->cfg.L);
+        L.init(ncur, c->cfg.L, c->cfg.stretch_m);
         int max_it = steps[cas];
         jacobi_solve(c, L, nxt, rho_n, max_it, tol[cas], false, 0.);
         cur.swap(nxt);
@@ -680,7 +720,7 @@ kfo_ctx *kfo_create(const kfo_config *cfg) {
     c->nzc = n / 2 + 1;
     c->N = (size_t)n * n * n;
     c->Nc = (size_t)n * n * c->nzc;
-    c->ax = axis_eq{-0.5 * cfg->L, cfg->L, n};
+    c->ax = axis_eq{-0.5 * cfg->L, cfg->L, n, cfg->stretch_m};
     c->kv.resize(n);
     for (int i = 0; i < n; ++i) c->kv[i] = c->ax.k_val_at(i);
     const double kmax = c->ax.k_val_at(n / 2);
@@ -715,11 +755,42 @@ kfo_ctx *kfo_create(const kfo_config *cfg) {
     c->mask.assign(c->N, 0.);
     int levels = cfg->poisson_mode == KFO_PS_FAS ? (cfg->mg_levels > 0 ? cfg->mg_levels : 1) : 1;
     c->lv.resize(levels);
-    for (int l = 0; l < levels; ++l) c->lv[l].init(n >> l, cfg->L);
+    for (int l = 0; l < levels; ++l) c->lv[l].init(n >> l, cfg->L, cfg->stretch_m);
+    /* OP_partial_derivative.cpp:60-80: dS_val = 1/dS of the direction's index,
+     * dealiased through FFT, the 2/3 filter and the inverse FFT */
+    c->stretched = cfg->stretch_m != 0.;
+    if (c->stretched)
+        for (int d = 0; d < 3; ++d) {
+            vec f(c->N), F;
+            for (int i = 0; i < n; ++i)
+                for (int j = 0; j < n; ++j)
+                    for (int k = 0; k < n; ++k) {
+                        const int q = d == 0 ? i : (d == 1 ? j : k);
+                        f[(size_t)k + n * ((size_t)j + (size_t)i * n)] = 1. / c->ax.dS(q);
+                    }
+            r2c(c, f, F);
+            dealias(c, F);
+            c2r(c, F, c->dsv[d]);
+        }
     return c;
 }
 
 void kfo_destroy(kfo_ctx *c) { delete c; }
+
+void kfo_positions(kfo_ctx *c, double *out) {
+    for (int i = -1; i <= c->n; ++i) out[i + 1] = c->ax.val_at(i);
+}
+
+void kfo_deriv(kfo_ctx *c, int dir, const double *in, double *out) {
+    vec a(in, in + 2 * c->Nc), b;
+    deriv(c, dir, a, b);
+    std::memcpy(out, b.data(), sizeof(double) * 2 * c->Nc);
+}
+
+void kfo_metric(kfo_ctx *c, double *out) {
+    const int n = c->n;
+    for (int i = 0; i < n; ++i) out[i] = c->stretched ? c->dsv[0][(size_t)i * n * n] : 1.;
+}
 
 void kfo_set_state(kfo_ctx *c, const double *ux, const double *uy, const double *uz,
                    const double *s) {
@@ -820,7 +891,7 @@ void kfo_c2r(int n, const double *in, double *out) {
 void kfo_transfer(int kind, int n, double L, const double *in, double *out) {
     size_t N = (size_t)n * n * n;
     vec a(in, in + N), b;
-    if (kind == 0) prolong(n, L, a, b);
+    if (kind == 0) prolong(n, L, 0., a, b);
     else if (kind == 1) inject(n, 2, a, b);
     else restrict_fw(n, a, b);
     std::memcpy(out, b.data(), sizeof(double) * b.size());

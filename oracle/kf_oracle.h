@@ -56,6 +56,8 @@ typedef struct {
     double coarse_tol;   /* FAS coarsest-level residual target                   */
     int max_cycles;      /* FAS V-cycle cap per solve                            */
     int phi_extrap;      /* linear extrapolation of phi in time for the start    */
+    double stretch_m;    /* 0: axis_CoEqSt; > 0: axis_CoSiSt(-L/2, L, n, m) on   */
+                         /* all three axes (sine-stretched, axis_SiSt.cpp)       */
 } kfo_config;
 
 typedef struct kfo_ctx kfo_ctx;
@@ -77,6 +79,13 @@ void kfo_set_sources(kfo_ctx *c, const double *nd, const double *mask);
 void kfo_set_phi(kfo_ctx *c, const double *phi);
 void kfo_get_phi(kfo_ctx *c, double *phi);
 int kfo_rhs(kfo_ctx *c, double t);
+/* positions val_at(i), i = -1..n (n + 2 values), of the context's axis */
+void kfo_positions(kfo_ctx *c, double *out);
+/* the derivative's metric factor 1/dS of direction 0 after the 2/3 filter
+ * (OP_partial_derivative.cpp:60-80), along that axis: n values */
+void kfo_metric(kfo_ctx *c, double *out);
+/* OP_partial_derivative on the context's grid: out = d/dx_dir of in (half spectra) */
+void kfo_deriv(kfo_ctx *c, int dir, const double *in, double *out);
 int kfo_rk4(kfo_ctx *c, double dt, int nsteps);
 double kfo_time(kfo_ctx *c);
 int kfo_poisson(kfo_ctx *c, double *phi_io, const double *rho);

@@ -3,7 +3,7 @@
  *
  * TEST INFRASTRUCTURE (oracle/_ref).  Compiled together with the reference's
  * unmodified sources (RKO4.cpp, rhs_standard.cpp, OP_*.cpp, operations.cpp,
- * field_*.cpp, field_interpolation.cpp, axis_EqSt.cpp, grid_base.cpp,
+ * field_*.cpp, field_interpolation.cpp, axis_EqSt.cpp, axis_SiSt.cpp, grid_base.cpp,
  * solver_poisson_jacobi_nlin.cpp, solver_poisson_multigrid.cpp, parameters.cpp)
  * so that the Python tests can drive the reference exactly as its driver does
  * (kielflow.cpp:156-286) on seeded in-memory inputs instead of HDF5 files.
@@ -16,6 +16,7 @@
 
 #include "RKO4.hpp"
 #include "axis_EqSt.hpp"
+#include "axis_SiSt.hpp"
 #include "field.hpp"
 #include "grid.hpp"
 #include "masks.hpp"
@@ -32,7 +33,11 @@
 
 namespace {
 
-grid make_grid(int n, double L) {
+grid make_grid(int n, double L, double m = 0.) {
+    if (m != 0.) {
+        axis_CoSiSt ax(-0.5 * L, L, n, m);
+        return grid(ax, ax, ax);
+    }
     axis_CoEqSt ax(-0.5 * L, L, n);
     return grid(ax, ax, ax);
 }
@@ -59,8 +64,8 @@ struct kfref_ctx {
     solver_poisson_jacobi_nlin nlj;
     solver_poisson_multigrid mg;
     std::unique_ptr<rhs_probe> rhs;
-    kfref_ctx(int n_, double L_, double M, double tau, double theta)
-        : n(n_), L(L_), omega(make_grid(n_, L_)), params(M, tau, theta, 0., 0.),
+    kfref_ctx(int n_, double L_, double M, double tau, double theta, double m)
+        : n(n_), L(L_), omega(make_grid(n_, L_, m)), params(M, tau, theta, 0., 0.),
           FUx(omega), FUy(omega), FUz(omega), Fni(omega), nd(omega), mask(omega), Phi(omega),
           bshape(0.), bvalue(0.), nlj(bshape, bvalue, .8), mg(nlj) {
         for (int i = 0; i < nd.N; ++i) nd.val[i] = mask.val[i] = Phi.val[i] = 0.;
@@ -76,11 +81,13 @@ const char *kfref_last_error(void) { return g_err.c_str(); }
 
 /* poisson_mode 0: the nonlinear Jacobi solver used directly as the RHS's
  * interface_poisson_solver (max_it sweeps, relative-update limit);
- * poisson_mode 1: the cascadic multigrid plan of kielflow.cpp:199-217. */
+ * poisson_mode 1: the cascadic multigrid plan of kielflow.cpp:199-217.
+ * m: 0 for axis_CoEqSt axes, else axis_CoSiSt(-L/2, L, n, m) axes (the
+ * frontend's grid, frontend.cpp:285-287). */
 kfref_ctx *kfref_create(int n, double L, double M, double tau, double theta, int poisson_mode,
-                        int nlj_max_it, double nlj_limit_max) {
+                        int nlj_max_it, double nlj_limit_max, double m) {
     try {
-        kfref_ctx *c = new kfref_ctx(n, L, M, tau, theta);
+        kfref_ctx *c = new kfref_ctx(n, L, M, tau, theta, m);
         c->nlj.set_max_iterations(nlj_max_it);
         c->nlj.set_limit_NormMax(nlj_limit_max);
         c->nlj.set_limit_NormSum(.5e-7);
@@ -271,6 +278,53 @@ int kfref_transfer(int kind, int n, double L, const double *in, double *out) {
     } catch (const char *e) { g_err = e; } catch (const std::string &e) { g_err = e; }
     catch (...) { g_err = "unknown exception"; }
     return -1;
+}
+
+/* Stretched-grid (axis_CoSiSt, m != 0) forms of the entries above. */
+void kfref_positions(int n, double L, double m, double *out) {
+    grid g = make_grid(n, L, m);
+    for (int i = -1; i <= n; ++i) out[i + 1] = g.x_axis->val_at(i);
+}
+
+void kfref_deriv_m(int n, double L, double m, int dir, const double *in, double *out) {
+    grid g = make_grid(n, L, m);
+    field_imag a(g), b(g);
+    put_c(a, in);
+    OP_partial_derivative op(g, dir == 0 ? e_x : (dir == 1 ? e_y : e_z));
+    op(a, b);
+    get_c(b, out);
+}
+
+int kfref_mg_solve_m(int n, double L, double m, double *phi_io, const double *rho) {
+    try {
+        grid g = make_grid(n, L, m);
+        field_real phi(g), r(g);
+        std::memcpy(phi.val, phi_io, sizeof(double) * phi.N);
+        std::memcpy(r.val, rho, sizeof(double) * r.N);
+        fkt3d_const bs(0.), bv(0.);
+        solver_poisson_jacobi_nlin nlj(bs, bv, .8);
+        nlj.set_max_iterations(80);
+        nlj.set_limit_NormMax(.5e-5);
+        nlj.set_limit_NormSum(.5e-7);
+        solver_poisson_multigrid mg(nlj);
+        int steps[4] = {0, -1, -1, -1};
+        MG_lvl_control shape[4] = {lvl_down3, lvl_up, lvl_up, lvl_up};
+        double tol[4] = {0.01, 0.0005, 0.0001, 0.0001};
+        mg.set_level_control(4, steps, shape, tol);
+        mg.solve(phi, r);
+        std::memcpy(phi_io, phi.val, sizeof(double) * phi.N);
+        return 0;
+    } catch (const char *e) { g_err = e; } catch (const std::string &e) { g_err = e; }
+    catch (...) { g_err = "unknown exception"; }
+    return -1;
+}
+
+void kfref_gauss_m(int n, double L, double m, double Q, double sigma, double *out) {
+    grid g = make_grid(n, L, m);
+    field_real f(g);
+    fkt3d_Gauss fk(Q, sigma, sigma, sigma);
+    f.fill(fk);
+    std::memcpy(out, f.val, sizeof(double) * f.N);
 }
 
 /* fkt3d_Gauss (masks.hpp:351-366) sampled on the grid through field_real::fill. */

@@ -20,18 +20,23 @@ DRIVER = os.path.join(ROOT, "oracle", "_ref", "drop_in_driver")
 
 
 @pytest.mark.skipif(not os.path.exists(DRIVER), reason="drop-in driver not built (needs the reference sources)")
-@pytest.mark.parametrize("n,steps", [(16, 3), (32, 2)])
-def test_reference_loop_with_gpu_adapters(tmp_path, n, steps):
+@pytest.mark.parametrize("n,steps,stretched", [(16, 3, False), (32, 2, False), (16, 3, True)])
+def test_reference_loop_with_gpu_adapters(tmp_path, n, steps, stretched):
+    """stretched: the frontend's axis_CoSiSt grid, read by the adapter from the
+    reference's own grid object."""
     L = I.L_DEFAULT
-    M, tau, theta, dt = 0.8, 0.1, 30.0, 0.05
+    m = I.frontend_stretch(L) if stretched else 0.0
+    M, tau, theta, dt = 0.8, 0.1, 30.0, 0.05 if not stretched else 0.02
     st = I.initial_state(n, seed=21)
-    nd = I.gauss_charge(n, L, -10.0, 0.5)
-    mask = I.sphere_mask(n, L, 0.5)
+    nd = I.gauss_charge(n, L, -10.0, 0.5, m)
+    mask = I.sphere_mask(n, L, 0.5, m)
     np.concatenate([np.ascontiguousarray(a).view(np.float64).ravel() for a in st]).tofile(tmp_path / "state.bin")
     nd.tofile(tmp_path / "nd.bin")
     mask.tofile(tmp_path / "mask.bin")
-    r = subprocess.run([DRIVER, str(tmp_path), str(n), str(M), str(tau), str(theta), str(dt), str(steps)],
-                       capture_output=True, text=True, timeout=600)
+    args = [DRIVER, str(tmp_path), str(n), str(M), str(tau), str(theta), str(dt), str(steps)]
+    if stretched:
+        args.append(repr(m))
+    r = subprocess.run(args, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     nc = n * n * (n // 2 + 1)
     ref = np.fromfile(tmp_path / "ref_state.bin").view(np.complex128).reshape(4, nc)

@@ -128,3 +128,54 @@ def test_workload_inputs_are_deterministic():
     assert a[3] == b[3]
     u = np.fft.irfftn(a[0][0], s=(16, 16, 16), axes=(0, 1, 2))
     assert 1e-4 < np.abs(u).max() < 1e-1
+
+
+def test_oracle_stretched_grid_matches_golden():
+    """axis_CoSiSt (the frontend's sine-stretched grid): positions, the sampled
+    dust, the chain-rule derivatives, the cascadic multigrid solve, the shipped
+    right-hand side and three RK4 steps of the reference, bit for bit."""
+    g = _gold("stretch16.npz")
+    m, n = float(g["m"]), int(g["n"])
+    assert m == pytest.approx(I.frontend_stretch(L), rel=1e-15)
+    cfg = bind.config(n, L, float(g["M"]), tau=float(g["tau"]), theta=float(g["theta"]),
+                      terms=bind.KFO_SHIPPED, poisson_mode=bind.PS_CASCADIC, stretch_m=m)
+    o = bind.Oracle(cfg)
+    assert np.array_equal(o.positions(), g["positions"])
+    assert np.array_equal(np.array([I.val_at(i, n, L, m) for i in range(-1, n + 1)]), g["positions"])
+    assert np.allclose(I.gauss_charge(n, L, -5.0, 0.7, m), g["gauss"], rtol=1e-14, atol=0)
+    for d, k in enumerate(("dx", "dy", "dz")):
+        assert np.array_equal(o.deriv(d, g["F"]), g[k]), k
+    st = [g["s0_ux"], g["s0_uy"], g["s0_uz"], g["s0_s"]]
+    o.set_state(st)
+    o.set_sources(g["nd"], g["mask"])
+    o.rhs()
+    for a, k in zip(o.get_state(), ("rhs_ux", "rhs_uy", "rhs_uz", "rhs_s")):
+        assert np.array_equal(a, g[k]), k
+    assert np.array_equal(o.get_phi(), g["rhs_phi"])
+    o2 = bind.Oracle(cfg)
+    o2.set_state(st)
+    o2.set_sources(g["nd"], g["mask"])
+    o2.rk4(float(g["dt"]), int(g["nsteps"]))
+    for a, k in zip(o2.get_state(), ("rk_ux", "rk_uy", "rk_uz", "rk_s")):
+        assert np.array_equal(a, g[k]), k
+    o3 = bind.Oracle(bind.config(32, L, 0.8, poisson_mode=bind.PS_CASCADIC, stretch_m=m))
+    assert np.array_equal(o3.poisson(np.zeros((32, 32, 32)), g["rho32"]), g["phi_cascadic32"])
+
+
+def test_oracle_stretched_fas_reaches_jacobi_solution():
+    """The FAS cycle on stretched spacings converges to the discrete solution
+    the point-Jacobi solver reaches (same stencil, same tolerance)."""
+    n = 32
+    m = I.frontend_stretch(L)
+    st = I.initial_state(n, seed=5)
+    nd = I.gauss_charge(n, L, -10.0, 0.5, m)
+    rho = np.exp(np.fft.irfftn(st[3], s=(n, n, n), axes=(0, 1, 2))) + nd
+    oj = bind.Oracle(bind.config(n, L, 0.8, poisson_mode=bind.PS_JACOBI_RES, nlj_max_it=200000, res_tol=1e-11,
+                                 stretch_m=m))
+    of = bind.Oracle(bind.config(n, L, 0.8, poisson_mode=bind.PS_FAS, mg_levels=2, res_tol=1e-11, stretch_m=m))
+    pj = oj.poisson(np.zeros((n, n, n)), rho)
+    pf = of.poisson(np.zeros((n, n, n)), rho)
+    # the Jacobi stop tests the iterate before its last sweep
+    assert oj.residual(pj, rho) <= 2e-11 and of.residual(pf, rho) <= 1e-11
+    assert np.abs(pj - pf).max() < 1e-9
+    assert of.stats().not_converged == 0
