@@ -209,7 +209,7 @@ int kf_save(kf_ctx *ctx, const char *path, int kind, double t);
 int kf_load(kf_ctx *ctx, const char *path, double *t_out);
 
 /* The frontend's initial state (frontend.cpp:255-330, create_input_from_
- * MGsolver and the filtering after it) on the context's equidistant grid:
+ * MGsolver and the filtering after it) on the context's grid:
  * phi solves lap phi = e^phi - (n_background + n_d) from phi = 0 with the
  * context's Poisson solver and its n_d (kf_set_sources), n = exp(-theta phi),
  * both filtered by exp(-2000 k~^15) in k-space, u' = 0; the state takes
