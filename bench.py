@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=8)
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison arm")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="keep the default kernel variants (no kf_autotune; profiling runs)")
     ap.add_argument("--cpu-ref", default="", help=argparse.SUPPRESS)
     ap.add_argument("--marks", default="100,500,2000", help="steps at which --workload precision compares")
     ap.add_argument("--adjoint-steps", type=int, default=200,
@@ -284,7 +286,9 @@ def run_kf(args):
         ctx.set_stream(stream.cuda_stream)
         ctx.set_state(*st)
         ctx.set_sources(nd, mask)
-        tune = ctx.autotune()  # radix plan and smoother shape, timed on this context
+        # radix plan and smoother shape, timed on this context
+        tune = ctx.autotune() if not args.no_tune else {"fft_plan": 0, "rbgs_rows": 8,
+                                                         "fft_radices": [[], []]}
         ctx.rk4(dt, args.warmup)
         ctx.synchronize()
         barrier()

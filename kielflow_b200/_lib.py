@@ -47,16 +47,17 @@ class Config(ctypes.Structure):
         ("res_tol", ctypes.c_double), ("mg_levels", ctypes.c_int), ("mg_pre", ctypes.c_int),
         ("mg_post", ctypes.c_int), ("coarse_tol", ctypes.c_double), ("max_cycles", ctypes.c_int),
         ("phi_extrap", ctypes.c_int), ("precision", ctypes.c_int), ("stretch_m", ctypes.c_double),
+        ("mg_omega", ctypes.c_double),
     ]
 
     @classmethod
     def make(cls, n, L, M, tau=0.1, theta=30.0, diff_D=0.0, sv_eps=0.5, sv_cut=0.0, pen_eta=0.0,
              terms=KF_T_SHIPPED, poisson_mode=KF_PS_JACOBI_REF, nlj_max_it=80, nlj_limit=0.5e-5,
              res_tol=1e-10, mg_levels=4, mg_pre=2, mg_post=2, coarse_tol=1e-13, max_cycles=50,
-             phi_extrap=0, precision=KF_FP64, stretch_m=0.0):
+             phi_extrap=0, precision=KF_FP64, stretch_m=0.0, mg_omega=0.0):
         return cls(n, L, M, tau, theta, diff_D, sv_eps, sv_cut, pen_eta, terms, poisson_mode, nlj_max_it,
                    nlj_limit, res_tol, mg_levels, mg_pre, mg_post, coarse_tol, max_cycles, phi_extrap, precision,
-                   stretch_m)
+                   stretch_m, mg_omega)
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -277,11 +277,12 @@ __global__ void __launch_bounds__(BS) k_dot_w(const double *__restrict__ w, cons
 // ---------------------------------------------------------------- linear (adjoint) Poisson
 // Solve (-L_h + c) psi = b, c = exp(phi) > 0, with the FAS framework of the
 // forward solver: the point equation A - D psi - c psi = 0 (A = 2 sum w psi_nb + b)
-// is linear, so the "Newton step" is the exact point solve psi = A / (D + c).
+// is linear, so the "Newton step" is the exact point solve psi = A / (D + c),
+// over-relaxed by om as the forward smoother (om = 1: the point solve itself).
 
 template <int BY = 8>
 __global__ void __launch_bounds__(32 * BY) k_rbgs_lin(double *__restrict__ phi, const double *__restrict__ rho,
-                                                      const double *__restrict__ cl, Lev L, int color) {
+                                                      const double *__restrict__ cl, Lev L, int color, double om) {
     const int n = L.n;
     const int k2 = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * BY + threadIdx.y, i = blockIdx.z;
     if (2 * k2 >= n || j >= n) return;
@@ -289,7 +290,8 @@ __global__ void __launch_bounds__(32 * BY) k_rbgs_lin(double *__restrict__ phi, 
     double A, D;
     point_coeffs_fast(phi, rho, L, i, j, k, A, D);
     const long q = lidx(i, j, k, n);
-    phi[q] = A / __dadd_rn(D, cl[q]);
+    const double y = A / __dadd_rn(D, cl[q]);
+    phi[q] = om == 1. ? y : __dadd_rn(phi[q], __dmul_rn(om, __dsub_rn(y, phi[q])));
 }
 
 __global__ void __launch_bounds__(256) k_residual_lin(const double *__restrict__ phi, const double *__restrict__ rho,

@@ -375,6 +375,9 @@ int jacobi_solve(kf_ctx *c, const LevelBuf &L, double *phi, double *tmp, const d
     return converged ? 0 : 1;
 }
 
+// over-relaxation factor of the FAS smoother's Newton step (0 selects 1)
+double mg_omega(const kf_config &cf) { return cf.mg_omega > 0. ? cf.mg_omega : 1.; }
+
 // `sweeps` red-black Gauss-Seidel sweeps on level L (phi in place), two
 // half-sweep launches each.  cc: the adjoint's e^phi (linear point solve) or
 // nullptr (Newton step).
@@ -382,24 +385,25 @@ void smooth(kf_ctx *c, LevelBuf &L, double *phi, const double *rho, const double
     const int n = L.n;
     const long N = (long)n * n * n;
     const int by = c->rbgs_by;
+    const double om = mg_omega(c->cfg);
     const dim3 g((n / 2 + 31) / 32, (n + by - 1) / by, n), b(32, by);
     for (int s = 0; s < sweeps; ++s)
         for (int color = 0; color < 2; ++color) {
             Launch L_(c, cls, 16. * N);
             if (cc) {
                 if (by == 4)
-                    k_rbgs_lin<4><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color);
+                    k_rbgs_lin<4><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color, om);
                 else if (by == 16)
-                    k_rbgs_lin<16><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color);
+                    k_rbgs_lin<16><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color, om);
                 else
-                    k_rbgs_lin<8><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color);
+                    k_rbgs_lin<8><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color, om);
             } else {
                 if (by == 4)
-                    k_rbgs<4><<<g, b, 0, c->st>>>(phi, rho, L.lev(), color);
+                    k_rbgs<4><<<g, b, 0, c->st>>>(phi, rho, L.lev(), color, om);
                 else if (by == 16)
-                    k_rbgs<16><<<g, b, 0, c->st>>>(phi, rho, L.lev(), color);
+                    k_rbgs<16><<<g, b, 0, c->st>>>(phi, rho, L.lev(), color, om);
                 else
-                    k_rbgs<8><<<g, b, 0, c->st>>>(phi, rho, L.lev(), color);
+                    k_rbgs<8><<<g, b, 0, c->st>>>(phi, rho, L.lev(), color, om);
             }
         }
 }
@@ -413,7 +417,7 @@ void vcycle(kf_ctx *c, int l) {
         Launch L_(c, KC_COARSE, 16. * N);
         const int bs = N >= 1024 ? 1024 : (int)((N + 31) / 32 * 32);
         k_coarse_solve<<<1, bs, (size_t)(16 * N + 24 * n), c->st>>>(L.phi, L.rho, L.lev(), cf.coarse_tol, 1000,
-                                                                   c->d_sweeps);
+                                                                   c->d_sweeps, mg_omega(cf));
         return;
     }
     smooth(c, L, L.phi, L.rho, nullptr, cf.mg_pre, l == 0 ? KC_RBGS : KC_MG_COARSE);

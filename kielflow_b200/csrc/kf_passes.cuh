@@ -228,37 +228,45 @@ k_z_c2r(const ZJob *__restrict__ jobs, int njobs, int nrows, Geo<T> g,
     const int r0 = tile * LZ;
     const T2 *inA = static_cast<const T2 *>(J.inA);
     const T2 *inB = static_cast<const T2 *>(J.inB);
+    // raw half spectra -> shared memory with asynchronous copies (all of a
+    // thread's loads in flight at once); the multipliers are applied below
     for (int idx = threadIdx.x; idx < 2 * LZ * NZC; idx += blockDim.x) {
         const int which = idx / (LZ * NZC);
         const int rem = idx - which * LZ * NZC;
         const int l = rem / NZC, k = rem - l * NZC;
         const int r = r0 + l;
         const T2 *src = which ? inB : inA;
-        const int mul = which ? J.mulB : J.mulA;
-        T2 x = mk<T2>((T)0, (T)0);
-        if (src && r < nrows) {
-            x = src[(long)r * NZC + k];
-            if (mul == MUL_IK) x = mul_ik(x, g.kv[k]);
-            if (mul == MUL_HALF && k > 0 && 2 * k < N) x = mk<T2>((T)0.5 * x.x, (T)0.5 * x.y);
-        }
-        if (k == 0 || 2 * k == N) x.y = (T)0;
-        half[idx] = x;
+        if (src && r < nrows)
+            cp_async_copy(half + idx, src + (long)r * NZC + k);
+        else
+            half[idx] = mk<T2>((T)0, (T)0);
     }
+    cp_async_commit();
+    cp_async_wait_all();
     __syncthreads();
     const int p = threadIdx.x % P, l = threadIdx.x / P;
     const T2 *hA = half + l * NZC;
     const T2 *hB = half + LZ * NZC + l * NZC;
+    // staged element kk (0 <= kk < NZC) times its job's multiplier, with the
+    // imaginary parts of the kz = 0 and kz = n/2 bins dropped
+    auto staged = [&](const T2 *h, int kk, int mul) {
+        T2 x = h[kk];
+        if (mul == MUL_IK) x = mul_ik(x, g.kv[kk]);
+        if (mul == MUL_HALF && kk > 0 && 2 * kk < N) x = mk<T2>((T)0.5 * x.x, (T)0.5 * x.y);
+        if (kk == 0 || 2 * kk == N) x.y = (T)0;
+        return x;
+    };
     T2 v[E];
 #pragma unroll
     for (int q = 0; q < E; ++q) {
         const int k = reg_row<N, P, PlanV<N, V>::R1>(p, q);
         T2 a, b;
         if (k < NZC) {
-            a = hA[k];
-            b = hB[k];
+            a = staged(hA, k, J.mulA);
+            b = staged(hB, k, J.mulB);
         } else {
-            a = hA[N - k];
-            b = hB[N - k];
+            a = staged(hA, N - k, J.mulA);
+            b = staged(hB, N - k, J.mulB);
             a.y = -a.y;
             b.y = -b.y;
         }

@@ -63,10 +63,11 @@ __device__ __forceinline__ void coeffs_t(const double *__restrict__ p, const dou
     else point_coeffs(p, rho, L, i, j, k, A, D);
 }
 
-// one Newton step on A - D x - e^x = 0 (the FAS smoother's point update)
-__device__ __forceinline__ double newton_step(double x, double A, double D) {
+// one Newton step on A - D x - e^x = 0, over-relaxed by om (the FAS
+// smoother's point update; om = 1: the plain Newton step)
+__device__ __forceinline__ double newton_step(double x, double A, double D, double om) {
     const double ex = exp(x);
-    return __dsub_rn(x, __dsub_rn(__dsub_rn(A, __dmul_rn(D, x)), ex) / __dsub_rn(-D, ex));
+    return __dsub_rn(x, __dmul_rn(om, __dsub_rn(__dsub_rn(A, __dmul_rn(D, x)), ex) / __dsub_rn(-D, ex)));
 }
 
 __device__ __forceinline__ double f_point(double A, double D, double x) {
@@ -229,7 +230,7 @@ __global__ void k_extrap(double *__restrict__ phi, double *__restrict__ phi_a, d
 // kf_autotune chooses; the arithmetic does not depend on it).
 template <int BY = 8>
 __global__ void __launch_bounds__(32 * BY) k_rbgs(double *__restrict__ phi, const double *__restrict__ rho, Lev L,
-                                                  int color) {
+                                                  int color, double om) {
     const int n = L.n;
     const int k2 = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * BY + threadIdx.y, i = blockIdx.z;
     if (2 * k2 >= n || j >= n) return;
@@ -237,7 +238,7 @@ __global__ void __launch_bounds__(32 * BY) k_rbgs(double *__restrict__ phi, cons
     double A, D;
     point_coeffs_fast(phi, rho, L, i, j, k, A, D);
     const long q = lidx(i, j, k, n);
-    phi[q] = newton_step(phi[q], A, D);
+    phi[q] = newton_step(phi[q], A, D, om);
 }
 
 // Coarsest-level solve in one block: the level (phi, rho and the axis
@@ -247,7 +248,7 @@ __global__ void __launch_bounds__(32 * BY) k_rbgs(double *__restrict__ phi, cons
 // memory: 16 n^3 + 24 n bytes.
 __global__ void __launch_bounds__(1024) k_coarse_solve(double *__restrict__ phi, const double *__restrict__ rho,
                                                        Lev L, double tol, int max_sweeps,
-                                                       int *__restrict__ sweeps_out) {
+                                                       int *__restrict__ sweeps_out, double om) {
     extern __shared__ __align__(16) double cs_sm[];
     __shared__ double sh[32];
     const int n = L.n;
@@ -299,7 +300,7 @@ __global__ void __launch_bounds__(1024) k_coarse_solve(double *__restrict__ phi,
                 double A, D;
                 point_coeffs_fast(sp, sr, Ls, i, j, k, A, D);
                 const int q = (int)lidx(i, j, k, n);
-                sp[q] = newton_step(sp[q], A, D);
+                sp[q] = newton_step(sp[q], A, D, om);
             }
             __syncthreads();
         }

@@ -19,7 +19,8 @@
  *  - KFO_PS_JACOBI_RES: the Jacobi sweeps of solver_poisson_jacobi_nlin with a
  *    max-norm residual stop;
  *  - KFO_PS_FAS: an FAS V-cycle (red-black point-Newton smoother built from
- *    iteration_loop's point update, injection for phi, full weighting for the
+ *    iteration_loop's point update, optionally over-relaxed by mg_omega,
+ *    injection for phi, full weighting for the
  *    residual, the trilinear OP_hto2h for the correction).
  */
 #include "kf_oracle.h"
@@ -424,7 +425,7 @@ double max_resid_fast(const level &L, const vec &phi, const vec &rho) {
 /* Red-black Gauss-Seidel-Newton sweep: at each point one Newton step on the
  * point equation A - D x - e^x = 0 of iteration_loop (:177-199), in place,
  * colour (i+j+k)%2 == 0 first. */
-void rbgs_sweep(const level &L, vec &phi, const vec &rho) {
+void rbgs_sweep(const level &L, vec &phi, const vec &rho, double om) {
     for (int color = 0; color < 2; ++color)
         for (int i = 0; i < L.n; ++i)
             for (int j = 0; j < L.n; ++j)
@@ -433,7 +434,7 @@ void rbgs_sweep(const level &L, vec &phi, const vec &rho) {
                     L.coeffs_fast(phi.data(), rho.data(), i, j, k, A, D);
                     const size_t q = L.idx(i, j, k);
                     const double x = phi[q], ex = exp(x);
-                    phi[q] = x - (A - D * x - ex) / (-D - ex);
+                    phi[q] = x - om * ((A - D * x - ex) / (-D - ex));
                 }
 }
 
@@ -451,6 +452,7 @@ void apply_N(const level &L, const vec &phi, vec &out) {
 void fas_vcycle(kfo_ctx *c, int l, vec &phi, const vec &rho) {
     const level &L = c->lv[l];
     const kfo_config &cf = c->cfg;
+    const double om = cf.mg_omega > 0. ? cf.mg_omega : 1.; /* over-relaxed point Newton step */
     if (l == (int)c->lv.size() - 1) {
         /* coarsest level: relaxed until its max residual is at most
            max(coarse_tol, 1e-4 x its value at entry), at most 1000 sweeps */
@@ -459,11 +461,11 @@ void fas_vcycle(kfo_ctx *c, int l, vec &phi, const vec &rho) {
             const double r = max_resid_fast(L, phi, rho);
             if (s == 0) r0 = r;
             if (r <= std::max(cf.coarse_tol, 1e-4 * r0)) break;
-            rbgs_sweep(L, phi, rho);
+            rbgs_sweep(L, phi, rho, om);
         }
         return;
     }
-    for (int s = 0; s < cf.mg_pre; ++s) rbgs_sweep(L, phi, rho);
+    for (int s = 0; s < cf.mg_pre; ++s) rbgs_sweep(L, phi, rho, om);
     vec r(phi.size());
     for (int i = 0; i < L.n; ++i)
         for (int j = 0; j < L.n; ++j)
@@ -481,7 +483,7 @@ void fas_vcycle(kfo_ctx *c, int l, vec &phi, const vec &rho) {
     vec e;
     prolong(Lc.n, cf.L, cf.stretch_m, phic, e);
     for (size_t q = 0; q < phi.size(); ++q) phi[q] += e[q];
-    for (int s = 0; s < cf.mg_post; ++s) rbgs_sweep(L, phi, rho);
+    for (int s = 0; s < cf.mg_post; ++s) rbgs_sweep(L, phi, rho, om);
 }
 
 /* solver_poisson_multigrid::solve with the plan of kielflow.cpp:207-217

@@ -58,6 +58,7 @@ typedef struct {
     int phi_extrap;      /* linear extrapolation of phi in time for the start    */
     double stretch_m;    /* 0: axis_CoEqSt; > 0: axis_CoSiSt(-L/2, L, n, m) on   */
                          /* all three axes (sine-stretched, axis_SiSt.cpp)       */
+    double mg_omega;     /* FAS: over-relaxation of the point Newton step (0: 1) */
 } kfo_config;
 
 typedef struct kfo_ctx kfo_ctx;
