@@ -116,6 +116,9 @@ struct kf_ctx {
     // the FAS V-cycle captured once as a CUDA graph (replayed every cycle)
     cudaGraphExec_t vgraph = nullptr;
     long long vgraph_kernels = 0;
+    // the part of a V-cycle after the finest level's residual (adaptive solves)
+    cudaGraphExec_t vgraph_tail = nullptr;
+    long long vgraph_tail_kernels = 0;
     // per-(precision, n) entry points
     void (*rhs_fn)(kf_ctx *) = nullptr;
     void (*r2c_fn)(kf_ctx *) = nullptr;
@@ -146,7 +149,7 @@ struct kf_ctx {
     cudaEvent_t ev_u = nullptr;
     double *stage64b = nullptr;  // FP32-bulk staging of the copy stream
     double step_dt = 0.;
-    long long step_kernels = 0, cycle_kernels = 0;
+    long long step_kernels = 0, cycle_kernels = 0, head_kernels = 0;
     int jV_x = 0, jV_y = 0, zV = 0, zW = 0, nWz = 0, nWf = 0, jW_y = 0, jW_x = 0, zS = 0, jS_y = 0, jS_x = 0;
     int jP_x = 0, jP_y = 0, zP = 0, jQ_x = 0, jQ_y = 0, zQ = 0;
 };
@@ -408,23 +411,31 @@ void smooth(kf_ctx *c, LevelBuf &L, double *phi, const double *rho, const double
         }
 }
 
-void vcycle(kf_ctx *c, int l) {
+void vcycle(kf_ctx *c, int l);
+
+// First part of a V-cycle on level l (not the coarsest): pre-smoothing and the
+// residual L.r; with_max also leaves max |L.r| in the d_max slots.
+void vcycle_head(kf_ctx *c, int l, bool with_max) {
     LevelBuf &L = c->lv[l];
     const kf_config &cf = c->cfg;
     const int n = L.n;
     const long N = (long)n * n * n;
-    if (l == (int)c->lv.size() - 1) {
-        Launch L_(c, KC_COARSE, 16. * N);
-        const int bs = N >= 1024 ? 1024 : (int)((N + 31) / 32 * 32);
-        k_coarse_solve<<<1, bs, (size_t)(16 * N + 24 * n), c->st>>>(L.phi, L.rho, L.lev(), cf.coarse_tol, 1000,
-                                                                   c->d_sweeps, mg_omega(cf));
-        return;
-    }
     smooth(c, L, L.phi, L.rho, nullptr, cf.mg_pre, l == 0 ? KC_RBGS : KC_MG_COARSE);
-    {
-        Launch L_(c, l == 0 ? KC_RESID : KC_MG_COARSE, 24. * N);
+    if (with_max) CK(cudaMemsetAsync(c->d_max, 0, 64 * sizeof(unsigned long long), c->st));
+    Launch L_(c, l == 0 ? KC_RESID : KC_MG_COARSE, 24. * N);
+    if (with_max)
+        k_residual<true, true><<<mg_grid(n, n), mg_block(), 0, c->st>>>(L.phi, L.rho, L.lev(), L.r, c->d_max);
+    else
         k_residual<true><<<mg_grid(n, n), mg_block(), 0, c->st>>>(L.phi, L.rho, L.lev(), L.r);
-    }
+}
+
+// The rest of the V-cycle on level l: restriction, the coarse cycle, the
+// correction and post-smoothing.
+void vcycle_tail(kf_ctx *c, int l) {
+    LevelBuf &L = c->lv[l];
+    const kf_config &cf = c->cfg;
+    const int n = L.n;
+    const long N = (long)n * n * n;
     LevelBuf &Lc = c->lv[l + 1];
     const long Nc3 = (long)Lc.n * Lc.n * Lc.n;
     {
@@ -446,6 +457,22 @@ void vcycle(kf_ctx *c, int l) {
     }
     smooth(c, L, L.phi, L.rho, nullptr, cf.mg_post, l == 0 ? KC_RBGS : KC_MG_COARSE);
     CK(cudaGetLastError());
+}
+
+void vcycle(kf_ctx *c, int l) {
+    LevelBuf &L = c->lv[l];
+    const kf_config &cf = c->cfg;
+    const int n = L.n;
+    const long N = (long)n * n * n;
+    if (l == (int)c->lv.size() - 1) {
+        Launch L_(c, KC_COARSE, 16. * N);
+        const int bs = N >= 1024 ? 1024 : (int)((N + 31) / 32 * 32);
+        k_coarse_solve<<<1, bs, (size_t)(16 * N + 24 * n), c->st>>>(L.phi, L.rho, L.lev(), cf.coarse_tol, 1000,
+                                                                   c->d_sweeps, mg_omega(cf));
+        return;
+    }
+    vcycle_head(c, l, false);
+    vcycle_tail(c, l);
 }
 
 // One FAS V-cycle on the finest level: replayed from a CUDA graph captured on
@@ -470,6 +497,39 @@ void run_vcycle(kf_ctx *c) {
     }
     CK(cudaGraphLaunch(c->vgraph, c->st));
     c->launches += c->vgraph_kernels;
+}
+
+// vcycle_tail(c, 0), replayed from its own graph as run_vcycle does
+void run_vcycle_tail(kf_ctx *c) {
+    if (c->prof) {
+        vcycle_tail(c, 0);
+        return;
+    }
+    if (!c->vgraph_tail) {
+        const long long l0 = c->launches;
+        CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+        vcycle_tail(c, 0);
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamEndCapture(c->st, &g));
+        cudaError_t e = cudaGraphInstantiate(&c->vgraph_tail, g, 0);
+        cudaGraphDestroy(g);
+        CK(e);
+        c->vgraph_tail_kernels = c->launches - l0;
+        c->launches = l0;
+    }
+    CK(cudaGraphLaunch(c->vgraph_tail, c->st));
+    c->launches += c->vgraph_tail_kernels;
+}
+
+// max over the 64 d_max slots (IEEE bit patterns of non-negative doubles)
+double read_max_slots(kf_ctx *c) {
+    CK(cudaMemcpyAsync(c->h_max, c->d_max, 64 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    unsigned long long m = 0;
+    for (int s = 0; s < 64; ++s) m = c->h_max[s] > m ? c->h_max[s] : m;
+    double r;
+    std::memcpy(&r, &m, sizeof(double));
+    return r;
 }
 
 // Poisson solve on c->phi with source c->rho.  Returns KF_OK or KF_ERR_NOT_CONVERGED.
@@ -527,6 +587,28 @@ int poisson(kf_ctx *c) {
         c->diag.stage_cycles[c->stage_idx & 3] += cf.max_cycles;
         c->diag.last_residual = r;
         if (r != r) throw KfError{KF_ERR_NAN, "NaN in the multigrid solve"};
+    } else if (c->lv.size() > 1) {
+        // test after each cycle's pre-smoothing on the residual the cycle
+        // computes anyway; the rest of the cycle only when it fails
+        double r = 0.;
+        int cyc = 0;
+        for (;;) {
+            vcycle_head(c, 0, true);
+            CK(cudaGetLastError());
+            r = read_max_slots(c);
+            if (!(r > cf.res_tol) || cyc >= cf.max_cycles) break;
+            run_vcycle_tail(c);
+            ++cyc;
+        }
+        c->diag.last_iterations = cyc;
+        c->diag.stage_cycles[c->stage_idx & 3] += cyc;
+        c->diag.total_iterations += cyc;
+        c->diag.last_residual = r;
+        if (r != r) throw KfError{KF_ERR_NAN, "NaN in the multigrid solve"};
+        if (r > cf.res_tol) {
+            c->diag.not_converged++;
+            rc = 1;
+        }
     } else {
         double r = max_residual(c, L0, c->phi, c->rho, true);
         int cyc = 0;
@@ -582,6 +664,76 @@ void poisson_captured(kf_ctx *c) {
     }
     LevelBuf &L0 = c->lv[0];
     const bool fixed = !(cf.res_tol > 0.);
+    c->head_kernels = 0;
+    if (!fixed && c->lv.size() > 1) {
+        // WHILE { head of the cycle (pre-smoothing, residual with its max);
+        //         k_fas_check_mid;  IF { rest of the cycle } }
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamGetCaptureInfo(c->st, &cs, nullptr, &g, nullptr, nullptr));
+        cudaGraphConditionalHandle hw, hi;
+        CK(cudaGraphConditionalHandleCreate(&hw, g, 0, 0));
+        CK(cudaGraphConditionalHandleCreate(&hi, g, 0, 0));
+        {
+            Launch L_(c, KC_MISC, 0.);
+            k_fas_begin<<<1, 32, 0, c->st>>>(c->dpois, hw);
+        }
+        const cudaGraphNode_t *deps = nullptr;
+        size_t ndeps = 0;
+        CK(cudaStreamGetCaptureInfo(c->st, &cs, nullptr, &g, &deps, &ndeps));
+        cudaGraphNodeParams wp = {cudaGraphNodeTypeConditional};
+        wp.conditional.handle = hw;
+        wp.conditional.type = cudaGraphCondTypeWhile;
+        wp.conditional.size = 1;
+        cudaGraphNode_t wnode;
+        CK(cudaGraphAddNode(&wnode, g, deps, ndeps, &wp));
+        CK(cudaStreamUpdateCaptureDependencies(c->st, &wnode, 1, cudaStreamSetCaptureDependencies));
+        cudaGraph_t body = wp.conditional.phGraph_out[0];
+        const long long l0 = c->launches;
+        cudaStream_t outer = c->st;
+        c->st = c->st_body;
+        cudaError_t e = cudaStreamBeginCaptureToGraph(c->st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            try {
+                vcycle_head(c, 0, true);
+                {
+                    Launch L_(c, KC_MISC, 0.);
+                    k_fas_check_mid<<<1, 32, 0, c->st>>>(c->d_max, c->dpois, cf.res_tol, cf.max_cycles, c->stage_idx,
+                                                         hw, hi);
+                }
+                c->head_kernels = c->launches - l0;
+                cudaGraph_t gb = nullptr;
+                CK(cudaStreamGetCaptureInfo(c->st, &cs, nullptr, &gb, &deps, &ndeps));
+                cudaGraphNodeParams ip = {cudaGraphNodeTypeConditional};
+                ip.conditional.handle = hi;
+                ip.conditional.type = cudaGraphCondTypeIf;
+                ip.conditional.size = 1;
+                cudaGraphNode_t inode;
+                CK(cudaGraphAddNode(&inode, gb, deps, ndeps, &ip));
+                CK(cudaStreamUpdateCaptureDependencies(c->st, &inode, 1, cudaStreamSetCaptureDependencies));
+                cudaGraph_t body_out = nullptr;
+                CK(cudaStreamEndCapture(c->st, &body_out));
+                CK(cudaStreamBeginCaptureToGraph(c->st, ip.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                 cudaStreamCaptureModeThreadLocal));
+                vcycle_tail(c, 0);
+                e = cudaStreamEndCapture(c->st, &body_out);
+            } catch (...) {
+                cudaGraph_t junk = nullptr;
+                cudaStreamEndCapture(c->st, &junk);
+                c->st = outer;
+                throw;
+            }
+        }
+        c->st = outer;
+        CK(e);
+        c->cycle_kernels = c->launches - l0;
+        if (extrap) {
+            Launch L_(c, KC_MISC, 0.);
+            k_hist_post<<<1, 32, 0, c->st>>>(c->dtime);
+        }
+        CK(cudaGetLastError());
+        return;
+    }
     auto resmax = [&](cudaStream_t st) {
         CK(cudaMemsetAsync(c->d_max, 0, 64 * sizeof(unsigned long long), st));
         Launch L_(c, KC_RESID, 16. * c->N);
@@ -1649,7 +1801,7 @@ void graph_end(kf_ctx *c) {
     c->tau_b = ht.tau_b;
     c->nhist = ht.nhist;
     const DevPois &o = c->hpois;
-    c->launches += (hp.total_cycles - o.total_cycles) * c->cycle_kernels;
+    c->launches += (hp.total_cycles - o.total_cycles) * c->cycle_kernels + (hp.solves - o.solves) * c->head_kernels;
     c->diag.solves += hp.solves - o.solves;
     c->diag.total_iterations += hp.total_cycles - o.total_cycles;
     if (hp.solves != o.solves) {
@@ -1733,6 +1885,8 @@ void drop_graphs(kf_ctx *c) {
     CK(cudaStreamSynchronize(c->st));
     if (c->vgraph) cudaGraphExecDestroy(c->vgraph);
     c->vgraph = nullptr;
+    if (c->vgraph_tail) cudaGraphExecDestroy(c->vgraph_tail);
+    c->vgraph_tail = nullptr;
     if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
     c->step_graph = nullptr;
     if (c->step_graph_wait) cudaGraphExecDestroy(c->step_graph_wait);
@@ -1862,6 +2016,7 @@ int kf_ctx_destroy(kf_ctx *c) {
     }
     for (auto e : c->evfree) cudaEventDestroy(e);
     if (c->vgraph) cudaGraphExecDestroy(c->vgraph);
+    if (c->vgraph_tail) cudaGraphExecDestroy(c->vgraph_tail);
     if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
     if (c->step_graph_wait) cudaGraphExecDestroy(c->step_graph_wait);
     if (c->ev_u) cudaEventDestroy(c->ev_u);

@@ -100,4 +100,41 @@ __global__ void k_fas_check(const unsigned long long *__restrict__ slots, DevPoi
     cudaGraphSetConditional(h, cont ? 1u : 0u);
 }
 
+// Adaptive FAS solve, one WHILE iteration = pre-smoothing and residual of the
+// finest level, this test, then (IF node) the rest of the V-cycle.  The test
+// uses the residual of the pre-smoothed iterate: the solve ends there when its
+// max |f| <= tol (or max_cycles cycles are done), so the returned phi carries
+// the measured residual and no cycle ends with a residual pass of its own.
+__global__ void k_fas_begin(DevPois *p, cudaGraphConditionalHandle hw) {
+    if (threadIdx.x || blockIdx.x) return;
+    p->cyc = 0;
+    cudaGraphSetConditional(hw, 1u);
+}
+
+__global__ void k_fas_check_mid(const unsigned long long *__restrict__ slots, DevPois *p, double tol, int max_cycles,
+                                int stage, cudaGraphConditionalHandle hw, cudaGraphConditionalHandle hi) {
+    if (threadIdx.x || blockIdx.x) return;
+    unsigned long long m = 0;
+    for (int s = 0; s < 64; ++s) m = slots[s] > m ? slots[s] : m;
+    const double r = __longlong_as_double((long long)m);
+    const int cyc = p->cyc;
+    p->r = r;
+    const bool cont = r > tol && cyc < max_cycles;
+    if (cont) {
+        p->cyc = cyc + 1;
+    } else {
+        p->solves += 1;
+        p->total_cycles += cyc;
+        p->last_cycles = cyc;
+        p->last_residual = r;
+        p->stage_cycles[stage & 3] += cyc;
+        if (r != r)
+            p->nans += 1;
+        else if (r > tol)
+            p->not_converged += 1;
+    }
+    cudaGraphSetConditional(hw, cont ? 1u : 0u);
+    cudaGraphSetConditional(hi, cont ? 1u : 0u);
+}
+
 }  // namespace kf

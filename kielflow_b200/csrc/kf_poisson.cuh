@@ -174,17 +174,36 @@ __global__ void __launch_bounds__(BS) k_reduce_final(const double *__restrict__ 
 inline dim3 mg_grid(int nx, int n) { return dim3((nx + 31) / 32, (n + 7) / 8, n); }
 inline dim3 mg_block() { return dim3(32, 8, 1); }
 
-// Pointwise residual r = f(phi) = lap_h phi + rho - e^phi on the whole level.
-template <bool FAST>
+// Pointwise residual r = f(phi) = lap_h phi + rho - e^phi on the whole level;
+// with MAX also max |r| (block maximum, then an atomic max on the IEEE bit
+// pattern into one of 64 slots, as k_resmax), so that the convergence test of
+// a cycle needs no pass of its own.
+template <bool FAST, bool MAX = false>
 __global__ void __launch_bounds__(256) k_residual(const double *__restrict__ phi, const double *__restrict__ rho,
-                                                  Lev L, double *__restrict__ r) {
+                                                  Lev L, double *__restrict__ r,
+                                                  unsigned long long *__restrict__ slots = nullptr) {
     const int n = L.n;
     const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, i = blockIdx.z;
-    if (k >= n || j >= n) return;
-    double A, D;
-    coeffs_t<FAST>(phi, rho, L, i, j, k, A, D);
-    const long id = lidx(i, j, k, n);
-    r[id] = f_point(A, D, phi[id]);
+    double af = 0.;
+    if (k < n && j < n) {
+        double A, D;
+        coeffs_t<FAST>(phi, rho, L, i, j, k, A, D);
+        const long id = lidx(i, j, k, n);
+        const double f = f_point(A, D, phi[id]);
+        r[id] = f;
+        af = fabs(f);
+    }
+    if (!MAX) return;
+    __shared__ double sh[8];
+    for (int o = 16; o > 0; o >>= 1) af = nmax(af, __shfl_xor_sync(0xffffffffu, af, o));
+    if (threadIdx.x == 0) sh[threadIdx.y] = af;
+    __syncthreads();
+    if (threadIdx.y == 0 && threadIdx.x == 0) {
+        double m = sh[0];
+        for (int w = 1; w < 8; ++w) m = nmax(m, sh[w]);
+        atomicMax(slots + ((blockIdx.x + blockIdx.y * gridDim.x + blockIdx.z) & 63),
+                  (unsigned long long)__double_as_longlong(m));
+    }
 }
 
 // max |f(phi)| over the level: each block covers a (32 x 8) tile of (k, j) for

@@ -449,6 +449,9 @@ void apply_N(const level &L, const vec &phi, vec &out) {
             }
 }
 
+void fas_head(kfo_ctx *c, int l, vec &phi, const vec &rho, vec &r);
+void fas_tail(kfo_ctx *c, int l, vec &phi, const vec &rho, const vec &r);
+
 void fas_vcycle(kfo_ctx *c, int l, vec &phi, const vec &rho) {
     const level &L = c->lv[l];
     const kfo_config &cf = c->cfg;
@@ -465,11 +468,29 @@ void fas_vcycle(kfo_ctx *c, int l, vec &phi, const vec &rho) {
         }
         return;
     }
+    vec r;
+    fas_head(c, l, phi, rho, r);
+    fas_tail(c, l, phi, rho, r);
+}
+
+/* first part of a V-cycle on level l (not the coarsest): pre-smoothing and the
+ * residual r of the pre-smoothed iterate */
+void fas_head(kfo_ctx *c, int l, vec &phi, const vec &rho, vec &r) {
+    const level &L = c->lv[l];
+    const kfo_config &cf = c->cfg;
+    const double om = cf.mg_omega > 0. ? cf.mg_omega : 1.;
     for (int s = 0; s < cf.mg_pre; ++s) rbgs_sweep(L, phi, rho, om);
-    vec r(phi.size());
+    r.assign(phi.size(), 0.);
     for (int i = 0; i < L.n; ++i)
         for (int j = 0; j < L.n; ++j)
             for (int k = 0; k < L.n; ++k) r[L.idx(i, j, k)] = L.resid_fast(phi.data(), rho.data(), i, j, k);
+}
+
+/* the rest: restriction, the coarse cycle, the correction, post-smoothing */
+void fas_tail(kfo_ctx *c, int l, vec &phi, const vec &rho, const vec &r) {
+    const level &L = c->lv[l];
+    const kfo_config &cf = c->cfg;
+    const double om = cf.mg_omega > 0. ? cf.mg_omega : 1.;
     vec phic, rc, Nc, rhoc;
     inject(L.n, 2, phi, phic);
     restrict_fw(L.n, r, rc);
@@ -525,6 +546,32 @@ int poisson(kfo_ctx *c, vec &phi, const vec &rho) {
     } else if (cf.poisson_mode == KFO_PS_CASCADIC) {
         cascadic_solve(c, phi, rho);
         c->stats.last_residual = max_resid(c->lv[0], phi, rho);
+    } else if (cf.res_tol > 0. && c->lv.size() > 1) {
+        /* the stop test runs on the residual of each cycle's pre-smoothed
+         * iterate (the one the cycle restricts); the rest of the cycle only
+         * when it fails, so the returned phi has the tested residual */
+        int cyc = 0;
+        double r = 0.;
+        vec rv;
+        for (;;) {
+            fas_head(c, 0, phi, rho, rv);
+            r = 0.;
+            for (double v : rv) {
+                const double a = std::fabs(v);
+                if (a != a) {
+                    r = a;
+                    break;
+                }
+                r = std::max(r, a);
+            }
+            if (!(r > cf.res_tol) || cyc >= cf.max_cycles) break;
+            fas_tail(c, 0, phi, rho, rv);
+            ++cyc;
+        }
+        c->stats.last_iterations = cyc;
+        c->stats.total_iterations += cyc;
+        c->stats.last_residual = r;
+        if (r > cf.res_tol) c->stats.not_converged++;
     } else {
         double r = max_resid_fast(c->lv[0], phi, rho);
         int cyc = 0;
