@@ -423,10 +423,13 @@ void vcycle_head(kf_ctx *c, int l, bool with_max) {
     smooth(c, L, L.phi, L.rho, nullptr, cf.mg_pre, l == 0 ? KC_RBGS : KC_MG_COARSE);
     if (with_max) CK(cudaMemsetAsync(c->d_max, 0, 64 * sizeof(unsigned long long), c->st));
     Launch L_(c, l == 0 ? KC_RESID : KC_MG_COARSE, 24. * N);
-    if (with_max)
-        k_residual<true, true><<<mg_grid(n, n), mg_block(), 0, c->st>>>(L.phi, L.rho, L.lev(), L.r, c->d_max);
-    else
+    if (with_max) {
+        dim3 g = mg_grid(n, n);
+        g.z = n < 64 ? n : 64;  // each block strides over n/64 i-planes
+        k_residual<true, true><<<g, mg_block(), 0, c->st>>>(L.phi, L.rho, L.lev(), L.r, c->d_max);
+    } else {
         k_residual<true><<<mg_grid(n, n), mg_block(), 0, c->st>>>(L.phi, L.rho, L.lev(), L.r);
+    }
 }
 
 // The rest of the V-cycle on level l: restriction, the coarse cycle, the

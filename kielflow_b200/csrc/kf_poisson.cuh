@@ -175,23 +175,26 @@ inline dim3 mg_grid(int nx, int n) { return dim3((nx + 31) / 32, (n + 7) / 8, n)
 inline dim3 mg_block() { return dim3(32, 8, 1); }
 
 // Pointwise residual r = f(phi) = lap_h phi + rho - e^phi on the whole level;
-// with MAX also max |r| (block maximum, then an atomic max on the IEEE bit
-// pattern into one of 64 slots, as k_resmax), so that the convergence test of
-// a cycle needs no pass of its own.
+// with MAX also max |r|, so that the convergence test of a cycle needs no pass
+// of its own: each block then covers the i-planes blockIdx.z, blockIdx.z +
+// gridDim.z, ... (launched with gridDim.z <= 64), takes the block
+// maximum and makes one atomic max on the IEEE bit pattern into one of 64 slots.
 template <bool FAST, bool MAX = false>
 __global__ void __launch_bounds__(256) k_residual(const double *__restrict__ phi, const double *__restrict__ rho,
                                                   Lev L, double *__restrict__ r,
                                                   unsigned long long *__restrict__ slots = nullptr) {
     const int n = L.n;
-    const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, i = blockIdx.z;
+    const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y;
     double af = 0.;
     if (k < n && j < n) {
-        double A, D;
-        coeffs_t<FAST>(phi, rho, L, i, j, k, A, D);
-        const long id = lidx(i, j, k, n);
-        const double f = f_point(A, D, phi[id]);
-        r[id] = f;
-        af = fabs(f);
+        for (int i = blockIdx.z; i < n; i += (MAX ? gridDim.z : n)) {
+            double A, D;
+            coeffs_t<FAST>(phi, rho, L, i, j, k, A, D);
+            const long id = lidx(i, j, k, n);
+            const double f = f_point(A, D, phi[id]);
+            r[id] = f;
+            af = nmax(af, fabs(f));
+        }
     }
     if (!MAX) return;
     __shared__ double sh[8];
