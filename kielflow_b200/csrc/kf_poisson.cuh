@@ -196,16 +196,17 @@ __global__ void __launch_bounds__(256) k_residual(const double *__restrict__ phi
             af = nmax(af, fabs(f));
         }
     }
-    if (!MAX) return;
-    __shared__ double sh[8];
-    for (int o = 16; o > 0; o >>= 1) af = nmax(af, __shfl_xor_sync(0xffffffffu, af, o));
-    if (threadIdx.x == 0) sh[threadIdx.y] = af;
-    __syncthreads();
-    if (threadIdx.y == 0 && threadIdx.x == 0) {
-        double m = sh[0];
-        for (int w = 1; w < 8; ++w) m = nmax(m, sh[w]);
-        atomicMax(slots + ((blockIdx.x + blockIdx.y * gridDim.x + blockIdx.z) & 63),
-                  (unsigned long long)__double_as_longlong(m));
+    if constexpr (MAX) {
+        __shared__ double sh[8];
+        for (int o = 16; o > 0; o >>= 1) af = nmax(af, __shfl_xor_sync(0xffffffffu, af, o));
+        if (threadIdx.x == 0) sh[threadIdx.y] = af;
+        __syncthreads();
+        if (threadIdx.y == 0 && threadIdx.x == 0) {
+            double m = sh[0];
+            for (int w = 1; w < 8; ++w) m = nmax(m, sh[w]);
+            atomicMax(slots + ((blockIdx.x + blockIdx.y * gridDim.x + blockIdx.z) & 63),
+                      (unsigned long long)__double_as_longlong(m));
+        }
     }
 }
 
