@@ -425,7 +425,7 @@ void vcycle_head(kf_ctx *c, int l, bool with_max) {
     Launch L_(c, l == 0 ? KC_RESID : KC_MG_COARSE, 24. * N);
     if (with_max) {
         dim3 g = mg_grid(n, n);
-        g.z = n < 64 ? n : 64;  // each block strides over n/64 i-planes
+        g.z = n < 16 ? n : 16;  // each block strides over n/16 i-planes (ncu, 256^3: 158 us; 64 groups 169 us)
         k_residual<true, true><<<g, mg_block(), 0, c->st>>>(L.phi, L.rho, L.lev(), L.r, c->d_max);
     } else {
         k_residual<true><<<mg_grid(n, n), mg_block(), 0, c->st>>>(L.phi, L.rho, L.lev(), L.r);

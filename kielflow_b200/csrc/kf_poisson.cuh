@@ -177,7 +177,7 @@ inline dim3 mg_block() { return dim3(32, 8, 1); }
 // Pointwise residual r = f(phi) = lap_h phi + rho - e^phi on the whole level;
 // with MAX also max |r|, so that the convergence test of a cycle needs no pass
 // of its own: each block then covers the i-planes blockIdx.z, blockIdx.z +
-// gridDim.z, ... (launched with gridDim.z <= 64), takes the block
+// gridDim.z, ... (launched with gridDim.z <= 16), takes the block
 // maximum and makes one atomic max on the IEEE bit pattern into one of 64 slots.
 template <bool FAST, bool MAX = false>
 __global__ void __launch_bounds__(256) k_residual(const double *__restrict__ phi, const double *__restrict__ rho,
