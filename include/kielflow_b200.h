@@ -56,9 +56,13 @@ extern "C" {
 #define KF_FP64 0
 #define KF_FP32_BULK 1 /* FFTs, products, RK4 in FP32; Poisson in FP64 */
 
+/* Context configuration.  Fields are only ever appended; a caller that
+ * zero-initializes the struct (kf_config c = {}) gets the documented default
+ * (0) of every field it does not set. */
 typedef struct {
     int n;             /* cubic grid n^3: 16, 32, 64, 96, 128 or 256                 */
-    double L;          /* box side; axes axis_CoEqSt(-L/2, L, n)                      */
+    double L;          /* box side; axes axis_CoEqSt(-L/2, L, n), or axis_CoSiSt      */
+                       /* with stretch_m                                             */
     double M;          /* Mach number (parameters::M)                                */
     double tau;        /* friction (parameters::tau)                                 */
     double theta;      /* Te/Ti (parameters::theta)                                  */
