@@ -1574,6 +1574,8 @@ void create(kf_ctx *c) {
     if (!(cf.L > 0.) || !(cf.theta != 0.)) throw KfError{KF_ERR_ARG, "L > 0 and theta != 0 required"};
     if (!(cf.stretch_m >= 0.) || !(2. * acos(-1.) * cf.stretch_m < cf.L))
         throw KfError{KF_ERR_ARG, "stretch_m must satisfy 0 <= 2 pi m < L (a monotone axis_CoSiSt map)"};
+    if (!(cf.mg_omega >= 0.) || !(cf.mg_omega < 2.))
+        throw KfError{KF_ERR_ARG, "mg_omega must lie in [0, 2) (0: the plain Newton step)"};
     c->stretched = cf.stretch_m != 0.;
     c->fp32 = cf.precision == KF_FP32_BULK;
     c->es = c->fp32 ? 4 : 8;

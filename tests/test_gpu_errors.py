@@ -63,6 +63,10 @@ def test_invalid_arguments():
     with pytest.raises(kf.KfError) as e:
         kf.Context(C.config_for(w, 32, pen_eta=1e-3))  # effect_penalization needs eta <= 0
     assert e.value.code == -1
+    for om in (-0.5, 2.0):  # over-relaxation outside [0, 2)
+        with pytest.raises(kf.KfError) as e:
+            kf.Context(C.config_for(w, 32, mg_omega=om))
+        assert e.value.code == -1
     ctx32, st, dt = make(precision=kf.KF_FP32_BULK)
     with ctx32:
         with pytest.raises(kf.KfError) as e:
