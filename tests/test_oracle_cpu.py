@@ -179,3 +179,33 @@ def test_oracle_stretched_fas_reaches_jacobi_solution():
     assert oj.residual(pj, rho) <= 2e-11 and of.residual(pf, rho) <= 1e-11
     assert np.abs(pj - pf).max() < 1e-9
     assert of.stats().not_converged == 0
+
+
+def test_known_answers_single_mode_mask_and_constant_source():
+    """Analytic checks of the restatement (no reference run needed):
+    - the spectral derivative of cos(2 pi m x / L) along each axis is
+      -(2 pi m / L) sin(2 pi m x / L) (OP_partial_derivative, uniform grid);
+    - the 2/3 mask keeps exactly the modes with |k~| < 2/3 (an independent count);
+    - with a constant source rho = c every solver's fixed point is phi = ln c."""
+    n, m = 32, 3
+    o = bind.Oracle(bind.config(n, L, 0.8, poisson_mode=bind.PS_JACOBI_RES, nlj_max_it=100000, res_tol=1e-13))
+    x = I.axis_values(n, L)
+    kx = 2.0 * np.pi * m / L
+    for d in range(3):
+        shape = [1, 1, 1]
+        shape[d] = n
+        f = np.broadcast_to(np.cos(kx * x).reshape(shape), (n, n, n)).copy()
+        df = bind.c2r(o.deriv(d, bind.r2c(f)))
+        want = np.broadcast_to((-kx * np.sin(kx * x)).reshape(shape), (n, n, n))
+        assert np.abs(df - want).max() < 1e-12 * kx
+    P = o.tables()[0]
+    k = I.k_values(n, L) / I.k_values(n, L)[n // 2]
+    kk = np.sqrt(k[:, None, None] ** 2 + k[None, :, None] ** 2 + k[None, None, : n // 2 + 1] ** 2)
+    assert int(P.sum()) == int((kk < 2.0 / 3.0).sum())
+    assert set(np.unique(P)) <= {0.0, 1.0}
+    for mode in (bind.PS_JACOBI_RES, bind.PS_FAS, bind.PS_CASCADIC):
+        oc = bind.Oracle(bind.config(n, L, 0.8, poisson_mode=mode, nlj_max_it=100000, res_tol=1e-13, mg_levels=2,
+                                     mg_omega=1.25))
+        c = 1.7
+        phi = oc.poisson(np.zeros((n, n, n)), np.full((n, n, n), c))
+        assert np.abs(phi - np.log(c)).max() < 1e-9, mode
