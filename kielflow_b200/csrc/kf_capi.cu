@@ -1568,7 +1568,7 @@ void create(kf_ctx *c) {
     CK(cudaGetDevice(&dev));
     cudaDeviceProp prop;
     CK(cudaGetDeviceProperties(&prop, dev));
-    if (prop.major != 10) throw KfError{KF_ERR_NO_DEVICE, "this build targets sm_100a (B200)"};
+    if (prop.major != 10) throw KfError{KF_ERR_NO_DEVICE, "this library targets sm_100a (B200)"};
     if (cf.precision != KF_FP64 && cf.precision != KF_FP32_BULK) throw KfError{KF_ERR_ARG, "precision"};
     if (cf.pen_eta > 0.) throw KfError{KF_ERR_ARG, "penalization damping must be <= 0 (effect_penalization.cpp:7-12)"};
     if (!(cf.L > 0.) || !(cf.theta != 0.)) throw KfError{KF_ERR_ARG, "L > 0 and theta != 0 required"};

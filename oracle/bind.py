@@ -57,7 +57,7 @@ class KfoStats(ctypes.Structure):
 
 def build(with_ref: bool = True) -> None:
     """Compile liboracle.so and, when the reference sources are present,
-    _ref/libkfref.so (the GPU box only uses the prebuilt files)."""
+    _ref/libkfref.so (a machine without the reference sources uses the prebuilt files)."""
     subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
     if with_ref and os.path.isdir(REF_SRC):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REF_SRC}"], check=True)

@@ -1,7 +1,7 @@
 /*
  * kf_oracle.cpp -- CPU restatement of the reference's RK4 time-step hot path.
  *
- * TEST INFRASTRUCTURE.  This is the checker the CUDA path is compared with; it
+ * TEST INFRASTRUCTURE.  This is the restatement the CUDA path is compared with; it
  * is never linked into kielflow_b200/.  Every function cites the reference code
  * it restates (paths relative to the reference project).  The arithmetic is kept
  * in the reference's operation order so that, with the same FFT (fftw_shim.c)

@@ -8,7 +8,7 @@
  * runtime bitmask and with the terms the reference's driver does not enable
  * (Laplacian diffusion, masking penalization, spectral-viscosity cutoff, a
  * residual-based Poisson stop and an FAS V-cycle) added.  Only tests/, bench.py's
- * CPU-baseline leg and __graft_entry__.smoke() call it, as the checker.
+ * CPU-baseline leg and __graft_entry__.smoke() call it, to compare the CUDA path with.
  */
 #ifndef KF_ORACLE_H_
 #define KF_ORACLE_H_
