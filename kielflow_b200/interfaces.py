@@ -25,20 +25,33 @@ import numpy as np
 
 from ._lib import (KF_FP64, KF_PS_FAS, KF_PS_JACOBI_REF, KF_T_SHIPPED, Config, Context, KfError)
 from .inputs import axis_values, k_values
+from .inputs import val_at as _val_at
 
 
 class Grid:
-    """``grid`` of three ``axis_CoEqSt(l0, L, n)`` axes (grid_base.cpp:9-17,
-    axis_EqSt.cpp:6-61), cubic, l0 = -L/2."""
+    """``grid`` of three alike axes (grid_base.cpp:9-17), cubic, l0 = -L/2:
+    ``axis_CoEqSt(l0, L, n)`` (axis_EqSt.cpp:6-61, type_id 1) or, with m > 0,
+    the sine-stretched ``axis_CoSiSt(l0, L, n, m)`` (axis_SiSt.cpp, type_id 3;
+    the reference frontend's grid uses m = L (1 - 0.3) / (2 pi))."""
 
-    def __init__(self, n: int, L: float):
+    def __init__(self, n: int, L: float, m: float = 0.0):
+        if not (0.0 <= m and 2.0 * math.acos(-1.0) * m < L):
+            raise ValueError("axis_CoSiSt needs 0 <= 2 pi m < L")
         self.Nx = self.Ny = self.Nz = int(n)
         self.n = int(n)
         self.L = float(L)
         self.l0 = -0.5 * L
+        self.m = float(m)
+        self.type_id = 3 if m else 1
 
     def val_at(self, i: int) -> float:
-        return self.l0 + i * (self.L / self.n)
+        return _val_at(i, self.n, self.L, self.m)
+
+    def dS(self, i: int) -> float:
+        """Derivative of the axis map at index i (axis_SiSt.cpp:158-164; 1 for axis_CoEqSt)."""
+        pi = math.acos(-1.0)
+        x = self.l0 + (self.L / self.n) * i
+        return 1.0 - (2.0 * pi * self.m / self.L) * math.cos(2.0 * pi * x / self.L)
 
     def k_val_at(self, i: int) -> float:
         pi = math.acos(-1.0)
@@ -46,7 +59,7 @@ class Grid:
         return (2.0 * pi * i / self.L) if i <= n // 2 else (2.0 * pi * (i - n) / self.L)
 
     def x(self) -> np.ndarray:
-        return axis_values(self.n, self.L)
+        return axis_values(self.n, self.L, self.m)
 
     def k(self) -> np.ndarray:
         return k_values(self.n, self.L)
@@ -91,7 +104,7 @@ class RhsStandard:
         self.params = params
         cfg = Config.make(grid.n, grid.L, params.M, tau=params.tau, theta=params.theta, diff_D=diff_D,
                           sv_eps=sv_eps, sv_cut=sv_cut, pen_eta=pen_eta, terms=terms,
-                          poisson_mode=poisson_mode, precision=precision, **poisson_kw)
+                          poisson_mode=poisson_mode, precision=precision, stretch_m=grid.m, **poisson_kw)
         self.ctx = Context(cfg)
         self.ctx.set_sources(density_dust, solid_mask)
         if potential is not None:
@@ -144,7 +157,8 @@ class PoissonSolver:
 
     def _context(self):
         if self._ctx is None:
-            cfg = Config.make(self.grid.n, self.grid.L, 0.0, poisson_mode=self.mode, **self.kw)
+            cfg = Config.make(self.grid.n, self.grid.L, 0.0, poisson_mode=self.mode, stretch_m=self.grid.m,
+                              **self.kw)
             self._ctx = Context(cfg)
         return self._ctx
 

@@ -45,3 +45,29 @@ def test_config_layout_matches_header():
     body = text[text.index("typedef struct {"):text.index("} kf_config;")]
     names = re.findall(r"\b(?:int|double)\s+(\w+);", body)
     assert names == [f for f, _ in kf.Config._fields_]
+
+
+def test_grid_mirror_axes():
+    """interfaces.Grid: axis_CoEqSt and the sine-stretched axis_CoSiSt positions
+    (the restatement's, which match the reference's), dS and the config it
+    hands to the contexts."""
+    import math
+
+    import numpy as np
+
+    from kielflow_b200 import inputs as I
+    from kielflow_b200.interfaces import Grid
+    from oracle import bind
+
+    L = I.L_DEFAULT
+    m = I.frontend_stretch(L)
+    for mm in (0.0, m):
+        g = Grid(16, L, mm)
+        o = bind.Oracle(bind.config(16, L, 1.0, stretch_m=mm))
+        assert np.array_equal(np.array([g.val_at(i) for i in range(-1, 17)]), o.positions())
+        assert g.type_id == (3 if mm else 1)
+    g = Grid(16, L, m)
+    assert abs(g.dS(8) - 0.3) < 1e-15 and abs(g.dS(0) - 1.7) < 1e-15
+    assert abs(sum(g.dS(i) for i in range(16)) * (L / 16) - L) < 1e-12
+    with pytest.raises(ValueError):
+        Grid(16, L, L / (2.0 * math.pi))
