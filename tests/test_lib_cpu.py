@@ -71,3 +71,36 @@ def test_grid_mirror_axes():
     assert abs(sum(g.dS(i) for i in range(16)) * (L / 16) - L) < 1e-12
     with pytest.raises(ValueError):
         Grid(16, L, L / (2.0 * math.pi))
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """sizeof and every field offset of the C ABI's structs, compiled from
+    include/kielflow_b200.h with the host C compiler, against the ctypes mirrors."""
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no host C compiler")
+    mirrors = {"kf_config": _lib.Config, "kf_diag_out": _lib.DiagOut, "kf_grad_out": _lib.GradOut,
+               "kf_tune_out": _lib.TuneOut, "kf_output": _lib.Output, "kf_file_info": _lib.FileInfo}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{HEADER}"', "int main(void) {"]
+    for cname, py in mirrors.items():
+        lines.append(f'printf("{cname} sizeof %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c99", "-o", str(exe), str(src)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {}
+    for line in out:
+        if line:
+            s, f, v = line.split()
+            got[(s, f)] = int(v)
+    for cname, py in mirrors.items():
+        assert got[(cname, "sizeof")] == ctypes.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
