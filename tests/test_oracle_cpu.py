@@ -228,3 +228,31 @@ def test_oracle_fas_over_relaxed_reaches_the_same_solution():
         assert o.residual(phi, rho) <= 1e-11 and s.not_converged == 0
         out[om] = (phi, s.last_iterations)
     assert np.abs(out[0.0][0] - out[1.25][0]).max() < 1e-10
+
+
+def test_oracle_config_layout_matches_its_header(tmp_path):
+    """kfo_config (oracle/kf_oracle.h) against bind.KfoConfig, compiled with the
+    host C compiler: size and every field offset."""
+    import ctypes
+    import os
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no host C compiler")
+    hdr = os.path.join(os.path.dirname(bind.__file__), "kf_oracle.h")
+    lines = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{hdr}"', "int main(void) {",
+             'printf("sizeof %zu\\n", sizeof(kfo_config));']
+    for f, _ in bind.KfoConfig._fields_:
+        lines.append(f'printf("{f} %zu\\n", offsetof(kfo_config, {f}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "kfo.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "kfo"
+    subprocess.run([cc, "-std=c99", "-o", str(exe), str(src)], check=True)
+    got = dict(line.split() for line in
+               subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines())
+    assert int(got["sizeof"]) == ctypes.sizeof(bind.KfoConfig)
+    for f, _ in bind.KfoConfig._fields_:
+        assert int(got[f]) == getattr(bind.KfoConfig, f).offset, f
