@@ -16,7 +16,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libkfref.so")
-REF_SRC = "/root/reference"
+# directory of the kielflow sources that `make ref` compiles; taken from the
+# environment only (a machine without them uses the prebuilt _ref files)
+REF_SRC = os.environ.get("KF_REFERENCE_SRC", "")
 
 KFO_POISSON = 1 << 0
 KFO_DISSIPATION = 1 << 1
@@ -59,8 +61,11 @@ def build(with_ref: bool = True) -> None:
     """Compile liboracle.so and, when the reference sources are present,
     _ref/libkfref.so (a machine without the reference sources uses the prebuilt files)."""
     subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
-    if with_ref and os.path.isdir(REF_SRC):
+    if with_ref and REF_SRC and os.path.isdir(REF_SRC):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REF_SRC}"], check=True)
+    elif with_ref and not ref_available():
+        print("oracle: KF_REFERENCE_SRC is not set to the kielflow sources and _ref/libkfref.so is "
+              "not built; the tests that compare against the reference itself will be skipped")
 
 
 def _p(a: np.ndarray):
@@ -91,6 +96,7 @@ def lib():
         L.kfo_positions.argtypes = [ctypes.c_void_p, _D]
         L.kfo_metric.argtypes = [ctypes.c_void_p, _D]
         L.kfo_deriv.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D]
+        L.kfo_penalize.argtypes = [ctypes.c_void_p, ctypes.c_double, _D, _D]
         L.kfo_rk4.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
         L.kfo_poisson.argtypes = [ctypes.c_void_p, _D, _D]
         L.kfo_poisson_stats_get.argtypes = [ctypes.c_void_p, ctypes.POINTER(KfoStats)]
@@ -142,6 +148,8 @@ def ref():
         R.kfref_mg_solve.argtypes = [ctypes.c_int, ctypes.c_double, _D, _D]
         R.kfref_transfer.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, _D, _D]
         R.kfref_gauss.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double, _D]
+        R.kfref_penalize.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double, _D, _D, _D]
+        R.kfref_diffuse.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, _D, _D]
         _ref = R
     return _ref
 
@@ -242,11 +250,42 @@ class Oracle:
         self.L.kfo_deriv(self.h, d, F.ctypes.data_as(_D), out.ctypes.data_as(_D))
         return out
 
+    def penalize(self, fix, F_in, F_out):
+        """The right-hand side's masking penalization of one field: returns
+        r2c((1 - H) c2r(F_out) + H pen_eta (c2r(F_in) - fix))."""
+        F_in = np.ascontiguousarray(F_in, np.complex128)
+        out = np.array(F_out, np.complex128, order="C", copy=True)
+        self.L.kfo_penalize(self.h, fix, F_in.ctypes.data_as(_D), out.ctypes.data_as(_D))
+        return out
+
     def metric(self):
         """The filtered 1/dS of the derivative along one axis (n values)."""
         out = np.zeros(self.n)
         self.L.kfo_metric(self.h, _p(out))
         return out
+
+
+def ref_penalize(n, L, eta, fix, H, F_in, F_out):
+    """effect_penalization(eta, H, fix).execute(F_in, F_out) of the reference
+    (effect_penalization.cpp:21-44); returns the new F_out."""
+    H = np.ascontiguousarray(H, np.float64)
+    F_in = np.ascontiguousarray(F_in, np.complex128)
+    out = np.array(F_out, np.complex128, order="C", copy=True)
+    R = ref()
+    if R.kfref_penalize(n, L, eta, fix, _p(H), F_in.ctypes.data_as(_D), out.ctypes.data_as(_D)):
+        raise RuntimeError(R.kfref_last_error().decode())
+    return out
+
+
+def ref_diffuse(n, L, nu, F_in, F_out):
+    """effect_diffusion(nu).execute(F_in, F_out) of the reference as written
+    (effect_diffusion.cpp:16-44); one grid size per process."""
+    F_in = np.ascontiguousarray(F_in, np.complex128)
+    out = np.array(F_out, np.complex128, order="C", copy=True)
+    R = ref()
+    if R.kfref_diffuse(n, L, nu, F_in.ctypes.data_as(_D), out.ctypes.data_as(_D)):
+        raise RuntimeError(R.kfref_last_error().decode())
+    return out
 
 
 def r2c(x: np.ndarray) -> np.ndarray:

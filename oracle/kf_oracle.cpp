@@ -220,6 +220,17 @@ void dealias(const kfo_ctx *c, vec &F) {
     }
 }
 
+/* effect_penalization::execute (effect_penalization.cpp:21-44), masking form,
+ * on one finished right-hand-side field: out <- r2c((1 - H) c2r(out)
+ * + H eta_d (q - q_fix)), with q the field's state in physical space
+ * (the reference forms it as iFFT of its `in`); b: scratch */
+void penalize(const kfo_ctx *c, const vec &q, double fix, vec &out, vec &b) {
+    c2r(c, out, b);
+    for (size_t i = 0; i < c->N; ++i)
+        b[i] = (1. - c->mask[i]) * b[i] + c->mask[i] * c->cfg.pen_eta * (q[i] - fix);
+    r2c(c, b, out);
+}
+
 /* OP_partial_derivative::operator() (OP_partial_derivative.cpp:104-136): i k
  * times the input; on a stretched axis, then dealiased, taken to physical
  * space, multiplied by the filtered 1/dS of the direction and transformed back. */
@@ -746,11 +757,7 @@ int rhs(kfo_ctx *c, vec *FU, vec &Fni, double t) {
         const double qfix[4] = {-cf.M, 0., 0., -10.};
         for (int q = 0; q < 4; ++q) {
             vec &out = q < 3 ? FU[q] : Fni;
-            const vec &qq = q < 3 ? U[q] : sd;
-            c2r(c, out, b1);
-            for (size_t i = 0; i < N; ++i)
-                b1[i] = (1. - c->mask[i]) * b1[i] + c->mask[i] * cf.pen_eta * (qq[i] - qfix[q]);
-            r2c(c, b1, out);
+            penalize(c, q < 3 ? U[q] : sd, qfix[q], out, b1);
             dealias(c, out);
         }
     }
@@ -834,6 +841,13 @@ void kfo_deriv(kfo_ctx *c, int dir, const double *in, double *out) {
     vec a(in, in + 2 * c->Nc), b;
     deriv(c, dir, a, b);
     std::memcpy(out, b.data(), sizeof(double) * 2 * c->Nc);
+}
+
+void kfo_penalize(kfo_ctx *c, double fix, const double *in, double *out) {
+    vec a(in, in + 2 * c->Nc), o(out, out + 2 * c->Nc), q, b;
+    c2r(c, a, q);
+    penalize(c, q, fix, o, b);
+    std::memcpy(out, o.data(), sizeof(double) * 2 * c->Nc);
 }
 
 void kfo_metric(kfo_ctx *c, double *out) {

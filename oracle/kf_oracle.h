@@ -87,6 +87,10 @@ void kfo_positions(kfo_ctx *c, double *out);
 void kfo_metric(kfo_ctx *c, double *out);
 /* OP_partial_derivative on the context's grid: out = d/dx_dir of in (half spectra) */
 void kfo_deriv(kfo_ctx *c, int dir, const double *in, double *out);
+/* the right-hand side's masking penalization of one field (the restatement of
+ * effect_penalization::execute, effect_penalization.cpp:21-44): out <- r2c((1 - H)
+ * c2r(out) + H pen_eta (c2r(in) - fix)), H = the mask of kfo_set_sources */
+void kfo_penalize(kfo_ctx *c, double fix, const double *in, double *out);
 int kfo_rk4(kfo_ctx *c, double dt, int nsteps);
 double kfo_time(kfo_ctx *c);
 int kfo_poisson(kfo_ctx *c, double *phi_io, const double *rho);

@@ -4,7 +4,8 @@
  * TEST INFRASTRUCTURE (oracle/_ref).  Compiled together with the reference's
  * unmodified sources (RKO4.cpp, rhs_standard.cpp, OP_*.cpp, operations.cpp,
  * field_*.cpp, field_interpolation.cpp, axis_EqSt.cpp, axis_SiSt.cpp, grid_base.cpp,
- * solver_poisson_jacobi_nlin.cpp, solver_poisson_multigrid.cpp, parameters.cpp)
+ * solver_poisson_jacobi_nlin.cpp, solver_poisson_multigrid.cpp, parameters.cpp,
+ * effect_penalization.cpp, effect_diffusion.cpp)
  * so that the Python tests can drive the reference exactly as its driver does
  * (kielflow.cpp:156-286) on seeded in-memory inputs instead of HDF5 files.
  * This file only wires objects together; every number comes from reference code.
@@ -17,6 +18,8 @@
 #include "RKO4.hpp"
 #include "axis_EqSt.hpp"
 #include "axis_SiSt.hpp"
+#include "effect_diffusion.hpp"
+#include "effect_penalization.hpp"
 #include "field.hpp"
 #include "grid.hpp"
 #include "masks.hpp"
@@ -325,6 +328,52 @@ void kfref_gauss_m(int n, double L, double m, double Q, double sigma, double *ou
     fkt3d_Gauss fk(Q, sigma, sigma, sigma);
     f.fill(fk);
     std::memcpy(out, f.val, sizeof(double) * f.N);
+}
+
+/* effect_penalization::execute (effect_penalization.cpp:21-44) on an n^3
+ * equidistant grid: out <- FFT((1 - H) iFFT(out) + H eta (iFFT(in) - fix)).
+ * The constructor's guard (:7-12) refuses eta > 0: -1 and kfref_last_error. */
+int kfref_penalize(int n, double L, double eta, double fix, const double *H, const double *in,
+                   double *out) {
+    try {
+        grid g = make_grid(n, L);
+        field_real mask(g);
+        field_imag a(g), b(g);
+        std::memcpy(mask.val, H, sizeof(double) * mask.N);
+        put_c(a, in);
+        put_c(b, out);
+        effect_penalization pen(eta, mask, fix);
+        pen.execute(a, b);
+        get_c(b, out);
+        return 0;
+    } catch (const char *e) { g_err = e; } catch (const std::string &e) { g_err = e; }
+    catch (...) { g_err = "unknown exception"; }
+    return -1;
+}
+
+/* effect_diffusion::execute (effect_diffusion.cpp:16-44) as written: out -=
+ * nu * (the three second derivatives of in).  Its derivative operators are
+ * function-static (built on the first call's grid), so one grid size per
+ * process: -2 for another size. */
+int kfref_diffuse(int n, double L, double nu, const double *in, double *out) {
+    static int first_n = -1;
+    if (first_n >= 0 && first_n != n) {
+        g_err = "effect_diffusion keeps static derivative operators: one grid size per process";
+        return -2;
+    }
+    first_n = n;
+    try {
+        static grid g = make_grid(n, L);
+        field_imag a(g), b(g);
+        put_c(a, in);
+        put_c(b, out);
+        effect_diffusion diff(nu);
+        diff.execute(a, b);
+        get_c(b, out);
+        return 0;
+    } catch (const char *e) { g_err = e; } catch (const std::string &e) { g_err = e; }
+    catch (...) { g_err = "unknown exception"; }
+    return -1;
 }
 
 /* fkt3d_Gauss (masks.hpp:351-366) sampled on the grid through field_real::fill. */

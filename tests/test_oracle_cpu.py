@@ -256,3 +256,95 @@ def test_oracle_config_layout_matches_its_header(tmp_path):
     assert int(got["sizeof"]) == ctypes.sizeof(bind.KfoConfig)
     for f, _ in bind.KfoConfig._fields_:
         assert int(got[f]) == getattr(bind.KfoConfig, f).offset, f
+
+
+# ------------------------------------------------- the terms the shipped RHS lacks
+# Diffusion, masking penalization and the spectral-viscosity cut are not called by
+# the reference's rhs_standard.cpp; their formula sources are effect_penalization.cpp
+# and effect_diffusion.cpp, compiled into oracle/_ref from the reference's sources.
+
+needs_ref = pytest.mark.skipif(not bind.ref_available(), reason="reference not compiled here")
+
+
+def _seeded_spectra(n, seed, count):
+    rng = np.random.default_rng(seed)
+    return [bind.r2c(rng.standard_normal((n, n, n))) for _ in range(count)]
+
+
+@needs_ref
+@pytest.mark.parametrize("fix", [0.0, -1.0, -10.0])
+def test_oracle_penalization_matches_reference_effect(fix):
+    """The restatement's masking penalization is effect_penalization::execute
+    (effect_penalization.cpp:21-44) bit for bit, on a ragged mask."""
+    n = 16
+    rng = np.random.default_rng(7)
+    H = (rng.random((n, n, n)) < 0.3).astype(np.float64)
+    H[0, 0, :] = 0.5  # a partial cell value, not only 0/1
+    F_in, F_out = _seeded_spectra(n, 11, 2)
+    o = bind.Oracle(bind.config(n, L, 1.0, pen_eta=C.PEN_ETA))
+    o.set_sources(np.zeros((n, n, n)), H)
+    assert np.array_equal(o.penalize(fix, F_in, F_out), bind.ref_penalize(n, L, C.PEN_ETA, fix, H, F_in, F_out))
+
+
+@needs_ref
+def test_reference_penalization_guard():
+    """effect_penalization's constructor refuses a positive damping (:7-12)
+    (the library's context refuses pen_eta > 0 the same way: GPU tests)."""
+    n = 8
+    F = _seeded_spectra(n, 3, 1)[0]
+    with pytest.raises(RuntimeError, match="damping"):
+        bind.ref_penalize(n, L, 1e-3, 0.0, np.zeros((n, n, n)), F, F)
+
+
+def test_oracle_diffusion_single_mode_known_answer():
+    """Laplacian diffusion alone: d/dt q^ = -D |k|^2 q^ for a single Fourier
+    mode of every field (k from the axis's k_val_at, the Nyquist +pi n/L of
+    axis_EqSt.cpp:57-61 included), to the last bit or two."""
+    n = 16
+    D = C.DIFF_D
+    kv = [2 * np.pi / L * (i if i <= n // 2 else i - n) for i in range(n)]
+    o = bind.Oracle(bind.config(n, L, 1.0, diff_D=D, terms=bind.KFO_DIFFUSION))
+    o.set_sources(np.zeros((n, n, n)), np.zeros((n, n, n)))
+    for m in [(1, 0, 1), (1, 2, 3), (0, 0, 5), (4, 4, 4), (8, 15, 7)]:
+        F = np.zeros((n, n, n // 2 + 1), np.complex128)
+        F[m] = 0.3 - 0.7j
+        o.set_state([F, 2 * F, -F, 0.5 * F])
+        o.rhs()
+        k2 = kv[m[0]] ** 2 + kv[m[1]] ** 2 + kv[m[2]] ** 2
+        for got, a in zip(o.get_state(), (1.0, 2.0, -1.0, 0.5)):
+            want = -D * k2 * a * F
+            assert np.abs(got - want).max() <= 4.5e-16 * np.abs(want).max()
+
+
+@needs_ref
+def test_oracle_diffusion_matches_reference_effect_imaginary_part():
+    """effect_diffusion::execute (effect_diffusion.cpp:16-44) subtracts nu times
+    the sum of the three second derivatives (OP_partial_derivative twice, the
+    Nyquist k of axis_EqSt.cpp:57-61 included) from the accumulator that the
+    right-hand side negates.  Its imaginary part agrees with the restatement to
+    rounding; its real part uses the imaginary parts again (:39-40), which the
+    restatement does not copy: there it is D |k|^2 Re q^."""
+    import subprocess
+    import sys
+    # effect_diffusion keeps function-static derivative operators: its own process
+    code = (
+        "import numpy as np, sys; sys.path.insert(0, %r)\n"
+        "from oracle import bind\n"
+        "from kielflow_b200 import inputs as I\n"
+        "n, L, D = 16, I.L_DEFAULT, 1e-3\n"
+        "rng = np.random.default_rng(5)\n"
+        "F = bind.r2c(rng.standard_normal((n, n, n)))\n"
+        "o = bind.Oracle(bind.config(n, L, 1.0, diff_D=D, terms=bind.KFO_DIFFUSION))\n"
+        "o.set_sources(np.zeros((n, n, n)), np.zeros((n, n, n)))\n"
+        "o.set_state([F, F, F, F]); o.rhs(); fb = -o.get_state()[3]\n"
+        "r = bind.ref_diffuse(n, L, D, F, np.zeros_like(F))\n"
+        "print(float(np.abs(r.imag - fb.imag).max() / np.abs(fb.imag).max()),"
+        " bool(np.array_equal(r.real, r.imag)),"
+        " float(np.abs(fb.real - fb.imag).max() / np.abs(fb.real).max()))\n"
+    ) % os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr
+    e_im, slip, re_vs_im = out.stdout.split()
+    assert float(e_im) <= 1e-15
+    assert slip == "True"           # the reference's real part repeats the imaginary sum
+    assert float(re_vs_im) > 1e-3   # the restatement's real part does not
