@@ -19,6 +19,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -46,6 +47,9 @@ def parse():
     ap.add_argument("--no-tune", action="store_true",
                     help="keep the default kernel variants (no kf_autotune; profiling runs)")
     ap.add_argument("--cpu-ref", default="", help=argparse.SUPPRESS)
+    ap.add_argument("--profile-range", action="store_true",
+                    help="bracket the timed steps of the first arm with cudaProfilerStart/Stop "
+                         "(for ncu --profile-from-start off); changes no work")
     ap.add_argument("--marks", default="100,500,2000", help="steps at which --workload precision compares")
     ap.add_argument("--adjoint-steps", type=int, default=200,
                     help="RK4 steps of the adjoint leg (128^3 FP64, checkpoints every 15); 0 skips it")
@@ -148,67 +152,88 @@ class _QuietStdout:
         os.close(self.null)
 
 
-def cpu_reference_rhs_seconds(nsamples: int, warmup: int, budget_s: float):
-    with _QuietStdout():
-        return _cpu_reference_rhs_seconds(nsamples, warmup, budget_s)
-
-
-def _cpu_reference_rhs_seconds(nsamples: int, warmup: int, budget_s: float):
-    """The reference's own rhs_standard::solve (its sources compiled here,
-    shipped term set, cascadic multigrid plan of kielflow.cpp:207-217) at 128^3
-    with the workload's M, tau, dust; returns per-sample seconds."""
+def workload_config(w, name, ws):
+    """The config dict of a workload, shared by both arms of the bench."""
     from kielflow_b200 import configs as C
-    from kielflow_b200 import inputs as I
-    from oracle import bind  # CPU baseline leg only
-    if not bind.ref_available():
-        return None, "oracle/_ref not built"
-    w = C.WORKLOADS["fp32bulk256"]
-    n = 128
-    st = I.initial_state(n, seed=0)
-    nd = I.gauss_charge(n, C.L_BOX, w["Q"], w["sigma"])
-    mask = I.sphere_mask(n, C.L_BOX, C.MASK_RADIUS)
-    R = bind.Reference(n, C.L_BOX, w["M"], w["tau"], C.THETA, poisson_mode=1)
-    R.set_real(0, nd)
-    R.set_real(1, mask)
-    times = []
-    t_start = time.time()
-    for i in range(warmup + nsamples):
-        R.set_state(st)
+    cfg = C.config_for(w)
+    st, nd, mask, dt = C.make_inputs(w)
+    return {"workload": f"{name}: {w['n']}^3 box 2*pi*4, M {w['M']}, nu {w['tau']}, Q {w['Q']}, sigma {w['sigma']}, "
+                        f"FAS {cfg.mg_levels} levels 2+2 to residual {cfg.res_tol:.3g} (FP32 bulk: 2^-23 max|n_d|; "
+                        f"FP64: 1e-10; at most {cfg.max_cycles} V-cycles per solve), penalization, diffusion 1e-3, "
+                        f"SV > 0.6 k_max",
+            "n": w["n"], "dt": dt, "l2": "inputs larger than L2 (state + work buffers > 2 GB)",
+            "axes": (f"axis_CoSiSt m {w['stretch']:.6g} (sine-stretched, chain-rule derivatives)"
+                     if w.get("stretch") else "axis_CoEqSt"),
+            "parallelism": f"replicas x{ws}"}
+
+
+def oracle_rk4_seconds(w, n, steps, warmup, budget_s):
+    """The CPU restatement of the path (oracle/, pinned to the reference's own
+    sources) on the workload's physics at n^3 in FP64: seconds of each timed
+    RK4 step, after `warmup` untimed steps, stopping once budget_s is spent
+    (at least one timed step).  Runs on all host cores (KF_ORACLE_THREADS)."""
+    from kielflow_b200 import configs as C
+    from oracle import bind  # CPU baseline / reference arm only
+    st, nd, mask, dt = C.make_inputs(w, n=n)
+    from kielflow_b200._lib import KF_FP64
+    cfg = C.config_for(w, n=n, precision=KF_FP64)  # the CPU path computes in double
+    o = bind.Oracle(bind.KfoConfig(*[getattr(cfg, f) for f, _ in bind.KfoConfig._fields_]))
+    o.set_state(st)
+    o.set_sources(nd, mask)
+    o.rk4(dt, warmup)
+    times, t_start = [], time.perf_counter()
+    while len(times) < steps:
         t0 = time.perf_counter()
-        R.rhs()
-        dt = time.perf_counter() - t0
-        if i >= warmup:
-            times.append(dt)
-        if time.time() - t_start > budget_s and times:
+        o.rk4(dt, 1)
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_start > budget_s:
             break
-    return times, None
+    return times, bind.lib().kfs_nthreads()
 
 
-def cpu_baseline_entry(times, n_full=256, n_sample=128):
-    scale = (n_full / n_sample) ** 3
+def cpu_baseline_entry(w, name):
+    """Bounded CPU sample for the GPU arm's line: two RK4 steps of the oracle
+    at 128^3 (after one untimed step), scaled to 256^3 by N log N."""
+    n_s, n_f = 128, w["n"]
+    times, cores = oracle_rk4_seconds(w, n_s, 2, 1, 60.0)
     t = statistics.mean(times)
-    return {"value": 1.0 / (4.0 * scale * t), "unit": UNIT, "cores": 1, "kind": "reference",
-            "sample": (f"{len(times)} x rhs_standard::solve of the reference (its own sources, shipped "
-                       f"terms, cascadic MG) at {n_sample}^3, mean {t:.2f} s, scaled by the point "
-                       f"count ({scale:.0f}x) to one 256^3 RHS and by 4 RHS per RK4 step; single "
-                       f"thread (the reference has no parallel regions)")}
+    scale = (n_f / n_s) ** 3 * (math.log(n_f) / math.log(n_s))
+    return {"value": 1.0 / (scale * t), "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": (f"{len(times)} RK4 steps of the CPU restatement (oracle/kf_oracle.cpp, pinned to the "
+                       f"reference's own rhs_standard/RKO4/solver sources) on the {name} physics at "
+                       f"{n_s}^3 in FP64, mean {t:.2f} s on {cores} threads, scaled by N log N "
+                       f"({scale:.2f}x) to {n_f}^3")}
 
 
 def run_reference(args):
+    """The reference arm: the CPU path on the GPU arm's own workload (the
+    FP32-bulk workload's physics, computed in FP64 as the reference's FFTW path
+    does), real RK4 steps at full size on all host cores."""
+    from kielflow_b200 import configs as C
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
-    times, err = cpu_reference_rhs_seconds(args.steps, min(args.warmup, 1), budget_s=150.0)
-    if times is None:
-        print(json.dumps({"impl": "reference", "unavailable": err}))
+    from oracle import bind
+    try:
+        bind.lib()
+    except OSError as e:
+        print(json.dumps({"impl": "reference", "unavailable": f"oracle not built: {e}"}))
         return 0
-    cb = cpu_baseline_entry(times)
-    v = cb["value"]
+    name = args.workload
+    w = C.WORKLOADS[name]
+    warm = min(args.warmup, 1)
+    times, cores = oracle_rk4_seconds(w, w["n"], args.steps, warm, budget_s=150.0)
+    tot = sum(times)
+    v = len(times) / tot
+    cb = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+          "sample": (f"{len(times)} full {w['n']}^3 RK4 steps (of {args.steps} requested; the timed region "
+                     f"stops after 150 s) of the CPU restatement (oracle/kf_oracle.cpp, pinned to the "
+                     f"reference's own sources: rhs_standard, RKO4, Poisson solvers, effect_penalization, "
+                     f"effect_diffusion) on {cores} threads, FP64, after {warm} untimed step")}
     out = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": len(times),
-           "warmup": min(args.warmup, 1), "ms_per_step": 1000.0 / v, "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": "fp32bulk256 (reference CPU path, sampled at 128^3)", "n": 256},
-           "impl": "reference", "cpu_baseline": cb,
+           "steps_requested": args.steps, "warmup": warm, "ms_per_step": 1000.0 * tot / len(times),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": workload_config(w, name, 1), "impl": "reference", "cpu_baseline": cb,
            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
     return 0
@@ -280,14 +305,14 @@ def run_kf(args):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         return float(t.item())
 
-    def timed_arm(precision, profile=False, clocks=False):
+    def timed_arm(precision, profile=False, clocks=False, prange=False):
         cfg = C.config_for(w, precision=precision)
         ctx = kf.Context(cfg)
         ctx.set_stream(stream.cuda_stream)
         ctx.set_state(*st)
         ctx.set_sources(nd, mask)
         # radix plan and smoother shape, timed on this context
-        tune = ctx.autotune() if not args.no_tune else {"fft_plan": 0, "rbgs_rows": 8,
+        tune = ctx.autotune() if not args.no_tune else {"fft_plan": 0, "rbgs_rows": 0,
                                                          "fft_radices": [[], []]}
         ctx.rk4(dt, args.warmup)
         ctx.synchronize()
@@ -296,11 +321,15 @@ def run_kf(args):
         sampler = ClockSampler(torch.cuda.current_device()) if clocks else None
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         l0 = ctx.launch_count()
+        if prange:
+            torch.cuda.profiler.start()
         with torch.cuda.stream(stream):
             e0.record(stream)
             ctx.rk4(dt, args.steps)
             e1.record(stream)
         stream.synchronize()
+        if prange:
+            torch.cuda.profiler.stop()
         torch.cuda.synchronize()
         barrier()
         launches = ctx.launch_count() - l0
@@ -308,6 +337,7 @@ def run_kf(args):
         ms = max_over_ranks(e0.elapsed_time(e1))
         d = ctx.diag()
         phi = ctx.get_phi()  # after warm-up + timed steps in both precisions
+        state = ctx.get_state()
         prof = None
         if profile:
             # per-kernel CUDA-event profile of further steps of the same run
@@ -317,9 +347,10 @@ def run_kf(args):
             prof = ctx.profile_read()
             ctx.profile(False)
         ctx.tune = tune
-        return ctx, ms, launches, prof, clk, d, phi
+        return ctx, ms, launches, prof, clk, d, phi, state
 
-    ctx32, ms32, launches, prof, clk, d32, phi32 = timed_arm(w["precision"], profile=True, clocks=True)
+    ctx32, ms32, launches, prof, clk, d32, phi32, st32 = timed_arm(w["precision"], profile=True, clocks=True,
+                                                                      prange=args.profile_range)
     value = ws * args.steps / (ms32 / 1000.0)
 
     # end-to-end through the C ABI with host (pinned) buffers: H2D state, one
@@ -363,12 +394,28 @@ def run_kf(args):
 
     fp64 = None
     if not args.no_fp64 and w["precision"] != kf.KF_FP64:
-        ctx64, ms64, _, _, _, d64, phi64 = timed_arm(kf.KF_FP64)
+        ctx64, ms64, _, _, _, d64, phi64, st64 = timed_arm(kf.KF_FP64)
         tune64 = ctx64.tune
         ctx64.close()
-        err = float(np.abs(phi32 - phi64).max() / np.abs(phi64).max())
+        n_ = w["n"]
+
+        def real(F):
+            return np.fft.irfftn(F, s=(n_, n_, n_), axes=(0, 1, 2))
+
+        def rel_linf(a, b):
+            return float(np.abs(a - b).max() / np.abs(b).max())
+
+        err = rel_linf(phi32, phi64)
+        u32 = np.stack([real(x) for x in st32[:3]])
+        u64 = np.stack([real(x) for x in st64[:3]])
+        u32[0] += w["M"]
+        u64[0] += w["M"]
+        errs = {"phi": err, "n": rel_linf(np.exp(real(st32[3])), np.exp(real(st64[3]))), "u_total": rel_linf(u32, u64),
+                "at_step": args.warmup + args.steps, "norm": "relative max-norm over the grid"}
+        del u32, u64
         fp64 = {"value": ws * args.steps / (ms64 / 1000.0), "ms_per_step": ms64 / args.steps,
                 "phi_rel_err_fp32_vs_fp64": max_over_ranks(err),
+                "fp32_vs_fp64_errors": {k: (max_over_ranks(v) if isinstance(v, float) else v) for k, v in errs.items()},
                 "charge_fp32": d32.charge, "charge_fp64": d64.charge,
                 "kinetic_fp32": d32.kinetic, "kinetic_fp64": d64.kinetic,
                 "tuning": {"fft_radices": tune64["fft_radices"][tune64["fft_plan"]],
@@ -397,8 +444,10 @@ def run_kf(args):
 
     cpu = None
     if not args.no_cpu and ws == 1:
-        times, err = cpu_reference_rhs_seconds(3, 0, budget_s=40.0)
-        cpu = cpu_baseline_entry(times) if times else {"unavailable": err}
+        try:
+            cpu = cpu_baseline_entry(w, args.workload)
+        except OSError as e:
+            cpu = {"unavailable": f"oracle not built: {e}"}
 
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
@@ -406,16 +455,9 @@ def run_kf(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32 bulk + fp64 Poisson"
         if w["precision"] == kf.KF_FP32_BULK else "f64",
         "data": "synthetic (seeded noise, Gaussian dust; seed = rank)",
-        "config": {"workload": f"{args.workload}: {w['n']}^3 box 2*pi*4, M {w['M']}, nu {w['tau']}, "
-                               f"Q {w['Q']}, sigma {w['sigma']}, FAS {C.config_for(w).mg_levels} levels 2+2 to 1e-10 "
-                               f"(at most {C.config_for(w).max_cycles} V-cycles per solve), penalization, "
-                               f"diffusion 1e-3, SV > 0.6 k_max",
-                   "n": w["n"], "dt": dt, "l2": "inputs larger than L2 (state + work buffers > 2 GB)",
-                   "axes": (f"axis_CoSiSt m {w['stretch']:.6g} (sine-stretched, chain-rule derivatives)"
-                            if w.get("stretch") else "axis_CoEqSt"),
-                   "parallelism": f"replicas x{ws}",
-                   "tuning": {"fft_radices": tune32["fft_radices"][tune32["fft_plan"]],
-                              "rbgs_rows": tune32["rbgs_rows"]}},
+        "config": workload_config(w, args.workload, ws),
+        "tuning": {"fft_radices": tune32["fft_radices"][tune32["fft_plan"]], "rbgs_rows": tune32["rbgs_rows"],
+                   "rbgs_rows_meaning": "0: streaming TMA-staged sweep (k_rbgs_march)"},
         "gpu_launches": launches,
         "roofline": roofline,
         "cpu_baseline": cpu,

@@ -252,16 +252,22 @@ int kf_batch_rk4_steps(kf_ctx *const *ctxs, int nctx, int nsteps, const double *
  * FFTW plans are chosen by FFTW_MEASURE inside fftw_plan_dft_*, OP_FFT.cpp).
  * fft_plan: radix plan of every transform kernel, 0 or 1 (two factorisations
  * of each supported n into radix stages, with different threads per line);
- * rbgs_rows: rows per block of the red-black smoother, 4, 8 or 16.  Results
- * do not depend on rbgs_rows (same arithmetic per point) and agree between
- * the fft plans to rounding. */
+ * rbgs_rows: the red-black smoother, 0 (the default) for the streaming sweep
+ * (one TMA-staged pass per sweep, the residual fused into the last
+ * pre-smoothing sweep) on multigrid levels with n a multiple of 64 and the
+ * 8-row half-sweep kernel below them, or 4, 8, 16 for half-sweep kernels with
+ * that many rows per block on every level.  Results do not depend on
+ * rbgs_rows (same arithmetic per point, bit for bit) and agree between the
+ * fft plans to rounding. */
 typedef struct kf_tune_out {
     int fft_plan;          /* chosen radix plan */
-    int rbgs_rows;         /* chosen rows per smoother block */
+    int rbgs_rows;         /* chosen smoother: rows per k_rbgs block (4, 8, 16), or 0 */
+                           /* for the streaming TMA-staged sweep (levels n >= 64)   */
     int fft_radices[2][4]; /* radix stages of plans 0 and 1 (0 = unused) */
     int fft_threads[2];    /* threads per transformed line of plans 0 and 1 */
     double fft_ms[2];      /* one right-hand side without its Poisson solve, per plan */
-    double rbgs_ms[3];     /* one finest-level smoothing sweep with 4, 8, 16 rows */
+    double rbgs_ms[4];     /* one finest-level smoothing sweep with 4, 8, 16 rows and */
+                           /* with the streaming sweep (-1: not available)          */
 } kf_tune_out;
 
 /* Time the variants on the context's own buffers (reps timed calls each,
@@ -351,8 +357,14 @@ int kf_adjoint_run(kf_ctx *ctx, int nsteps, double dt, int ckpt_every, int flags
  * cuda_stream (NULL: the legacy default stream) and the call returns
  * without waiting.  All calls on one device share that array: calls that
  * overlap on the GPU race and must be serialised by the caller.  The first
- * call on each device looks up the array's device address; make it before
- * any stream capture.  Errors are reported by kf_last_error(NULL). */
+ * call on each device is a warm-up: it looks up the array's device address
+ * and, under lazy module loading (the CUDA default), loads the module, which
+ * places the array in device memory and synchronises; make it before the
+ * allocation-free part of the program and before any stream capture (a
+ * captured first call returns KF_ERR_ARG).  Later uncaptured calls look the
+ * address up again, so it stays right after a cudaDeviceReset.  An error
+ * already pending from earlier work is reported (KF_ERR_CUDA) and left
+ * pending.  Errors are reported by kf_last_error(NULL). */
 int kf_fft_r2c_noalloc(int n, const double *in_real, double *out_complex, void *cuda_stream);
 
 #ifdef __cplusplus

@@ -83,7 +83,7 @@ class GradOut(ctypes.Structure):
 class TuneOut(ctypes.Structure):
     """kf_tune_out (include/kielflow_b200.h)."""
     _fields_ = [("fft_plan", ctypes.c_int), ("rbgs_rows", ctypes.c_int), ("fft_radices", (ctypes.c_int * 4) * 2),
-                ("fft_threads", ctypes.c_int * 2), ("fft_ms", ctypes.c_double * 2), ("rbgs_ms", ctypes.c_double * 3)]
+                ("fft_threads", ctypes.c_int * 2), ("fft_ms", ctypes.c_double * 2), ("rbgs_ms", ctypes.c_double * 4)]
 
     def as_dict(self):
         return {"fft_plan": self.fft_plan, "rbgs_rows": self.rbgs_rows,
@@ -348,7 +348,9 @@ class Context:
         return o.as_dict()
 
     def set_tuning(self, fft_plan: int, rbgs_rows: int):
-        """kf_set_tuning: select the transform plan (0, 1) and smoother rows (4, 8, 16)."""
+        """kf_set_tuning: select the transform plan (0, 1) and the smoother: 0 for the
+        streaming TMA-staged sweep (the default), or 4, 8, 16 rows per block of the
+        half-sweep kernel."""
         self._check(self.L.kf_set_tuning(self.h, fft_plan, rbgs_rows))
 
     def rk4(self, dt: float, nsteps: int = 1):

@@ -54,6 +54,16 @@ WORKLOADS = {
 }
 
 
+def fp32_res_tol(Q: float, sigma: float) -> float:
+    """Residual target of the FP64 Poisson solve when its source comes from an
+    FP32 state (KF_FP32_BULK): the FP32 unit roundoff 2^-23 times the largest
+    magnitude of the source rho = e^s + n_d, which the grain's peak density
+    |Q| / (pi^1.5 sigma^3) sets (fkt3d_Gauss, masks.hpp:351-366).  Below that the
+    solve only resolves the rounding of its own input; the FP64 residual, Newton
+    update and coarsest solve are unchanged.  The FP64 path keeps 1e-10."""
+    return 2.0 ** -23 * abs(Q) / (math.pi ** 1.5 * sigma ** 3)
+
+
 def config_for(w: dict, n: int | None = None, precision: int | None = None, **over) -> Config:
     """kf_config of a workload dict (optionally on another grid size)."""
     n = n or w["n"]
@@ -69,12 +79,13 @@ def config_for(w: dict, n: int | None = None, precision: int | None = None, **ov
         while m > 16 and m % 2 == 0:
             m //= 2
             levels += 1
+    prec = w["precision"] if precision is None else precision
+    res_tol = fp32_res_tol(w["Q"], w["sigma"]) if prec == KF_FP32_BULK else 1e-10
     kw = dict(tau=w["tau"], theta=THETA, diff_D=DIFF_D, sv_eps=0.5, sv_cut=0.6 if w["sv"] else 0.0,
               pen_eta=PEN_ETA, terms=terms, poisson_mode=w["poisson_mode"], nlj_max_it=100000,
-              nlj_limit=0.5e-5, res_tol=1e-10, mg_levels=levels, mg_pre=2, mg_post=2, coarse_tol=1e-13,
+              nlj_limit=0.5e-5, res_tol=res_tol, mg_levels=levels, mg_pre=2, mg_post=2, coarse_tol=1e-13,
               max_cycles=w.get("max_cycles", 100), phi_extrap=1, mg_omega=w.get("omega", MG_OMEGA),
-              precision=w["precision"] if precision is None else precision,
-              stretch_m=w.get("stretch", 0.0))
+              precision=prec, stretch_m=w.get("stretch", 0.0))
     kw.update(over)
     return Config.make(n, L_BOX, w["M"], **kw)
 

@@ -21,6 +21,7 @@
 #include "../../include/kielflow_b200.h"
 #include "kf_adjoint.cuh"
 #include "kf_graph.cuh"
+#include "kf_march.cuh"
 #include "kf_passes.cuh"
 #include "kf_pointwise.cuh"
 #include "kf_poisson.cuh"
@@ -45,6 +46,7 @@ struct LevelBuf {
     int n = 0;
     double *dd = nullptr, *dp = nullptr, *dm = nullptr, *ip = nullptr, *im = nullptr, *gam = nullptr;
     double *phi = nullptr, *rho = nullptr, *r = nullptr, *phi0 = nullptr;
+    double *t = nullptr;  // second potential of the streaming smoother (k_rbgs_march), n >= MT_TK
     Lev lev() const { return Lev{n, dd, dp, dm, ip, im}; }
 };
 
@@ -81,6 +83,7 @@ struct kf_ctx {
     double *h_red = nullptr;
     int *d_sweeps = nullptr;
     unsigned long long *d_max = nullptr, *h_max = nullptr;
+    int *d_err = nullptr, *h_err = nullptr;  // kernel error word (bit 0: a bounded copy wait gave up)
     // RK4 time (Runge_kutta_O4::t_) and the phi history for extrapolated starts
     double t = 0., t_stage = 0.;
     double *phi_a = nullptr;
@@ -131,7 +134,8 @@ struct kf_ctx {
     OutState *out = nullptr;
     bool phi_given = false;
     int fftv = 0;     // radix-plan variant of the transform kernels (kf_autotune)
-    int rbgs_by = 8;  // rows per block of the red-black smoother (kf_autotune)
+    int rbgs_by = 0;  // smoother variant (kf_autotune): 0 streaming k_rbgs_march, else k_rbgs rows per block
+    bool march_maps = false;  // the driver's tensor-map encoder is available
     int stage_idx = 0;  // RK stage of the right-hand side being evaluated (0..3)
     // one RK4 step captured as a CUDA graph (FAS or no Poisson, profile off):
     // time / warm-start history and solve statistics live on the device
@@ -168,7 +172,7 @@ inline int nblk(long work, int bs) { return (int)((work + bs - 1) / bs); }
 // Kernel classes for the profile (kf_profile_read); names in kf_profile_class_name.
 enum KCls { KC_AXIS_INV, KC_AXIS_FWD, KC_Z_C2R, KC_Z_R2C, KC_XASM, KC_PROD, KC_LIN, KC_RHO, KC_RK,
             KC_JACOBI, KC_RBGS, KC_RESID, KC_TRANSFER, KC_COARSE, KC_REDUCE, KC_MISC, KC_ADJ_PW, KC_ADJ_MG,
-            KC_MG_COARSE,
+            KC_MG_COARSE, KC_MARCH, KC_MARCH_RES,
             KC_N };
 const char *const kKClsName[KC_N] = {"k_axis_pass(inverse)", "k_axis_pass(forward)", "k_z_c2r", "k_z_r2c",
                                      "k_xfwd_assemble", "k_products", "k_lin", "k_rho", "k_rk", "k_jacobi",
@@ -176,7 +180,8 @@ const char *const kKClsName[KC_N] = {"k_axis_pass(inverse)", "k_axis_pass(forwar
                                      "k_coarse_solve", "k_reduce_final", "conversion/diagnostics",
                                      "adjoint pointwise (k_prod_vjp/k_vjp_assemble/k_adj_stage/...)",
                                      "adjoint Poisson (linear multigrid)",
-                                     "FAS levels below the finest (k_rbgs/k_residual/transfers)"};
+                                     "FAS levels below the finest (k_rbgs/k_residual/transfers)",
+                                     "k_rbgs_march(sweep)", "k_rbgs_march(sweep+residual)"};
 
 void prof_flush(kf_ctx *c) {
     if (c->recs.empty()) return;
@@ -306,6 +311,19 @@ int red_blocks(long N) {
     return (int)(nb < 1184 ? nb : 1184);
 }
 
+// The kernel error word: queued for reading before a synchronisation
+// (kerr_fetch) and checked after it (kerr_check, which clears it)
+void kerr_fetch(kf_ctx *c) {
+    CK(cudaMemcpyAsync(c->h_err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+}
+void kerr_check(kf_ctx *c) {
+    if (*c->h_err) {
+        *c->h_err = 0;
+        CK(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st));
+        throw KfError{KF_ERR_CUDA, "a shared-memory copy of the multigrid smoother did not land within its wait limit"};
+    }
+}
+
 double max_residual(kf_ctx *c, const LevelBuf &L, const double *phi, const double *rho, bool fast) {
     const long N = (long)L.n * L.n * L.n;
     CK(cudaMemsetAsync(c->d_max, 0, 64 * sizeof(unsigned long long), c->st));
@@ -320,7 +338,9 @@ double max_residual(kf_ctx *c, const LevelBuf &L, const double *phi, const doubl
     }
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(c->h_max, c->d_max, 64 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->st));
+    kerr_fetch(c);
     CK(cudaStreamSynchronize(c->st));
+    kerr_check(c);
     unsigned long long m = 0;
     for (int s = 0; s < 64; ++s) m = c->h_max[s] > m ? c->h_max[s] : m;
     double r;
@@ -381,13 +401,97 @@ int jacobi_solve(kf_ctx *c, const LevelBuf &L, double *phi, double *tmp, const d
 // over-relaxation factor of the FAS smoother's Newton step (0 selects 1)
 double mg_omega(const kf_config &cf) { return cf.mg_omega > 0. ? cf.mg_omega : 1.; }
 
+// ------------------------------------------------------- streaming smoother
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library)
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return (EncodeTiledFn)p;
+    }();
+    return fn;
+}
+
+// Tensor map of an n^3 FP64 level whose copies are single rows of MT_PITCH
+// doubles (x = k fastest, then j, then i)
+bool row_map(CUtensorMap *m, const double *base, int n) {
+    const EncodeTiledFn f = encode_tiled();
+    if (!f) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)n, (cuuint64_t)n, (cuuint64_t)n};
+    const cuuint64_t strides[2] = {(cuuint64_t)n * 8, (cuuint64_t)n * n * 8};
+    const cuuint32_t box[3] = {MT_PITCH, 1, 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    return f(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void *)base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// planes per CTA of the streaming smoother: at least three waves of CTAs at
+// 256^3 (128 tiles x 8 chunks), the ghost planes (2 H per chunk) small
+int march_ci(int n) { return n >= 256 ? 32 : (n >= 128 ? 16 : 8); }
+constexpr int MT_TJ = 8;
+
+bool march_level(const LevelBuf &L) { return L.n >= MT_TK && L.n % MT_TK == 0 && L.n % MT_TJ == 0; }
+
+bool march_ok(const kf_ctx *c, const LevelBuf &L) { return c->rbgs_by == 0 && c->march_maps && L.t && march_level(L); }
+
+void march_attrs() {
+    CK(cudaFuncSetAttribute(k_rbgs_march<MM_RES, MT_TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)march_smem<MM_RES, MT_TJ>(32)));
+    CK(cudaFuncSetAttribute(k_rbgs_march<MM_SWEEP, MT_TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)march_smem<MM_SWEEP, MT_TJ>(32)));
+    CK(cudaFuncSetAttribute(k_rbgs_march<MM_SWEEP_RES, MT_TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)march_smem<MM_SWEEP_RES, MT_TJ>(32)));
+}
+
+// One streaming pass on level L: src -> dst (a whole red-black sweep) and/or
+// the residual r of the result, max |r| into `slots` when given.
+template <int MODE>
+void march(kf_ctx *c, const LevelBuf &L, const double *src, const double *rho, double *dst, double *r,
+           unsigned long long *slots, int cls) {
+    const int n = L.n, ci = march_ci(n);
+    CUtensorMap mp, mr;
+    if (!row_map(&mp, src, n) || !row_map(&mr, rho, n))
+        throw KfError{KF_ERR_CUDA, "cuTensorMapEncodeTiled refused a multigrid level"};
+    MarchArgs a{dst, r, src, rho, L.dd, L.ip, L.im, slots, c->d_err, n, ci, n / MT_TK, mg_omega(c->cfg)};
+    const dim3 g((n / MT_TK) * (n / MT_TJ), n / ci);
+    const long N = (long)n * n * n;
+    Launch L_(c, cls, (MODE == MM_SWEEP_RES ? 32. : 24.) * N);
+    k_rbgs_march<MODE, MT_TJ><<<g, MT_THREADS, march_smem<MODE, MT_TJ>(ci), c->st>>>(mp, mr, a);
+}
+
 // `sweeps` red-black Gauss-Seidel sweeps on level L (phi in place), two
 // half-sweep launches each.  cc: the adjoint's e^phi (linear point solve) or
 // nullptr (Newton step).
+void smooth_plain(kf_ctx *c, LevelBuf &L, double *phi, const double *rho, const double *cc, int sweeps, int cls);
+
 void smooth(kf_ctx *c, LevelBuf &L, double *phi, const double *rho, const double *cc, int sweeps, int cls) {
+    if (!cc && march_ok(c, L) && phi != L.t) {
+        // streaming passes phi -> t -> phi; an odd sweep first in place
+        if (sweeps & 1) smooth_plain(c, L, phi, rho, nullptr, 1, cls);
+        const int mc = cls == KC_RBGS ? KC_MARCH : cls;
+        for (int s = 0; s + 1 < sweeps; s += 2) {
+            march<MM_SWEEP>(c, L, phi, rho, L.t, nullptr, nullptr, mc);
+            march<MM_SWEEP>(c, L, L.t, rho, phi, nullptr, nullptr, mc);
+        }
+        return;
+    }
+    smooth_plain(c, L, phi, rho, cc, sweeps, cls);
+}
+
+// `sweeps` red-black sweeps as two half-sweep launches each (k_rbgs, or
+// k_rbgs_lin with the adjoint's e^phi)
+void smooth_plain(kf_ctx *c, LevelBuf &L, double *phi, const double *rho, const double *cc, int sweeps, int cls) {
     const int n = L.n;
     const long N = (long)n * n * n;
-    const int by = c->rbgs_by;
+    const int by = c->rbgs_by ? c->rbgs_by : 8;
     const double om = mg_omega(c->cfg);
     const dim3 g((n / 2 + 31) / 32, (n + by - 1) / by, n), b(32, by);
     for (int s = 0; s < sweeps; ++s)
@@ -420,6 +524,29 @@ void vcycle_head(kf_ctx *c, int l, bool with_max) {
     const kf_config &cf = c->cfg;
     const int n = L.n;
     const long N = (long)n * n * n;
+    if (march_ok(c, L) && cf.mg_pre >= 1) {
+        // the last pre-smoothing sweep fused with the residual (and its max):
+        // the sweeps before it leave the potential in L.t
+        int s = cf.mg_pre - 1;
+        const int cls = l == 0 ? KC_MARCH : KC_MG_COARSE;
+        if (s > 0 && s % 2 == 0) {
+            smooth_plain(c, L, L.phi, L.rho, nullptr, 1, l == 0 ? KC_RBGS : KC_MG_COARSE);
+            --s;
+        }
+        if (s == 0) {
+            CK(cudaMemcpyAsync(L.t, L.phi, 8 * (size_t)N, cudaMemcpyDeviceToDevice, c->st));
+        } else {
+            march<MM_SWEEP>(c, L, L.phi, L.rho, L.t, nullptr, nullptr, cls);
+            for (; s > 1; s -= 2) {
+                march<MM_SWEEP>(c, L, L.t, L.rho, L.phi, nullptr, nullptr, cls);
+                march<MM_SWEEP>(c, L, L.phi, L.rho, L.t, nullptr, nullptr, cls);
+            }
+        }
+        if (with_max) CK(cudaMemsetAsync(c->d_max, 0, 64 * sizeof(unsigned long long), c->st));
+        march<MM_SWEEP_RES>(c, L, L.t, L.rho, L.phi, L.r, with_max ? c->d_max : nullptr,
+                            l == 0 ? KC_MARCH_RES : KC_MG_COARSE);
+        return;
+    }
     smooth(c, L, L.phi, L.rho, nullptr, cf.mg_pre, l == 0 ? KC_RBGS : KC_MG_COARSE);
     if (with_max) CK(cudaMemsetAsync(c->d_max, 0, 64 * sizeof(unsigned long long), c->st));
     Launch L_(c, l == 0 ? KC_RESID : KC_MG_COARSE, 24. * N);
@@ -527,7 +654,9 @@ void run_vcycle_tail(kf_ctx *c) {
 // max over the 64 d_max slots (IEEE bit patterns of non-negative doubles)
 double read_max_slots(kf_ctx *c) {
     CK(cudaMemcpyAsync(c->h_max, c->d_max, 64 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->st));
+    kerr_fetch(c);
     CK(cudaStreamSynchronize(c->st));
+    kerr_check(c);
     unsigned long long m = 0;
     for (int s = 0; s < 64; ++s) m = c->h_max[s] > m ? c->h_max[s] : m;
     double r;
@@ -1362,6 +1491,8 @@ void build_levels(kf_ctx *c) {
     if (cf.poisson_mode == KF_PS_FAS && ((long)(c->n >> (nl - 1)) * (c->n >> (nl - 1)) * (c->n >> (nl - 1)) > 8192))
         throw KfError{KF_ERR_ARG, "coarsest FAS level above 8192 points (shared-memory solve); add levels"};
     CK(cudaFuncSetAttribute(k_coarse_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    march_attrs();
+    c->march_maps = encode_tiled() != nullptr;  // before the levels: L.t depends on it
     c->lv.resize(nl);
     for (int l = 0; l < nl; ++l) {
         LevelBuf &L = c->lv[l];
@@ -1396,6 +1527,11 @@ void build_levels(kf_ctx *c) {
         CK(cudaMemcpy(L.gam, gam.data(), 8 * n, cudaMemcpyHostToDevice));
         const size_t bytes = sizeof(double) * (size_t)n * n * n;
         L.r = dalloc<double>(c, bytes);
+        if (cf.poisson_mode == KF_PS_FAS && march_level(L) && c->march_maps) {
+            L.t = dalloc<double>(c, bytes);
+            CUtensorMap probe;  // the encoder must accept this level's row copies
+            if (!row_map(&probe, L.t, n)) L.t = nullptr;
+        }
         if (l == 0) {
             L.phi = c->phi;
             L.rho = c->rho;
@@ -1620,6 +1756,9 @@ void create(kf_ctx *c) {
     c->partial = dalloc<double>(c, sizeof(double) * KF_RED * c->npartial);
     c->red = dalloc<double>(c, sizeof(double) * 8);
     c->d_sweeps = dalloc<int>(c, sizeof(int) * 4);
+    c->d_err = dalloc<int>(c, sizeof(int));
+    CK(cudaMemset(c->d_err, 0, sizeof(int)));
+    CK(cudaMallocHost(&c->h_err, sizeof(int)));
     c->d_max = dalloc<unsigned long long>(c, 64 * sizeof(unsigned long long));
     CK(cudaMallocHost(&c->h_max, 64 * sizeof(unsigned long long)));
     if (cf.phi_extrap) c->phi_a = dalloc<double>(c, 8 * c->N);
@@ -1799,7 +1938,9 @@ void graph_end(kf_ctx *c) {
     DevPois hp;
     CK(cudaMemcpyAsync(&ht, c->dtime, sizeof(DevTime), cudaMemcpyDeviceToHost, c->st));
     CK(cudaMemcpyAsync(&hp, c->dpois, sizeof(DevPois), cudaMemcpyDeviceToHost, c->st));
+    kerr_fetch(c);
     CK(cudaStreamSynchronize(c->st));
+    kerr_check(c);
     c->t = ht.t;
     c->t_stage = ht.t_stage;
     c->tau_a = ht.tau_a;
@@ -1955,7 +2096,8 @@ void autotune(kf_ctx *c, int reps, kf_tune_out *o) {
     c->stage_idx = si;
     r.fft_plan = r.fft_ms[1] < r.fft_ms[0] ? 1 : 0;
     // smoother shapes: sweeps of a copy of the finest-level potential
-    const int rows[3] = {4, 8, 16};
+    // (rows 0: the streaming k_rbgs_march where the level allows it)
+    const int rows[4] = {4, 8, 16, 0};
     r.rbgs_rows = by;
     if (c->rho && !c->lv.empty()) {
         LevelBuf &L0 = c->lv[0];
@@ -1964,9 +2106,14 @@ void autotune(kf_ctx *c, int reps, kf_tune_out *o) {
         try {
             CK(cudaMemcpyAsync(tmp, c->phi, 8 * (size_t)c->N, cudaMemcpyDeviceToDevice, c->st));
             int best = -1;
-            for (int k = 0; k < 3; ++k) {
+            for (int k = 0; k < 4; ++k) {
                 c->rbgs_by = rows[k];
-                r.rbgs_ms[k] = time_candidate(c, reps, [&] { smooth(c, L0, tmp, c->rho, nullptr, 1, KC_RBGS); });
+                if (rows[k] == 0 && !march_ok(c, L0)) {
+                    r.rbgs_ms[k] = -1.;
+                    continue;
+                }
+                r.rbgs_ms[k] =
+                    0.5 * time_candidate(c, reps, [&] { smooth(c, L0, tmp, c->rho, nullptr, 2, KC_RBGS); });
                 if (best < 0 || r.rbgs_ms[k] < r.rbgs_ms[best]) best = k;
             }
             r.rbgs_rows = rows[best];
@@ -2032,6 +2179,7 @@ int kf_ctx_destroy(kf_ctx *c) {
     for (void *p : c->allocs) cudaFree(p);
     if (c->h_red) cudaFreeHost(c->h_red);
     if (c->h_max) cudaFreeHost(c->h_max);
+    if (c->h_err) cudaFreeHost(c->h_err);
     if (c->st && c->own_stream) cudaStreamDestroy(c->st);
     delete c;
     return KF_OK;
@@ -2149,8 +2297,9 @@ int kf_autotune(kf_ctx *c, int reps, kf_tune_out *out) {
 
 int kf_set_tuning(kf_ctx *c, int fft_plan, int rbgs_rows) {
     return guarded(c, [&] {
-        if ((fft_plan != 0 && fft_plan != 1) || (rbgs_rows != 4 && rbgs_rows != 8 && rbgs_rows != 16))
-            throw KfError{KF_ERR_ARG, "kf_set_tuning: fft_plan 0 or 1, rbgs_rows 4, 8 or 16"};
+        if ((fft_plan != 0 && fft_plan != 1) ||
+            (rbgs_rows != 0 && rbgs_rows != 4 && rbgs_rows != 8 && rbgs_rows != 16))
+            throw KfError{KF_ERR_ARG, "kf_set_tuning: fft_plan 0 or 1, rbgs_rows 0, 4, 8 or 16"};
         if (c->capturing) throw KfError{KF_ERR_ARG, "kf_set_tuning during a capture"};
         const bool changed = fft_plan != c->fftv || rbgs_rows != c->rbgs_by;
         c->fftv = fft_plan;

@@ -17,10 +17,21 @@
 // and must be serialised by the caller.  Each call writes every scratch entry
 // it reads before reading it, so nothing has to start at zero.
 //
-// Set-up: the first call on each device looks up the array's device address
-// with cudaGetSymbolAddress (the array's name is only a host-side stand-in;
-// handing it to a kernel would fault or silently use the wrong memory).  That
-// first call on a device should therefore be made before any stream capture.
+// Set-up: each call outside a stream capture looks up the array's device
+// address with cudaGetSymbolAddress (the array's name is only a host-side
+// stand-in; handing it to a kernel would fault or silently use the wrong
+// memory) and remembers it per device; a call made while its stream is being
+// captured uses the remembered address.  Looking it up again on every
+// uncaptured call keeps the address right after a cudaDeviceReset, which
+// reloads the module (possibly elsewhere).  With lazy module loading (the CUDA
+// default since 12.2) the first call on a device also loads this module,
+// which places the static array in device memory and synchronises: that first
+// call is a warm-up, to be made before the allocation-free part of the
+// program and before any stream capture.
+//
+// An asynchronous error that is already pending when a call starts (from
+// earlier, unrelated work) is reported as such and left pending; the call's
+// own launch errors are reported as its own.
 #include <cmath>
 #include <mutex>
 #include <string>
@@ -113,10 +124,21 @@ extern "C" int kf_fft_r2c_noalloc(int n, const double *in_real, double *out_comp
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return fail(KF_ERR_NO_DEVICE, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
     if (dev < 0 || dev >= 64) return fail(KF_ERR_ARG, "kf_fft_r2c_noalloc: device ordinal above 63");
+    cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+    e = cudaPeekAtLastError();
+    if (e != cudaSuccess)
+        return fail(KF_ERR_CUDA, std::string("kf_fft_r2c_noalloc: an earlier CUDA error is pending (not cleared): ") +
+                                     cudaGetErrorString(e));
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(st, &cap);
+    if (e != cudaSuccess) return fail(KF_ERR_CUDA, std::string("cudaStreamIsCapturing: ") + cudaGetErrorString(e));
     unsigned char *scratch;
     {
         std::lock_guard<std::mutex> lk(g_mu);
-        if (!g_scratch[dev]) {
+        if (cap == cudaStreamCaptureStatusNone || !g_scratch[dev]) {
+            if (cap != cudaStreamCaptureStatusNone)
+                return fail(KF_ERR_ARG, "kf_fft_r2c_noalloc: the first call on a device must not be captured "
+                                        "(it looks up the static array's address)");
             void *ptr = nullptr;
             e = cudaGetSymbolAddress(&ptr, kf_noalloc_scratch);
             if (e != cudaSuccess)
@@ -125,7 +147,6 @@ extern "C" int kf_fft_r2c_noalloc(int n, const double *in_real, double *out_comp
         }
         scratch = g_scratch[dev];
     }
-    cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
     e = n == 16 ? run<16>(in_real, out_complex, scratch, st)
       : n == 32 ? run<32>(in_real, out_complex, scratch, st)
                 : run<64>(in_real, out_complex, scratch, st);

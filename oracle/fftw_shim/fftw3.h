@@ -53,6 +53,18 @@ void kfs_r2c_3d(int n0, int n1, int n2, const double *in, double *out_interleave
 void kfs_c2r_3d(int n0, int n1, int n2, const double *in_interleaved, double *out);
 void kfs_fft_1d(int n, int sign, double *data_interleaved);
 
+/* Runs fn(begin, end, ctx) over contiguous pieces of [0, n) on the host's
+ * cores (threads only when built with KFS_THREADS, the oracle's build; the
+ * reference's build stays single-threaded, as FFTW_ESTIMATE plans without
+ * fftw_plan_with_nthreads are).  Pieces of fewer than min_items items are not
+ * split off.  Callers give each item work whose result does not depend on the
+ * other items, so the number of threads changes no result. */
+typedef void (*kfs_range_fn)(long begin, long end, void *ctx);
+void kfs_parallel(long n, long min_items, kfs_range_fn fn, void *ctx);
+/* threads kfs_parallel uses: KF_ORACLE_THREADS, else the online cores (1
+ * without KFS_THREADS) */
+int kfs_nthreads(void);
+
 #ifdef __cplusplus
 }
 #endif

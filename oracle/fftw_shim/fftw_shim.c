@@ -24,6 +24,66 @@
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+#ifdef KFS_THREADS
+#include <pthread.h>
+#include <unistd.h>
+#endif
+
+/* ------------------------------------------------------------ host threads */
+int kfs_nthreads(void) {
+#ifdef KFS_THREADS
+    static int nt = 0;
+    if (!nt) {
+        const char *e = getenv("KF_ORACLE_THREADS");
+        long v = e ? strtol(e, NULL, 10) : sysconf(_SC_NPROCESSORS_ONLN);
+        nt = v < 1 ? 1 : (v > 256 ? 256 : (int)v);
+    }
+    return nt;
+#else
+    return 1;
+#endif
+}
+
+#ifdef KFS_THREADS
+typedef struct {
+    kfs_range_fn fn;
+    void *ctx;
+    long b, e;
+} kfs_piece;
+
+static void *kfs_piece_run(void *a) {
+    kfs_piece *p = (kfs_piece *)a;
+    p->fn(p->b, p->e, p->ctx);
+    return NULL;
+}
+#endif
+
+void kfs_parallel(long n, long min_items, kfs_range_fn fn, void *ctx) {
+    if (n <= 0) return;
+    long T = kfs_nthreads();
+    if (min_items < 1) min_items = 1;
+    if (T > n / min_items) T = n / min_items;
+#ifdef KFS_THREADS
+    if (T > 1) {
+        pthread_t th[256];
+        kfs_piece pc[256];
+        int started[256];
+        for (long t = 0; t < T; ++t) {
+            pc[t].fn = fn;
+            pc[t].ctx = ctx;
+            pc[t].b = n * t / T;
+            pc[t].e = n * (t + 1) / T;
+            started[t] = t > 0 && pthread_create(&th[t], NULL, kfs_piece_run, &pc[t]) == 0;
+        }
+        for (long t = 0; t < T; ++t)
+            if (!started[t]) kfs_piece_run(&pc[t]); /* piece 0, or a thread that could not start */
+        for (long t = 1; t < T; ++t)
+            if (started[t]) pthread_join(th[t], NULL);
+        return;
+    }
+#endif
+    fn(0, n, ctx);
+}
 
 #define KFS_MAXF 40
 
@@ -138,46 +198,73 @@ static void kfs_exec1d(const kfs_plan1d *p, int B, int sign, double *buf, double
 /* Complex FFT along a strided axis of an interleaved complex array:
  * lines are data[off + t*stride] for t < n, with the line start offsets
  * given by  outer * ostride + c  for outer < nouter, c < ninner (contiguous). */
-static void kfs_axis_pass(const kfs_plan1d *p, double *data, int nouter, size_t ostride,
-                          int ninner, size_t stride, int sign) {
-    const int n = p->n;
+typedef struct {
+    const kfs_plan1d *p;
+    double *data;
+    long nblk;
+    size_t ostride, stride;
+    int ninner, sign;
+} kfs_axis_job;
+
+/* line blocks [b, e) of an axis pass; scratch per piece */
+static void kfs_axis_range(long b, long e, void *ctx) {
+    const kfs_axis_job *J = (const kfs_axis_job *)ctx;
+    const int n = J->p->n;
     double *buf = (double *)malloc(sizeof(double) * 2 * (size_t)n * KFS_B);
     double *scr = (double *)malloc(sizeof(double) * 2 * (size_t)n * KFS_B);
-    for (int o = 0; o < nouter; ++o) {
-        for (int c0 = 0; c0 < ninner; c0 += KFS_B) {
-            int B = ninner - c0 < KFS_B ? ninner - c0 : KFS_B;
-            for (int t = 0; t < n; ++t) {
-                const double *src = data + 2 * (o * ostride + (size_t)t * stride + c0);
-                memcpy(buf + 2 * (size_t)t * B, src, sizeof(double) * 2 * B);
-            }
-            kfs_exec1d(p, B, sign, buf, scr);
-            for (int t = 0; t < n; ++t) {
-                double *dst = data + 2 * (o * ostride + (size_t)t * stride + c0);
-                memcpy(dst, buf + 2 * (size_t)t * B, sizeof(double) * 2 * B);
-            }
+    for (long w = b; w < e; ++w) {
+        const int o = (int)(w / J->nblk), c0 = (int)(w % J->nblk) * KFS_B;
+        int B = J->ninner - c0 < KFS_B ? J->ninner - c0 : KFS_B;
+        for (int t = 0; t < n; ++t) {
+            const double *src = J->data + 2 * (o * J->ostride + (size_t)t * J->stride + c0);
+            memcpy(buf + 2 * (size_t)t * B, src, sizeof(double) * 2 * B);
+        }
+        kfs_exec1d(J->p, B, J->sign, buf, scr);
+        for (int t = 0; t < n; ++t) {
+            double *dst = J->data + 2 * (o * J->ostride + (size_t)t * J->stride + c0);
+            memcpy(dst, buf + 2 * (size_t)t * B, sizeof(double) * 2 * B);
         }
     }
     free(buf);
     free(scr);
 }
 
-void kfs_r2c_3d(int n0, int n1, int n2, const double *in, double *out) {
-    const int nzc = n2 / 2 + 1;
-    const size_t rows = (size_t)n0 * n1;
-    kfs_plan1d pz, py, px;
-    kfs_plan1d_init(&pz, n2);
+/* Complex FFT along a strided axis of an interleaved complex array:
+ * lines are data[off + t*stride] for t < n, with the line start offsets
+ * given by  outer * ostride + c  for outer < nouter, c < ninner (contiguous).
+ * Blocks of KFS_B lines are independent, and a line's arithmetic does not
+ * depend on its block. */
+static void kfs_axis_pass(const kfs_plan1d *p, double *data, int nouter, size_t ostride,
+                          int ninner, size_t stride, int sign) {
+    kfs_axis_job J = {p, data, (ninner + KFS_B - 1) / KFS_B, ostride, stride, ninner, sign};
+    kfs_parallel((long)nouter * J.nblk, 4, kfs_axis_range, &J);
+}
+
+typedef struct {
+    const kfs_plan1d *p;
+    const double *in;
+    double *out;
+    size_t rows;
+    int n2, nzc;
+} kfs_z_job;
+
+/* z pass of an r2c: row pairs [b, e) packed as one complex line each */
+static void kfs_r2c_z_range(long b, long e, void *ctx) {
+    const kfs_z_job *J = (const kfs_z_job *)ctx;
+    const int n2 = J->n2, nzc = J->nzc;
     double *z = (double *)malloc(sizeof(double) * 2 * n2);
     double *s = (double *)malloc(sizeof(double) * 2 * n2);
-    for (size_t r = 0; r < rows; r += 2) {
-        const double *a = in + r * n2;
-        const double *b = (r + 1 < rows) ? in + (r + 1) * n2 : NULL;
+    for (long r2 = b; r2 < e; ++r2) {
+        const size_t r = 2 * (size_t)r2;
+        const double *a = J->in + r * n2;
+        const double *bb = (r + 1 < J->rows) ? J->in + (r + 1) * n2 : NULL;
         for (int t = 0; t < n2; ++t) {
             z[2 * t] = a[t];
-            z[2 * t + 1] = b ? b[t] : 0.0;
+            z[2 * t + 1] = bb ? bb[t] : 0.0;
         }
-        kfs_exec1d(&pz, 1, -1, z, s);
-        double *oa = out + 2 * r * nzc;
-        double *ob = b ? out + 2 * (r + 1) * nzc : NULL;
+        kfs_exec1d(J->p, 1, -1, z, s);
+        double *oa = J->out + 2 * r * nzc;
+        double *ob = bb ? J->out + 2 * (r + 1) * nzc : NULL;
         for (int k = 0; k < nzc; ++k) {
             int km = (n2 - k) % n2;
             double zr = z[2 * k], zi = z[2 * k + 1];
@@ -192,6 +279,15 @@ void kfs_r2c_3d(int n0, int n1, int n2, const double *in, double *out) {
     }
     free(z);
     free(s);
+}
+
+void kfs_r2c_3d(int n0, int n1, int n2, const double *in, double *out) {
+    const int nzc = n2 / 2 + 1;
+    const size_t rows = (size_t)n0 * n1;
+    kfs_plan1d pz, py, px;
+    kfs_plan1d_init(&pz, n2);
+    kfs_z_job J = {&pz, in, out, rows, n2, nzc};
+    kfs_parallel((long)((rows + 1) / 2), 8, kfs_r2c_z_range, &J);
     kfs_plan1d_free(&pz);
     kfs_plan1d_init(&py, n1);
     kfs_axis_pass(&py, out, n0, (size_t)n1 * nzc, nzc, (size_t)nzc, -1);
@@ -201,24 +297,16 @@ void kfs_r2c_3d(int n0, int n1, int n2, const double *in, double *out) {
     kfs_plan1d_free(&px);
 }
 
-void kfs_c2r_3d(int n0, int n1, int n2, const double *in, double *out) {
-    const int nzc = n2 / 2 + 1;
-    const size_t rows = (size_t)n0 * n1;
-    double *w = (double *)malloc(sizeof(double) * 2 * rows * nzc);
-    memcpy(w, in, sizeof(double) * 2 * rows * nzc);
-    kfs_plan1d px, py, pz;
-    kfs_plan1d_init(&px, n0);
-    kfs_axis_pass(&px, w, 1, 0, n1 * nzc, (size_t)n1 * nzc, +1);
-    kfs_plan1d_free(&px);
-    kfs_plan1d_init(&py, n1);
-    kfs_axis_pass(&py, w, n0, (size_t)n1 * nzc, nzc, (size_t)nzc, +1);
-    kfs_plan1d_free(&py);
-    kfs_plan1d_init(&pz, n2);
+/* z pass of a c2r: row pairs [b, e) from the Hermitian half spectra */
+static void kfs_c2r_z_range(long b, long e, void *ctx) {
+    const kfs_z_job *J = (const kfs_z_job *)ctx;
+    const int n2 = J->n2, nzc = J->nzc;
     double *z = (double *)malloc(sizeof(double) * 2 * n2);
     double *s = (double *)malloc(sizeof(double) * 2 * n2);
-    for (size_t r = 0; r < rows; r += 2) {
-        const double *A = w + 2 * r * nzc;
-        const double *Bv = (r + 1 < rows) ? w + 2 * (r + 1) * nzc : NULL;
+    for (long r2 = b; r2 < e; ++r2) {
+        const size_t r = 2 * (size_t)r2;
+        const double *A = J->in + 2 * r * nzc;
+        const double *Bv = (r + 1 < J->rows) ? J->in + 2 * (r + 1) * nzc : NULL;
         for (int k = 0; k < n2; ++k) {
             double ar, ai, br = 0.0, bi = 0.0;
             if (k < nzc) {
@@ -236,9 +324,9 @@ void kfs_c2r_3d(int n0, int n1, int n2, const double *in, double *out) {
             z[2 * k] = ar - bi;
             z[2 * k + 1] = ai + br;
         }
-        kfs_exec1d(&pz, 1, +1, z, s);
-        double *oa = out + r * n2;
-        double *ob = Bv ? out + (r + 1) * n2 : NULL;
+        kfs_exec1d(J->p, 1, +1, z, s);
+        double *oa = J->out + r * n2;
+        double *ob = Bv ? J->out + (r + 1) * n2 : NULL;
         for (int t = 0; t < n2; ++t) {
             oa[t] = z[2 * t];
             if (ob) ob[t] = z[2 * t + 1];
@@ -246,6 +334,23 @@ void kfs_c2r_3d(int n0, int n1, int n2, const double *in, double *out) {
     }
     free(z);
     free(s);
+}
+
+void kfs_c2r_3d(int n0, int n1, int n2, const double *in, double *out) {
+    const int nzc = n2 / 2 + 1;
+    const size_t rows = (size_t)n0 * n1;
+    double *w = (double *)malloc(sizeof(double) * 2 * rows * nzc);
+    memcpy(w, in, sizeof(double) * 2 * rows * nzc);
+    kfs_plan1d px, py, pz;
+    kfs_plan1d_init(&px, n0);
+    kfs_axis_pass(&px, w, 1, 0, n1 * nzc, (size_t)n1 * nzc, +1);
+    kfs_plan1d_free(&px);
+    kfs_plan1d_init(&py, n1);
+    kfs_axis_pass(&py, w, n0, (size_t)n1 * nzc, nzc, (size_t)nzc, +1);
+    kfs_plan1d_free(&py);
+    kfs_plan1d_init(&pz, n2);
+    kfs_z_job J = {&pz, w, out, rows, n2, nzc};
+    kfs_parallel((long)((rows + 1) / 2), 8, kfs_c2r_z_range, &J);
     kfs_plan1d_free(&pz);
     free(w);
 }

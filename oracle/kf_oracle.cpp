@@ -38,6 +38,21 @@ namespace {
 
 typedef std::vector<double> vec;
 
+/* f(i) for i in [0, n) on the host's cores (kfs_parallel): every use below
+ * gives each i work whose result does not depend on any other i (pointwise
+ * passes, independent transform lines, the points of one red-black colour,
+ * per-plane partial maxima), so the threads change no result; the sums whose
+ * order matters (the Jacobi sweep's statistics) stay sequential. */
+template <class F> void par_for(long n, long min_items, const F &f) {
+    kfs_parallel(
+        n, min_items,
+        [](long b, long e, void *ctx) {
+            const F &g = *static_cast<const F *>(ctx);
+            for (long i = b; i < e; ++i) g(i);
+        },
+        (void *)&f);
+}
+
 /* axis_CoEqSt (axis_EqSt.cpp:52-61) and, with m > 0, axis_CoSiSt: the
  * periodic sine-stretched axis x = S(l0 + L i/N), S(x) = x - m sin(2 pi x/L)
  * (axis_SiSt.cpp:93-116 val_at, :153-164 S and dS; k_val_at :120-124 is the
@@ -209,15 +224,15 @@ void c2r(const kfo_ctx *c, const vec &in, vec &out) {
     out.resize(c->N);
     kfs_c2r_3d(c->n, c->n, c->n, in.data(), out.data());
     double Norm = 1. / ((double)c->N);
-    for (size_t i = 0; i < c->N; ++i) out[i] = out[i] * Norm;
+    par_for((long)(c->N), 16384, [&](long i) { out[i] = out[i] * Norm; });
 }
 
 /* OP_dealiasing::operator() (OP_dealiasing.cpp:5-13) */
 void dealias(const kfo_ctx *c, vec &F) {
-    for (size_t i = 0; i < c->Nc; ++i) {
+    par_for((long)c->Nc, 16384, [&](long i) {
         F[2 * i] *= c->P[i];
         F[2 * i + 1] *= c->P[i];
-    }
+    });
 }
 
 /* effect_penalization::execute (effect_penalization.cpp:21-44), masking form,
@@ -226,8 +241,8 @@ void dealias(const kfo_ctx *c, vec &F) {
  * (the reference forms it as iFFT of its `in`); b: scratch */
 void penalize(const kfo_ctx *c, const vec &q, double fix, vec &out, vec &b) {
     c2r(c, out, b);
-    for (size_t i = 0; i < c->N; ++i)
-        b[i] = (1. - c->mask[i]) * b[i] + c->mask[i] * c->cfg.pen_eta * (q[i] - fix);
+    par_for((long)c->N, 16384,
+            [&](long i) { b[i] = (1. - c->mask[i]) * b[i] + c->mask[i] * c->cfg.pen_eta * (q[i] - fix); });
     r2c(c, b, out);
 }
 
@@ -237,27 +252,28 @@ void penalize(const kfo_ctx *c, const vec &q, double fix, vec &out, vec &b) {
 void deriv(const kfo_ctx *c, int dir, const vec &in, vec &out) {
     out.resize(2 * c->Nc);
     const int n = c->n, nzc = c->nzc;
-    for (int i = 0; i < n; ++i)
+    par_for(n, 1, [&](long i) {
         for (int j = 0; j < n; ++j)
             for (int k = 0; k < nzc; ++k) {
                 size_t ijk = (size_t)k + nzc * ((size_t)j + (size_t)i * n);
-                int q = dir == 0 ? i : (dir == 1 ? j : k);
+                int q = dir == 0 ? (int)i : (dir == 1 ? j : k);
                 double kk = c->kv[q];
                 double tmp = in[2 * ijk];
                 out[2 * ijk] = -kk * in[2 * ijk + 1];
                 out[2 * ijk + 1] = kk * tmp;
             }
+    });
     if (!c->stretched) return;
     dealias(c, out);
     vec t;
     c2r(c, out, t);
     const vec &d = c->dsv[dir];
-    for (size_t i = 0; i < c->N; ++i) t[i] = t[i] * d[i];
+    par_for((long)(c->N), 16384, [&](long i) { t[i] = t[i] * d[i]; });
     r2c(c, t, out);
 }
 
 void add(vec &a, const vec &b) {
-    for (size_t i = 0; i < a.size(); ++i) a[i] += b[i];
+    par_for((long)(a.size()), 16384, [&](long i) { a[i] += b[i]; });
 }
 
 /* ------------------------------------------------------------ Poisson solvers */
@@ -275,22 +291,33 @@ double jacobi_sweep(kfo_ctx *c, const level &L, const vec &in, vec &out, const v
     c->infinum = in[0];
     double rmax = 0.;
     const int n = L.n;
-    for (int i = 0; i < n; ++i)
+    const size_t N = (size_t)n * n * n;
+    /* the point updates on the host's cores; the statistics in the
+     * reference's point order (its sums are order dependent) */
+    vec pnew(N), f0a(N);
+    const double om = c->omega_SOR;
+    par_for(n, 1, [&](long i) {
         for (int j = 0; j < n; ++j)
             for (int k = 0; k < n; ++k) {
                 double A, D;
-                L.coeffs(in.data(), rho.data(), i, j, k, A, D);
-                double P_old = in[L.idx(i, j, k)];
-                double f0 = A - D * P_old - exp(P_old);
-                if (fabs(f0) > rmax) rmax = fabs(f0);
+                L.coeffs(in.data(), rho.data(), (int)i, j, k, A, D);
+                const size_t q = L.idx((int)i, j, k);
+                double P_old = in[q];
+                f0a[q] = A - D * P_old - exp(P_old);
                 double P_new = newton_point(P_old, A, D);
-                double delta = fabs(P_new - P_old);
-                out[L.idx(i, j, k)] = (1. - c->omega_SOR) * P_old + c->omega_SOR * P_new;
-                c->supremum = (P_new < c->supremum) ? c->supremum : P_new; /* max<double> (o_math.hpp) */
-                c->infinum = !(P_new < c->infinum) ? c->infinum : P_new;   /* min<double> (o_math.hpp) */
-                c->norm_max = (delta < c->norm_max) ? c->norm_max : delta;
-                c->norm_sum += delta;
+                pnew[q] = P_new;
+                out[q] = (1. - om) * P_old + om * P_new;
             }
+    });
+    for (size_t q = 0; q < N; ++q) {
+        const double f0 = f0a[q], P_new = pnew[q];
+        if (fabs(f0) > rmax) rmax = fabs(f0);
+        double delta = fabs(P_new - in[q]);
+        c->supremum = (P_new < c->supremum) ? c->supremum : P_new; /* max<double> (o_math.hpp) */
+        c->infinum = !(P_new < c->infinum) ? c->infinum : P_new;   /* min<double> (o_math.hpp) */
+        c->norm_max = (delta < c->norm_max) ? c->norm_max : delta;
+        c->norm_sum += delta;
+    }
     /* Carre's SOR factor (:237-252) */
     c->norm_sum = c->norm_sum / ((double)L.n * L.n * L.n);
     if ((c->norm_max < c->norm_max_old) && (iteration > 1)) {
@@ -341,11 +368,12 @@ int jacobi_solve(kfo_ctx *c, const level &L, vec &phi, const vec &rho, int &max_
 void inject(int nf, int step, const vec &in, vec &out) {
     int nc = nf / step;
     out.assign((size_t)nc * nc * nc, 0.);
-    for (int i = 0; i < nc; ++i)
+    par_for(nc, 1, [&](long i) {
         for (int j = 0; j < nc; ++j)
             for (int k = 0; k < nc; ++k)
                 out[(size_t)k + nc * ((size_t)j + (size_t)i * nc)] =
                     in[(size_t)(step * k) + nf * ((size_t)(step * j) + (size_t)(step * i) * nf)];
+    });
 }
 
 /* OP_hto2h: trilinear prolongation in z, then y, then x passes
@@ -356,31 +384,38 @@ void prolong(int nc, double L, double m, const vec &in, vec &out) {
     out.assign((size_t)nf * nf * nf, 0.);
     auto id = [nf](int i, int j, int k) { return (size_t)k + nf * ((size_t)j + (size_t)i * nf); };
     auto w = [nf](int i) { return i < 0 ? i + nf : (i > nf - 1 ? i - nf : i); };
-    for (int i = 0; i < nc; i++)
+    /* each pass reads only points the earlier passes wrote */
+    par_for(nc, 1, [&](long i) {
         for (int j = 0; j < nc; j++)
             for (int k = 0; k < nc; k++)
-                out[id(2 * i, 2 * j, 2 * k)] = in[(size_t)k + nc * ((size_t)j + (size_t)i * nc)];
-    for (int i = 0; i < nf - 1; i += 2)
+                out[id(2 * (int)i, 2 * j, 2 * k)] = in[(size_t)k + nc * ((size_t)j + (size_t)i * nc)];
+    });
+    par_for(nf / 2, 1, [&](long ii) {
+        const int i = 2 * (int)ii;
         for (int j = 0; j < nf; j += 2)
             for (int k = 1; k < nf; k += 2) {
                 double z1 = ax.val_at(k - 1), z2 = ax.val_at(k + 1), z = ax.val_at(k);
                 double g = (z - z1) / (z2 - z1);
                 out[id(i, j, k)] = (1. - g) * out[id(i, j, w(k - 1))] + g * out[id(i, j, w(k + 1))];
             }
-    for (int i = 0; i < nf; i += 2)
+    });
+    par_for(nf / 2, 1, [&](long ii) {
+        const int i = 2 * (int)ii;
         for (int j = 1; j < nf; j += 2) {
             double y1 = ax.val_at(j - 1), y2 = ax.val_at(j + 1), y = ax.val_at(j);
             double g = (y - y1) / (y2 - y1);
             for (int k = 0; k < nf; k += 1)
                 out[id(i, j, k)] = (1. - g) * out[id(i, w(j - 1), k)] + g * out[id(i, w(j + 1), k)];
         }
-    for (int i = 1; i < nf; i += 2) {
+    });
+    par_for(nf / 2, 1, [&](long ii) {
+        const int i = 2 * (int)ii + 1;
         double x1 = ax.val_at(i - 1), x2 = ax.val_at(i + 1), x = ax.val_at(i);
         double g = (x - x1) / (x2 - x1);
         for (int j = 0; j < nf; j += 1)
             for (int k = 0; k < nf; k += 1)
                 out[id(i, j, k)] = (1. - g) * out[id(w(i - 1), j, k)] + g * out[id(w(i + 1), j, k)];
-    }
+    });
 }
 
 /* Full-weighting restriction n -> n/2 (new for the FAS cycle): tensor product of
@@ -389,7 +424,8 @@ void restrict_fw(int nf, const vec &in, vec &out) {
     int nc = nf / 2;
     out.assign((size_t)nc * nc * nc, 0.);
     const double w[3] = {0.25, 0.5, 0.25};
-    for (int i = 0; i < nc; ++i)
+    par_for(nc, 1, [&](long il) {
+        const int i = (int)il;
         for (int j = 0; j < nc; ++j)
             for (int k = 0; k < nc; ++k) {
                 double s = 0.;
@@ -409,27 +445,44 @@ void restrict_fw(int nf, const vec &in, vec &out) {
                 }
                 out[(size_t)k + nc * ((size_t)j + (size_t)i * nc)] = s;
             }
+    });
 }
 
 double max_resid(const level &L, const vec &phi, const vec &rho) {
-    double r = 0.;
-    for (int i = 0; i < L.n; ++i)
+    /* per-plane maxima, then their maximum: f > r never takes a NaN, and the
+     * maximum of the other values does not depend on the order */
+    vec rp(L.n, 0.);
+    par_for(L.n, 1, [&](long i) {
+        double r = 0.;
         for (int j = 0; j < L.n; ++j)
             for (int k = 0; k < L.n; ++k) {
-                double f = fabs(L.resid(phi.data(), rho.data(), i, j, k));
+                double f = fabs(L.resid(phi.data(), rho.data(), (int)i, j, k));
                 if (f > r) r = f;
             }
+        rp[i] = r;
+    });
+    double r = 0.;
+    for (double v : rp)
+        if (v > r) r = v;
     return r;
 }
 
 double max_resid_fast(const level &L, const vec &phi, const vec &rho) {
-    double r = 0.;
-    for (int i = 0; i < L.n; ++i)
+    /* per-plane maxima, then their maximum: f > r never takes a NaN, and the
+     * maximum of the other values does not depend on the order */
+    vec rp(L.n, 0.);
+    par_for(L.n, 1, [&](long i) {
+        double r = 0.;
         for (int j = 0; j < L.n; ++j)
             for (int k = 0; k < L.n; ++k) {
-                double f = fabs(L.resid_fast(phi.data(), rho.data(), i, j, k));
+                double f = fabs(L.resid_fast(phi.data(), rho.data(), (int)i, j, k));
                 if (f > r) r = f;
             }
+        rp[i] = r;
+    });
+    double r = 0.;
+    for (double v : rp)
+        if (v > r) r = v;
     return r;
 }
 
@@ -437,8 +490,10 @@ double max_resid_fast(const level &L, const vec &phi, const vec &rho) {
  * point equation A - D x - e^x = 0 of iteration_loop (:177-199), in place,
  * colour (i+j+k)%2 == 0 first. */
 void rbgs_sweep(const level &L, vec &phi, const vec &rho, double om) {
+    /* the points of one colour read only points of the other */
     for (int color = 0; color < 2; ++color)
-        for (int i = 0; i < L.n; ++i)
+        par_for(L.n, 1, [&](long il) {
+            const int i = (int)il;
             for (int j = 0; j < L.n; ++j)
                 for (int k = (i + j + color) & 1; k < L.n; k += 2) {
                     double A, D;
@@ -447,17 +502,19 @@ void rbgs_sweep(const level &L, vec &phi, const vec &rho, double om) {
                     const double x = phi[q], ex = exp(x);
                     phi[q] = x - om * ((A - D * x - ex) / (-D - ex));
                 }
+        });
 }
 
 /* N(phi) = -lap_h phi + e^phi = -f(phi; rho = 0) at every point */
 void apply_N(const level &L, const vec &phi, vec &out) {
     out.resize(phi.size());
-    for (int i = 0; i < L.n; ++i)
+    par_for(L.n, 1, [&](long i) {
         for (int j = 0; j < L.n; ++j)
             for (int k = 0; k < L.n; ++k) {
-                size_t q = L.idx(i, j, k);
-                out[q] = 0. - L.resid_fast(phi.data(), nullptr, i, j, k);
+                size_t q = L.idx((int)i, j, k);
+                out[q] = 0. - L.resid_fast(phi.data(), nullptr, (int)i, j, k);
             }
+    });
 }
 
 void fas_head(kfo_ctx *c, int l, vec &phi, const vec &rho, vec &r);
@@ -492,9 +549,11 @@ void fas_head(kfo_ctx *c, int l, vec &phi, const vec &rho, vec &r) {
     const double om = cf.mg_omega > 0. ? cf.mg_omega : 1.;
     for (int s = 0; s < cf.mg_pre; ++s) rbgs_sweep(L, phi, rho, om);
     r.assign(phi.size(), 0.);
-    for (int i = 0; i < L.n; ++i)
+    par_for(L.n, 1, [&](long i) {
         for (int j = 0; j < L.n; ++j)
-            for (int k = 0; k < L.n; ++k) r[L.idx(i, j, k)] = L.resid_fast(phi.data(), rho.data(), i, j, k);
+            for (int k = 0; k < L.n; ++k)
+                r[L.idx((int)i, j, k)] = L.resid_fast(phi.data(), rho.data(), (int)i, j, k);
+    });
 }
 
 /* the rest: restriction, the coarse cycle, the correction, post-smoothing */
@@ -508,13 +567,13 @@ void fas_tail(kfo_ctx *c, int l, vec &phi, const vec &rho, const vec &r) {
     const level &Lc = c->lv[l + 1];
     apply_N(Lc, phic, Nc); /* -lap_c phic + e^phic */
     rhoc.resize(phic.size());
-    for (size_t q = 0; q < phic.size(); ++q) rhoc[q] = Nc[q] + rc[q];
+    par_for((long)(phic.size()), 16384, [&](long q) { rhoc[q] = Nc[q] + rc[q]; });
     vec phic0 = phic;
     fas_vcycle(c, l + 1, phic, rhoc);
-    for (size_t q = 0; q < phic.size(); ++q) phic[q] = phic[q] - phic0[q];
+    par_for((long)(phic.size()), 16384, [&](long q) { phic[q] = phic[q] - phic0[q]; });
     vec e;
     prolong(Lc.n, cf.L, cf.stretch_m, phic, e);
-    for (size_t q = 0; q < phi.size(); ++q) phi[q] += e[q];
+    par_for((long)(phi.size()), 16384, [&](long q) { phi[q] += e[q]; });
     for (int s = 0; s < cf.mg_post; ++s) rbgs_sweep(L, phi, rho, om);
 }
 
@@ -610,11 +669,11 @@ void phi_guess(kfo_ctx *c, double t, bool &newtime) {
     if (!c->cfg.phi_extrap || !newtime || c->nhist == 0) return;
     if (c->nhist >= 2) {
         const double w = (t - c->tau_b) / (c->tau_b - c->tau_a);
-        for (size_t i = 0; i < c->N; ++i) {
+        par_for((long)c->N, 16384, [&](long i) {
             const double b = c->Phi[i], a = c->phi_a[i];
             c->Phi[i] = b + w * (b - a);
             c->phi_a[i] = b;
-        }
+        });
     } else {
         c->phi_a = c->Phi;
     }
@@ -640,7 +699,7 @@ int rhs(kfo_ctx *c, vec *FU, vec &Fni, double t) {
         F1 = Fni;
         dealias(c, F1);
         c2r(c, F1, b1);
-        for (size_t i = 0; i < N; ++i) b1[i] = exp(b1[i]) + c->nd[i];
+        par_for((long)(N), 16384, [&](long i) { b1[i] = exp(b1[i]) + c->nd[i]; });
         bool newtime;
         phi_guess(c, t, newtime);
         rc = poisson(c, c->Phi, b1);
@@ -649,7 +708,7 @@ int rhs(kfo_ctx *c, vec *FU, vec &Fni, double t) {
     }
     /* [dissipation & spectral viscosity] :119-209 */
     const bool diss = T & KFO_DISSIPATION, sv = T & KFO_SVISCOSITY;
-    for (size_t i = 0; i < Nc; ++i) {
+    par_for((long)Nc, 16384, [&](long i) {
         for (int q = 0; q < 3; ++q)
             for (int ri = 0; ri < 2; ++ri) {
                 double u = FU[q][2 * i + ri];
@@ -659,14 +718,15 @@ int rhs(kfo_ctx *c, vec *FU, vec &Fni, double t) {
                                                 : 0.;
             }
         for (int ri = 0; ri < 2; ++ri) FBn[2 * i + ri] = sv ? c->SV[i] * Fni[2 * i + ri] : 0.;
-    }
+    });
     /* [Laplacian diffusion] (new term; -D |k|^2 q^ in d/dt, +D |k|^2 q^ in FB) */
     if (T & KFO_DIFFUSION) {
-        for (size_t i = 0; i < Nc; ++i)
+        par_for((long)Nc, 16384, [&](long i) {
             for (int ri = 0; ri < 2; ++ri) {
                 for (int q = 0; q < 3; ++q) FBu[q][2 * i + ri] += cf.diff_D * c->K2[i] * FU[q][2 * i + ri];
                 FBn[2 * i + ri] += cf.diff_D * c->K2[i] * Fni[2 * i + ri];
             }
+        });
     }
     /* [E-force + pressure] :218-248 */
     const bool pres = T & KFO_PRESSURE, eint = T & KFO_E_INT;
@@ -674,21 +734,21 @@ int rhs(kfo_ctx *c, vec *FU, vec &Fni, double t) {
         if (eint) {
             r2c(c, c->Phi, F1);
             if (pres)
-                for (size_t i = 0; i < Nc; ++i) {
+                par_for((long)Nc, 16384, [&](long i) {
                     F1[2 * i] *= c->PF[i];
                     F1[2 * i + 1] *= c->PF[i];
-                }
+                });
         }
         if (pres && eint) {
-            for (size_t i = 0; i < Nc; ++i) {
+            par_for((long)Nc, 16384, [&](long i) {
                 F1[2 * i] += Fni[2 * i] / cf.theta;
                 F1[2 * i + 1] += Fni[2 * i + 1] / cf.theta;
-            }
+            });
         } else if (pres) {
-            for (size_t i = 0; i < Nc; ++i) {
+            par_for((long)Nc, 16384, [&](long i) {
                 F1[2 * i] = Fni[2 * i] / cf.theta;
                 F1[2 * i + 1] = Fni[2 * i + 1] / cf.theta;
-            }
+            });
         }
         for (int d = 0; d < 3; ++d) {
             deriv(c, d, F1, F2);
@@ -706,9 +766,9 @@ int rhs(kfo_ctx *c, vec *FU, vec &Fni, double t) {
     /* [mean flow] :279-311 */
     if (T & KFO_E_EXT) {
         for (int q = 0; q < 3; ++q)
-            for (size_t i = 0; i < 2 * Nc; ++i) FBu[q][i] += cf.M * dFU[q][0][i];
+            par_for((long)(2 * Nc), 16384, [&](long i) { FBu[q][i] += cf.M * dFU[q][0][i]; });
         deriv(c, 0, Fni, F1);
-        for (size_t i = 0; i < 2 * Nc; ++i) FBn[i] += cf.M * F1[i];
+        par_for((long)(2 * Nc), 16384, [&](long i) { FBn[i] += cf.M * F1[i]; });
     }
     /* [continuity] :315-345 */
     if (T & KFO_CONTINUITY) {
@@ -718,15 +778,15 @@ int rhs(kfo_ctx *c, vec *FU, vec &Fni, double t) {
         if (!(T & KFO_E_EXT)) deriv(c, 0, Fni, F1); /* :322 relies on :305 */
         dealias(c, F1);
         c2r(c, F1, b1);
-        for (size_t i = 0; i < N; ++i) b2[i] = b1[i] * U[0][i];
+        par_for((long)(N), 16384, [&](long i) { b2[i] = b1[i] * U[0][i]; });
         deriv(c, 1, Fni, F1);
         dealias(c, F1);
         c2r(c, F1, b1);
-        for (size_t i = 0; i < N; ++i) b2[i] += b1[i] * U[1][i];
+        par_for((long)(N), 16384, [&](long i) { b2[i] += b1[i] * U[1][i]; });
         deriv(c, 2, Fni, F1);
         dealias(c, F1);
         c2r(c, F1, b1);
-        for (size_t i = 0; i < N; ++i) b2[i] += b1[i] * U[2][i];
+        par_for((long)(N), 16384, [&](long i) { b2[i] += b1[i] * U[2][i]; });
         r2c(c, b2, F1);
         add(FBn, F1);
     }
@@ -736,11 +796,11 @@ int rhs(kfo_ctx *c, vec *FU, vec &Fni, double t) {
             for (int d = 0; d < 3; ++d) dealias(c, dFU[q][d]);
         for (int q = 0; q < 3; ++q) {
             c2r(c, dFU[q][0], b1);
-            for (size_t i = 0; i < N; ++i) b2[i] = U[0][i] * b1[i];
+            par_for((long)(N), 16384, [&](long i) { b2[i] = U[0][i] * b1[i]; });
             c2r(c, dFU[q][1], b1);
-            for (size_t i = 0; i < N; ++i) b2[i] += U[1][i] * b1[i];
+            par_for((long)(N), 16384, [&](long i) { b2[i] += U[1][i] * b1[i]; });
             c2r(c, dFU[q][2], b1);
-            for (size_t i = 0; i < N; ++i) b2[i] += U[2][i] * b1[i];
+            par_for((long)(N), 16384, [&](long i) { b2[i] += U[2][i] * b1[i]; });
             r2c(c, b2, F1);
             add(FBu[q], F1);
         }
@@ -749,8 +809,8 @@ int rhs(kfo_ctx *c, vec *FU, vec &Fni, double t) {
     vec sd;
     if (T & KFO_PENALIZATION) c2r(c, Fni, sd); /* dealiased s in physical space */
     for (int q = 0; q < 3; ++q)
-        for (size_t i = 0; i < 2 * Nc; ++i) FU[q][i] = -FBu[q][i];
-    for (size_t i = 0; i < 2 * Nc; ++i) Fni[i] = -FBn[i];
+        par_for((long)(2 * Nc), 16384, [&](long i) { FU[q][i] = -FBu[q][i]; });
+    par_for((long)(2 * Nc), 16384, [&](long i) { Fni[i] = -FBn[i]; });
     /* [penalization] masking form of effect_penalization.cpp:35 on the finished
      * right-hand side, then the 2/3 filter (cf. rhs_standard.cpp:491-532) */
     if (T & KFO_PENALIZATION) {
@@ -785,7 +845,7 @@ kfo_ctx *kfo_create(const kfo_config *cfg) {
     c->SV.resize(c->Nc);
     c->PF.resize(c->Nc);
     c->K2.resize(c->Nc);
-    for (int i = 0; i < n; ++i)
+    par_for(n, 1, [&](long i) {
         for (int j = 0; j < n; ++j)
             for (int k = 0; k < c->nzc; ++k) {
                 size_t ijk = (size_t)k + c->nzc * ((size_t)j + (size_t)i * n);
@@ -804,6 +864,7 @@ kfo_ctx *kfo_create(const kfo_config *cfg) {
                 c->PF[ijk] = exp(-2000. * pow(kq, 15.));
                 c->K2[ijk] = kx * kx + ky * ky + kz * kz;
             }
+    });
     for (int q = 0; q < 3; ++q) c->FU[q].assign(2 * c->Nc, 0.);
     c->Fs.assign(2 * c->Nc, 0.);
     c->Phi.assign(c->N, 0.);
@@ -898,23 +959,24 @@ int kfo_rk4(kfo_ctx *c, double dt, int nsteps) {
         if (rc) return rc;
         for (int q = 0; q < 4; ++q) {
             R2[q].resize(M);
-            for (size_t i = 0; i < M; ++i) R2[q][i] = R0[q][i] + 0.5 * dt * R1[q][i];
+            par_for((long)(M), 16384, [&](long i) { R2[q][i] = R0[q][i] + 0.5 * dt * R1[q][i]; });
         }
         if ((rc = rhs(c, R2, R2[3], t0 + 0.5 * dt))) return rc;
         for (int q = 0; q < 4; ++q) {
             R3[q].resize(M);
-            for (size_t i = 0; i < M; ++i) R3[q][i] = R0[q][i] + 0.5 * dt * R2[q][i];
+            par_for((long)(M), 16384, [&](long i) { R3[q][i] = R0[q][i] + 0.5 * dt * R2[q][i]; });
         }
         if ((rc = rhs(c, R3, R3[3], t0 + 0.5 * dt))) return rc;
         for (int q = 0; q < 4; ++q) {
             R4[q].resize(M);
-            for (size_t i = 0; i < M; ++i) R4[q][i] = R0[q][i] + 1.0 * dt * R3[q][i];
+            par_for((long)(M), 16384, [&](long i) { R4[q][i] = R0[q][i] + 1.0 * dt * R3[q][i]; });
         }
         if ((rc = rhs(c, R4, R4[3], t0 + 1.0 * dt))) return rc;
         for (int q = 0; q < 4; ++q)
-            for (size_t i = 0; i < M; ++i)
+            par_for((long)M, 16384, [&](long i) {
                 (*Y[q])[i] = R0[q][i] + (dt / 6.) * (1. * R1[q][i] + 2. * R2[q][i] + 2. * R3[q][i] +
                                                       1. * R4[q][i]);
+            });
         c->t = t0 + dt;
     }
     return 0;
@@ -948,7 +1010,7 @@ void kfo_c2r(int n, const double *in, double *out) {
     size_t N = (size_t)n * n * n;
     kfs_c2r_3d(n, n, n, in, out);
     double Norm = 1. / ((double)N);
-    for (size_t i = 0; i < N; ++i) out[i] = out[i] * Norm;
+    par_for((long)(N), 16384, [&](long i) { out[i] = out[i] * Norm; });
 }
 
 void kfo_transfer(int kind, int n, double L, const double *in, double *out) {

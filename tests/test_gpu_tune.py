@@ -76,18 +76,45 @@ def test_rk4_fas_variants_vs_oracle(rows):
     assert rel(gphi, o.get_phi()) < TOL64
 
 
-def test_rbgs_rows_bit_identical():
-    n = 64
+@pytest.mark.parametrize("n,levels", [(64, 3), (128, 4), (256, 6)])
+def test_rbgs_variants_bit_identical(n, levels):
+    """The half-sweep kernels (4, 8, 16 rows) and the streaming TMA-staged
+    sweep (rows 0; levels n >= 64, residual fused into the last pre-smoothing
+    sweep) give the same potential bit for bit, with the same cycle count."""
     st = I.initial_state(n, seed=5)
     nd = I.gauss_charge(n, L, -10.0, 0.5)
     rho = np.exp(np.fft.irfftn(st[3], s=(n, n, n), axes=(0, 1, 2))) + nd
-    cfg = kf.Config.make(n, L, 0.8, poisson_mode=kf.KF_PS_FAS, mg_levels=3, res_tol=1e-11)
-    out = {}
+    cfg = kf.Config.make(n, L, 0.8, poisson_mode=kf.KF_PS_FAS, mg_levels=levels, res_tol=1e-11, mg_omega=1.25)
+    out, cyc = {}, {}
     with kf.Context(cfg) as ctx:
-        for rows in (4, 8, 16):
+        for rows in ((4, 8, 16, 0) if n == 64 else (8, 0)):
             ctx.set_tuning(0, rows)
             out[rows] = ctx.poisson(np.zeros((n, n, n)), rho)
-    assert np.array_equal(out[4], out[8]) and np.array_equal(out[16], out[8])
+            cyc[rows] = ctx.diag().last_iterations
+    for rows in out:
+        assert np.array_equal(out[rows], out[8]), rows
+        assert cyc[rows] == cyc[8]
+
+
+@pytest.mark.parametrize("prec", [kf.KF_FP64, kf.KF_FP32_BULK])
+def test_rk4_streaming_smoother_bit_identical(prec):
+    """Captured FAS steps at 128^3 (levels 128 and 64 streamed): state,
+    potential and V-cycle counts equal to the half-sweep kernels'."""
+    n, steps = 128, 2
+    w = C.WORKLOADS["fas128"]
+    st, nd, mask, dt = C.make_inputs(w, n=n)
+    cfg = C.config_for(w, n=n, precision=prec)
+    res = {}
+    for rows in (8, 0):
+        with kf.Context(cfg) as ctx:
+            ctx.set_tuning(0, rows)
+            ctx.set_state(*st)
+            ctx.set_sources(nd, mask)
+            ctx.rk4(dt, steps)
+            res[rows] = (ctx.get_state(), ctx.get_phi(), ctx.diag().total_iterations)
+    (s8, p8, c8), (s0, p0, c0) = res[8], res[0]
+    assert all(np.array_equal(a, b) for a, b in zip(s8, s0))
+    assert np.array_equal(p8, p0) and c8 == c0
 
 
 def test_autotune_keeps_state_and_steps():
@@ -105,12 +132,13 @@ def test_autotune_keeps_state_and_steps():
             c.rk4(dt, 2)
         s0, p0 = a.get_state(), a.get_phi()
         t = a.autotune(3)
-        assert t["fft_plan"] in (0, 1) and t["rbgs_rows"] in (4, 8, 16)
+        assert t["fft_plan"] in (0, 1) and t["rbgs_rows"] in (0, 4, 8, 16)
         for rad, thr in zip(t["fft_radices"], t["fft_threads"]):
             assert int(np.prod(rad)) == n and thr > 0
-        assert min(t["fft_ms"]) > 0 and min(t["rbgs_ms"]) > 0
+        timed = [x for x in t["rbgs_ms"] if x > 0]
+        assert min(t["fft_ms"]) > 0 and len(timed) == 4  # 64^3: the streaming sweep is a candidate
         assert t["fft_ms"][t["fft_plan"]] == min(t["fft_ms"])
-        assert t["rbgs_ms"][(4, 8, 16).index(t["rbgs_rows"])] == min(t["rbgs_ms"])
+        assert t["rbgs_ms"][(4, 8, 16, 0).index(t["rbgs_rows"])] == min(timed)
         s1, p1 = a.get_state(), a.get_phi()
         assert all(np.array_equal(x, y) for x, y in zip(s0, s1)) and np.array_equal(p0, p1)
         b.set_tuning(t["fft_plan"], t["rbgs_rows"])

@@ -51,6 +51,35 @@ def test_noalloc_r2c_matches_context_r2c_on_two_calls(n):
             assert np.abs(got - ref).max() <= TOL * np.abs(ref).max()
 
 
+def test_noalloc_allocates_nothing_on_a_side_stream():
+    """After the warm-up call (which may load the module and its static
+    array), further calls on a non-default stream leave the device's free
+    memory unchanged and match kf_fft_r2c."""
+    import torch
+    lib = _lib.load_library()
+    n = 64
+    rng = np.random.default_rng(7)
+    side = torch.cuda.Stream()
+    x = rng.standard_normal((n, n, n))
+    xin = torch.from_numpy(x).cuda()
+    out = torch.zeros((n, n, n // 2 + 1), dtype=torch.complex128, device="cuda")
+    with kf.Context(kf.Config.make(n, L, 0.8)) as ctx:
+        ref = ctx.r2c(x)
+    torch.cuda.synchronize()
+    assert _call(lib, n, xin, out, side.cuda_stream) == 0, lib.kf_last_error(None).decode()  # warm-up
+    side.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(2):
+        out.zero_()
+        torch.cuda.synchronize()
+        assert _call(lib, n, xin, out, side.cuda_stream) == 0, lib.kf_last_error(None).decode()
+        side.synchronize()
+        got = out.cpu().numpy()
+        assert np.abs(got - ref).max() <= TOL * np.abs(ref).max()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+
+
 def test_noalloc_rejects_grids_beyond_its_scratch():
     import torch
     lib = _lib.load_library()
