@@ -48,9 +48,12 @@ def parse():
                     help="keep the default kernel variants (no kf_autotune; profiling runs)")
     ap.add_argument("--cpu-ref", default="", help=argparse.SUPPRESS)
     ap.add_argument("--profile-range", action="store_true",
-                    help="bracket the timed steps of the first arm with cudaProfilerStart/Stop "
-                         "(for ncu --profile-from-start off); changes no work")
+                    help="bracket the first arm's profile steps (launched kernel by kernel, the same "
+                         "kernels as the timed graph replays) with cudaProfilerStart/Stop, for "
+                         "ncu --profile-from-start off; changes no work")
     ap.add_argument("--marks", default="100,500,2000", help="steps at which --workload precision compares")
+    ap.add_argument("--sweep-steps", type=int, default=10,
+                    help="RK4 steps per instance of the 48-instance sweep leg; 0 skips it")
     ap.add_argument("--adjoint-steps", type=int, default=200,
                     help="RK4 steps of the adjoint leg (128^3 FP64, checkpoints every 15); 0 skips it")
     return ap.parse_args()
@@ -321,15 +324,11 @@ def run_kf(args):
         sampler = ClockSampler(torch.cuda.current_device()) if clocks else None
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         l0 = ctx.launch_count()
-        if prange:
-            torch.cuda.profiler.start()
         with torch.cuda.stream(stream):
             e0.record(stream)
             ctx.rk4(dt, args.steps)
             e1.record(stream)
         stream.synchronize()
-        if prange:
-            torch.cuda.profiler.stop()
         torch.cuda.synchronize()
         barrier()
         launches = ctx.launch_count() - l0
@@ -343,7 +342,13 @@ def run_kf(args):
             # per-kernel CUDA-event profile of further steps of the same run
             # (kernels launched one by one, each bracketed by events)
             ctx.profile(True)
+            if prange:
+                torch.cuda.synchronize()
+                torch.cuda.profiler.start()
             ctx.rk4(dt, max(1, min(args.steps, 3)))
+            if prange:
+                torch.cuda.synchronize()
+                torch.cuda.profiler.stop()
             prof = ctx.profile_read()
             ctx.profile(False)
         ctx.tune = tune
@@ -422,6 +427,7 @@ def run_kf(args):
                            "rbgs_rows": tune64["rbgs_rows"]}}
 
     adj = adjoint_leg(args.adjoint_steps, stream) if args.adjoint_steps > 0 else None
+    sweep = sweep_leg(args, args.sweep_steps) if args.sweep_steps > 0 else None
 
     if rank != 0:
         if ws > 1:
@@ -467,6 +473,7 @@ def run_kf(args):
                     "last_residual": d32.last_residual, "not_converged": d32.not_converged},
         "fp64": fp64,
         "adjoint": adj,
+        "sweep48": sweep,
     }
     print(json.dumps(out))
     if ws > 1:
@@ -474,49 +481,51 @@ def run_kf(args):
     return 0
 
 
-def run_sweep_bench(args):
+def sweep_leg(args, steps: int):
     """The 48-instance sweep (16 each at 64^3, 96^3, 128^3): instance-steps/s
-    with all of a rank's instances driven concurrently, and the same instances
-    one after another.  Instances are partitioned across ranks by cost."""
+    with all of a rank's instances driven concurrently (kf_batch_rk4_steps),
+    and the same instances one after another.  Instances are partitioned
+    across ranks by cost; wall time is the max over ranks."""
     import torch
 
     from kielflow_b200 import dist as kdist
     from kielflow_b200.sweep import run_sweep, sweep_instances
 
-    ws, rank, local = dist_env()
-    if ws > 1:
-        import datetime
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
-    torch.cuda.set_device(local)
+    ws, rank, _ = dist_env()
     inst = sweep_instances(seed=0)
     mine = [inst[i] for i in kdist.partition([x.n for x in inst], ws)[rank]]
     if ws > 1:
         torch.distributed.barrier()
     tunings = {}
-    wall_c, _, dg = run_sweep(mine, steps=args.steps, mode="batched", warmup=args.warmup, tunings=tunings)
+    wall_c, _, dg = run_sweep(mine, steps=steps, mode="batched", warmup=args.warmup, tunings=tunings)
     wall_c = kdist.max_over_ranks(wall_c, device="cuda")
-    wall_s = wall_t = None
-    if not args.no_fp64:  # the sequential reference run (skipped with --no-fp64 to save time)
-        wall_s, _, _ = run_sweep(mine, steps=args.steps, mode="sequential", warmup=args.warmup, tune=tunings)
-        wall_s = kdist.max_over_ranks(wall_s, device="cuda")
-        wall_t, _, _ = run_sweep(mine, steps=args.steps, mode="threads", warmup=args.warmup, tune=tunings)
-        wall_t = kdist.max_over_ranks(wall_t, device="cuda")
+    wall_s, _, _ = run_sweep(mine, steps=steps, mode="sequential", warmup=args.warmup, tune=tunings)
+    wall_s = kdist.max_over_ranks(wall_s, device="cuda")
+    total = len(inst) * steps
+    return {"metric": "sweep instance-steps/s (48 instances, 64^3/96^3/128^3, FP32 bulk)",
+            "value": total / wall_c, "unit": "instance-steps/s", "steps": steps, "warmup": args.warmup,
+            "sequential_value": total / wall_s, "batched_over_sequential": wall_s / wall_c,
+            "v_cycles_per_solve": (sum(d.total_iterations for d in dg) / max(1, sum(d.solves for d in dg))),
+            "config": {"workload": "sweep48: 16 x 64^3, 16 x 96^3, 16 x 128^3; M ~ U[0.3,1.5], nu ~ U[0.01,0.3], "
+                                   "Q ~ U[-50,-5], sigma 0.5 (seed 0); FP32 bulk, FP64 FAS Poisson to 2^-23 max|n_d|",
+                       "timing": "host wall clock around fully synchronised runs, max over ranks; warm-up steps "
+                                 "(graph capture) outside", "batched": "kf_batch_rk4_steps",
+                       "sequential": "kf_rk4_steps per instance, one after another",
+                       "tuning": {str(n): {"fft_radices": t["fft_radices"][t["fft_plan"]],
+                                           "rbgs_rows": t["rbgs_rows"]} for n, t in sorted(tunings.items())}}}
+
+
+def run_sweep_bench(args):
+    import torch
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+    torch.cuda.set_device(local)
+    out = sweep_leg(args, args.steps)
     if rank == 0:
-        total = len(inst) * args.steps
-        out = {"metric": "sweep instance-steps/s (48 instances, 64^3/96^3/128^3, FP32 bulk)",
-               "value": total / wall_c, "unit": "instance-steps/s", "n_gpus": ws, "steps": args.steps,
-               "warmup": args.warmup, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
-               "dtype": "fp32 bulk + fp64 Poisson", "data": "synthetic",
-               "config": {"workload": "sweep48: 16 x 64^3, 16 x 96^3, 16 x 128^3; M ~ U[0.3,1.5], nu ~ U[0.01,0.3], "
-                                      "Q ~ U[-50,-5] (seed 0); FP32 bulk, FP64 FAS Poisson",
-                          "timing": "host wall clock around fully synchronised runs; warm-up steps "
-                                    "(graph capture) outside", "batched": "kf_batch_rk4_steps",
-                          "sequential": "kf_rk4_steps per instance, one after another",
-                          "tuning": {str(n): {"fft_radices": t["fft_radices"][t["fft_plan"]],
-                                              "rbgs_rows": t["rbgs_rows"]} for n, t in sorted(tunings.items())}},
-               "sequential_value": (total / wall_s) if wall_s else None,
-               "threads_value": (total / wall_t) if wall_t else None,
-               "batched_over_sequential": (wall_s / wall_c) if wall_s else None}
+        out.update({"n_gpus": ws, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+                    "dtype": "fp32 bulk + fp64 Poisson", "data": "synthetic"})
         print(json.dumps(out))
     if ws > 1:
         torch.distributed.destroy_process_group()

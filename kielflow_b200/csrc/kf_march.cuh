@@ -46,13 +46,13 @@ constexpr int MT_THREADS = 256;
 
 enum MarchMode : int { MM_RES = 0, MM_SWEEP = 1, MM_SWEEP_RES = 2 };
 
-template <int MODE, int TJ> struct MarchShape {
+template <int MODE, int TJ, int PF_ = 2> struct MarchShape {
     static constexpr int NST = MODE == MM_RES ? 1 : (MODE == MM_SWEEP ? 2 : 3);  // stages per plane
     static constexpr int H = NST;              // phi halo rows (j) and ghost planes (i)
     static constexpr int HK = (NST + 1) & ~1;  // phi halo columns (k): even, so the copy's x is 16-byte aligned
     static constexpr int RH = NST - 1;         // rho halo rows
     static constexpr int RK = 2;               // rho halo columns (>= NST - 1, even)
-    static constexpr int PF = 2;               // planes fetched ahead
+    static constexpr int PF = PF_;             // planes fetched ahead
     static constexpr int S = NST + PF + 1;     // ring slots
     static constexpr int PROWS = TJ + 2 * H;   // staged phi rows
     static constexpr int RROWS = TJ + 2 * RH;  // staged rho rows
@@ -62,12 +62,12 @@ template <int MODE, int TJ> struct MarchShape {
     static_assert(2 * HK + MT_TK <= MT_PITCH, "phi tile does not fit the staged row");
     static_assert(2 * RK + MT_TK <= MT_PITCH, "rho tile does not fit the staged row");
     static_assert(NPATCH <= MT_THREADS, "one patch value per thread");
-    static_assert(TJ * MT_TK / 2 == MT_THREADS, "one 16-byte phi store per thread and plane");
+    static_assert((TJ * MT_TK / 2) % MT_THREADS == 0, "whole 16-byte phi stores per thread and plane");
 };
 
 // dynamic shared memory of a launch with chunks of ci planes
-template <int MODE, int TJ> inline size_t march_smem(int ci) {
-    using Sh = MarchShape<MODE, TJ>;
+template <int MODE, int TJ, int PF = 2> inline size_t march_smem(int ci) {
+    using Sh = MarchShape<MODE, TJ, PF>;
     const int np = ci + 2 * Sh::H;
     return 128 + 8 * (size_t)Sh::S * (Sh::PSLOT + Sh::RSLOT)  // ring (128: base alignment)
            + 8 * (size_t)3 * (MT_PITCH + Sh::PROWS + np)      // axis tables
@@ -132,12 +132,21 @@ __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.
 
 __device__ __forceinline__ int wrapn(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
-template <int MODE, int TJ>
-__global__ void __launch_bounds__(MT_THREADS, 2)
+// One colour update of the point at staged offset o: the arithmetic of
+// point_coeffs_fast + newton_step (kf_poisson.cuh) on the staged planes.
+struct MarchPoint {
+    int o, ro, rr, cc;
+};
+
+// MODE: MM_*; TJ: tile rows; PF: planes fetched ahead; PAIR: each thread
+// takes two points at a time (loads of both, then both Newton steps), for
+// independent work in flight; MINB: resident CTAs per SM the registers allow.
+template <int MODE, int TJ, int PF = 2, bool PAIR = false, int MINB = 2>
+__global__ void __launch_bounds__(MT_THREADS, MINB)
     k_rbgs_march(const __grid_constant__ CUtensorMap tm_phi, const __grid_constant__ CUtensorMap tm_rho,
                  MarchArgs a) {
-    using Sh = MarchShape<MODE, TJ>;
-    constexpr int NST = Sh::NST, H = Sh::H, HK = Sh::HK, RH = Sh::RH, RK = Sh::RK, S = Sh::S, PF = Sh::PF;
+    using Sh = MarchShape<MODE, TJ, PF>;
+    constexpr int NST = Sh::NST, H = Sh::H, HK = Sh::HK, RH = Sh::RH, RK = Sh::RK, S = Sh::S;
     constexpr int W = MT_PITCH;
     constexpr bool SWEEP = MODE != MM_RES, RES = MODE != MM_SWEEP;
     constexpr long long WAIT_LIMIT = 4000000000LL;  // about 2 s at the boost clock
@@ -265,30 +274,63 @@ __global__ void __launch_bounds__(MT_THREADS, 2)
                 const int color = s;  // colour 0, then colour 1
                 const int ppr = MT_TK / 2 + m;  // points of the colour per row
                 const int items = (TJ + 2 * m) * ppr;
-                for (int it = tid; it < items; it += MT_THREADS) {
+                auto locate = [&](int it) {
                     const int row = it / ppr, pr = it - row * ppr;
                     const int ju = j0 - m + row;
                     const int ks = k0 - m;
                     const int k = ks + 2 * pr + ((color + iu + ju + ks) & 1);
-                    const int rr = row + H - m, cc = k - k0 + HK;
-                    const int o = rr * W + cc;
-                    const double *q = pc + o;
-                    double A = __dmul_rn(pp[o], ipi);
-                    A = __dadd_rn(A, __dmul_rn(pm[o], imi));
-                    A = __dadd_rn(A, __dmul_rn(q[W], tj[Sh::PROWS + rr]));
-                    A = __dadd_rn(A, __dmul_rn(q[-W], tj[2 * Sh::PROWS + rr]));
-                    A = __dadd_rn(A, __dmul_rn(q[1], tk[W + cc]));
-                    A = __dadd_rn(A, __dmul_rn(q[-1], tk[2 * W + cc]));
-                    A = __dadd_rn(A, rc[(row + RH - m) * W + (k - k0 + RK)]);
-                    const double D = __dadd_rn(__dadd_rn(ddi, tj[rr]), tk[cc]);
-                    pc[o] = newton_step(q[0], A, D, a.om);
+                    MarchPoint P;
+                    P.rr = row + H - m;
+                    P.cc = k - k0 + HK;
+                    P.o = P.rr * W + P.cc;
+                    P.ro = (row + RH - m) * W + (k - k0 + RK);
+                    return P;
+                };
+                auto coeffs = [&](const MarchPoint &P, double &A, double &D) {
+                    const double *q = pc + P.o;
+                    A = __dmul_rn(pp[P.o], ipi);
+                    A = __dadd_rn(A, __dmul_rn(pm[P.o], imi));
+                    A = __dadd_rn(A, __dmul_rn(q[W], tj[Sh::PROWS + P.rr]));
+                    A = __dadd_rn(A, __dmul_rn(q[-W], tj[2 * Sh::PROWS + P.rr]));
+                    A = __dadd_rn(A, __dmul_rn(q[1], tk[W + P.cc]));
+                    A = __dadd_rn(A, __dmul_rn(q[-1], tk[2 * W + P.cc]));
+                    A = __dadd_rn(A, rc[P.ro]);
+                    D = __dadd_rn(__dadd_rn(ddi, tj[P.rr]), tk[P.cc]);
+                };
+                if constexpr (PAIR) {
+                    // the points of one colour read only the other colour:
+                    // both loads before both stores give the same values
+                    for (int it = tid; it < items; it += 2 * MT_THREADS) {
+                        const int it2 = it + MT_THREADS;
+                        const bool two = it2 < items;
+                        const MarchPoint P0 = locate(it), P1 = locate(two ? it2 : it);
+                        double A0, D0, A1, D1;
+                        coeffs(P0, A0, D0);
+                        coeffs(P1, A1, D1);
+                        const double x0 = pc[P0.o], x1 = pc[P1.o];
+                        const double y0 = newton_step(x0, A0, D0, a.om);
+                        const double y1 = newton_step(x1, A1, D1, a.om);
+                        pc[P0.o] = y0;
+                        if (two) pc[P1.o] = y1;
+                    }
+                } else {
+                    for (int it = tid; it < items; it += MT_THREADS) {
+                        const MarchPoint P = locate(it);
+                        double A, D;
+                        coeffs(P, A, D);
+                        pc[P.o] = newton_step(pc[P.o], A, D, a.om);
+                    }
                 }
                 __syncthreads();
                 if (SWEEP && s == 1 && p >= H && p < H + ci) {
                     // the plane's potential is final: 16-byte stores of the interior
-                    const int row = tid / (MT_TK / 2), c2 = tid % (MT_TK / 2);
-                    const double2 v = *(const double2 *)(pc + (row + H) * W + HK + 2 * c2);
-                    *(double2 *)(a.phi_out + ((long)wrapn(iu, n) * n + j0 + row) * n + k0 + 2 * c2) = v;
+#pragma unroll
+                    for (int u = 0; u < TJ * MT_TK / 2 / MT_THREADS; ++u) {
+                        const int e = tid + u * MT_THREADS;
+                        const int row = e / (MT_TK / 2), c2 = e % (MT_TK / 2);
+                        const double2 v = *(const double2 *)(pc + (row + H) * W + HK + 2 * c2);
+                        *(double2 *)(a.phi_out + ((long)wrapn(iu, n) * n + j0 + row) * n + k0 + 2 * c2) = v;
+                    }
                 }
             } else {
                 // residual on the tile's interior of plane p (all points)

@@ -214,13 +214,18 @@ def test_fp32_bulk_vs_fp64_oracle():
 
 # 96^3: the radix-3 plans (96 = 6 * 4 * 4 and 4 * 4 * 6) in the right-hand side
 # and RK4, in both precisions
-@pytest.mark.parametrize("case", ["all_jacobi", "penalized", "linear"])
+@pytest.mark.parametrize("case", ["all_fas", "penalized", "linear"])
 @pytest.mark.parametrize("plan", [0, 1])
 def test_rhs96_vs_oracle(case, plan):
+    """At 96^3 the Poisson solve of the full set is the sweep's FAS cycle (the
+    Jacobi solver of configuration 0 runs only at 32^3: its Carre factor comes
+    from a sum whose order differs between the GPU tree and the reference's
+    loop, which over the thousands of sweeps at 96^3 reaches 1e-11)."""
     n = 96
-    w = C.WORKLOADS["jacobi32"]
+    w = C.WORKLOADS["fas128" if case == "all_fas" else "jacobi32"]
     st, nd, mask, dt = C.make_inputs(w, n=n, seed=3)
-    cfg = C.config_for(w, n=n, terms=RHS_CASES[case], sv_cut=0.6)
+    terms = kf.KF_T_ALL if case == "all_fas" else RHS_CASES[case]
+    cfg = C.config_for(w, n=n, terms=terms, sv_cut=0.6)
     with kf.Context(cfg) as ctx:
         ctx.set_tuning(plan, 0)
         ctx.set_state(*st)
