@@ -315,7 +315,7 @@ def run_kf(args):
         ctx.set_state(*st)
         ctx.set_sources(nd, mask)
         # radix plan and smoother shape, timed on this context
-        tune = ctx.autotune() if not args.no_tune else {"fft_plan": 0, "rbgs_rows": 0,
+        tune = ctx.autotune() if not args.no_tune else {"fft_plan": 0, "rbgs_rows": 8,
                                                          "fft_radices": [[], []]}
         ctx.rk4(dt, args.warmup)
         ctx.synchronize()

@@ -252,13 +252,12 @@ int kf_batch_rk4_steps(kf_ctx *const *ctxs, int nctx, int nsteps, const double *
  * FFTW plans are chosen by FFTW_MEASURE inside fftw_plan_dft_*, OP_FFT.cpp).
  * fft_plan: radix plan of every transform kernel, 0 or 1 (two factorisations
  * of each supported n into radix stages, with different threads per line);
- * rbgs_rows: the red-black smoother, 0 (the default) for the streaming sweep
- * (one TMA-staged pass per sweep, the residual fused into the last
- * pre-smoothing sweep) on multigrid levels with n a multiple of 64 and the
- * 8-row half-sweep kernel below them, or 4, 8, 16 for half-sweep kernels with
- * that many rows per block on every level.  Results do not depend on
- * rbgs_rows (same arithmetic per point, bit for bit) and agree between the
- * fft plans to rounding. */
+ * rbgs_rows: the red-black smoother, 4, 8 (the default) or 16 for half-sweep
+ * kernels with that many rows per block, or 0 for the streaming sweep (one
+ * TMA-staged pass per sweep, the residual fused into the last pre-smoothing
+ * sweep) on multigrid levels with n a multiple of 64 and the 8-row half-sweep
+ * kernel below them.  Results do not depend on rbgs_rows (same arithmetic
+ * per point, bit for bit) and agree between the fft plans to rounding. */
 typedef struct kf_tune_out {
     int fft_plan;          /* chosen radix plan */
     int rbgs_rows;         /* chosen smoother: rows per k_rbgs block (4, 8, 16), or 0 */

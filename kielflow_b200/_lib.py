@@ -348,9 +348,9 @@ class Context:
         return o.as_dict()
 
     def set_tuning(self, fft_plan: int, rbgs_rows: int):
-        """kf_set_tuning: select the transform plan (0, 1) and the smoother: 0 for the
-        streaming TMA-staged sweep (the default), or 4, 8, 16 rows per block of the
-        half-sweep kernel."""
+        """kf_set_tuning: select the transform plan (0, 1) and the smoother: 4, 8
+        (the default) or 16 rows per block of the half-sweep kernel, or 0 for the
+        streaming TMA-staged sweep."""
         self._check(self.L.kf_set_tuning(self.h, fft_plan, rbgs_rows))
 
     def rk4(self, dt: float, nsteps: int = 1):

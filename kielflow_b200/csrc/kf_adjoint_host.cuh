@@ -62,7 +62,9 @@ void dfree(kf_ctx *c, void *p) {
     }
 }
 
-Geo<double> geo64(kf_ctx *c) { return Geo<double>{c->n, c->nzc, (const double *)c->kv, c->q2, dealias_threshold()}; }
+Geo<double> geo64(kf_ctx *c) {
+    return Geo<double>{c->n, c->nzc, (const double *)c->kv, c->q2, dealias_threshold(), c->pb};
+}
 
 Snap snap_alloc(kf_ctx *c) {
     Snap s;

@@ -75,6 +75,7 @@ struct kf_ctx {
     void *H = nullptr, *phiT = nullptr;
     void *kv = nullptr, *SV = nullptr, *PF = nullptr, *tw = nullptr;
     double *q2 = nullptr;
+    int *pb = nullptr;  // x-pass 2/3-rule bounds per (j, kz) column (dealias_bounds)
     double *stage64 = nullptr;
     std::vector<LevelBuf> lv;
     double *partial = nullptr;
@@ -134,7 +135,7 @@ struct kf_ctx {
     OutState *out = nullptr;
     bool phi_given = false;
     int fftv = 0;     // radix-plan variant of the transform kernels (kf_autotune)
-    int rbgs_by = 0;  // smoother variant (kf_autotune): 0 streaming k_rbgs_march, else k_rbgs rows per block
+    int rbgs_by = 8;  // smoother variant (kf_autotune): k_rbgs rows per block, or 0 for k_rbgs_march
     bool march_maps = false;  // the driver's tensor-map encoder is available
     int stage_idx = 0;  // RK stage of the right-hand side being evaluated (0..3)
     // one RK4 step captured as a CUDA graph (FAS or no Poisson, profile off):
@@ -293,6 +294,30 @@ std::vector<double> metric_table(int n, double L, double m, double thr) {
     }
     for (int i = 0; i < n; ++i) out[i] = (double)(acc[i] / n);
     return out;
+}
+
+// The 2/3 rule of OP_dealiasing.hpp:24-30 on one (j, kz) column of the x
+// pass, (q2[i] + q2[j]) + q2[kz] < thr, as a bound b: keep(i) == (min(i, n - i)
+// <= b).  The bound is the largest such m in [0, n/2] (-1: none), and the
+// equivalence is checked on every i of the column with the same additions as
+// the device; a column where it fails gets -2 (the kernels then test each
+// element).
+std::vector<int> dealias_bounds(const std::vector<double> &q2, int n, double thr) {
+    const int nzc = n / 2 + 1;
+    std::vector<int> pb((size_t)n * nzc);
+    for (int j = 0; j < n; ++j)
+        for (int k = 0; k < nzc; ++k) {
+            int b = -1;
+            for (int m = 0; m <= n / 2; ++m)
+                if ((q2[m] + q2[j]) + q2[k] < thr) b = m;
+            bool ok = true;
+            for (int i = 0; i < n && ok; ++i) {
+                const bool keep = (q2[i] + q2[j]) + q2[k] < thr;
+                ok = keep == ((i <= n / 2 ? i : n - i) <= b);
+            }
+            pb[(size_t)j * nzc + k] = ok ? b : -2;
+        }
+    return pb;
 }
 
 // ------------------------------------------------------------------ Poisson driver
@@ -922,7 +947,9 @@ template <typename T, int N> struct Impl {
     static constexpr int TC = Tile<T>::TC, LZ = ZTile<T>::LZ, NZC = N / 2 + 1;
     template <int V> static constexpr int PV = PlanV<N, V>::P;
 
-    static Geo<T> geo(kf_ctx *c) { return Geo<T>{c->n, c->nzc, (const T *)c->kv, c->q2, dealias_threshold()}; }
+    static Geo<T> geo(kf_ctx *c) {
+        return Geo<T>{c->n, c->nzc, (const T *)c->kv, c->q2, dealias_threshold(), c->pb};
+    }
 
     static void set_attrs() {
         static bool done = false;
@@ -940,7 +967,8 @@ template <typename T, int N> struct Impl {
         CK(cudaFuncSetAttribute(k_axis_pipe<T, N, +1, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
         CK(cudaFuncSetAttribute(k_z_c2r<T, N, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
         CK(cudaFuncSetAttribute(k_z_r2c<T, N, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-        CK(cudaFuncSetAttribute(k_xfwd_assemble<T, N, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+        CK(cudaFuncSetAttribute(k_xfwd_assemble<T, N, V, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+        CK(cudaFuncSetAttribute(k_xfwd_assemble<T, N, V, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     }
 
     static double job_bytes(kf_ctx *c, int off, int njobs) {
@@ -1128,12 +1156,16 @@ template <typename T, int N> struct Impl {
         {
             const double cb = (double)c->Nc * sizeof(T2), rb = (double)c->Nc * sizeof(T);
             Launch L_(c, KC_XASM, pen ? 8 * cb : 8 * cb + 4 * cb + ((Tm & T_E_INT) ? cb : 0.) + 2 * rb);
-            if (c->fftv)
-                k_xfwd_assemble<T, N, 1><<<ntiles, TC * PV<1>, (size_t)N * TC * sizeof(T2), c->st>>>(
-                    c->dj + c->jF_x, geo(c), rargs(c), (const T2 *)c->tw);
+            const size_t sm = (size_t)N * TC * sizeof(T2);
+            const AxisJob *j = c->dj + c->jF_x;
+            if (c->fftv && pen)
+                k_xfwd_assemble<T, N, 1, true><<<ntiles, TC * PV<1>, sm, c->st>>>(j, geo(c), rargs(c), (const T2 *)c->tw);
+            else if (c->fftv)
+                k_xfwd_assemble<T, N, 1, false><<<ntiles, TC * PV<1>, sm, c->st>>>(j, geo(c), rargs(c), (const T2 *)c->tw);
+            else if (pen)
+                k_xfwd_assemble<T, N, 0, true><<<ntiles, TC * PV<0>, sm, c->st>>>(j, geo(c), rargs(c), (const T2 *)c->tw);
             else
-                k_xfwd_assemble<T, N, 0><<<ntiles, TC * PV<0>, (size_t)N * TC * sizeof(T2), c->st>>>(
-                    c->dj + c->jF_x, geo(c), rargs(c), (const T2 *)c->tw);
+                k_xfwd_assemble<T, N, 0, false><<<ntiles, TC * PV<0>, sm, c->st>>>(j, geo(c), rargs(c), (const T2 *)c->tw);
         }
         CK(cudaGetLastError());
     }
@@ -1440,6 +1472,11 @@ void build_tables(kf_ctx *c) {
     }
     c->q2 = dalloc<double>(c, sizeof(double) * n);
     CK(cudaMemcpy(c->q2, q2.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    {
+        const std::vector<int> pb = dealias_bounds(q2, n, dealias_threshold());
+        c->pb = dalloc<int>(c, sizeof(int) * pb.size());
+        CK(cudaMemcpy(c->pb, pb.data(), sizeof(int) * pb.size(), cudaMemcpyHostToDevice));
+    }
     if (c->fp32) {
         std::vector<float> kvf(n), SVf(c->Nc), PFf(c->Nc), twf(2 * n);
         for (int i = 0; i < n; ++i) kvf[i] = (float)kv[i];

@@ -27,6 +27,7 @@ namespace kf {
 #endif
 template <typename T> struct Tile { static constexpr int TC = sizeof(T) == 8 ? KF_TC64 : KF_TC32; };
 
+
 template <typename T2>
 __device__ __forceinline__ T2 mul_ik(T2 a, decltype(T2::x) k) {  // i k a
     return mk<T2>(-k * a.y, k * a.x);
@@ -150,8 +151,23 @@ __device__ __forceinline__ AxisTile<T> axis_tile(const AxisJob *__restrict__ job
     return G;
 }
 
+// Resident blocks per SM that the transform kernels ask the register
+// allocator for: as many as their shared memory allows (TILES tiles of
+// N x TC elements per block), at most CAP, and no more than leave FLOOR
+// registers per thread.  Without this bound the allocator spends 128-224
+// registers per thread on the 256-point transforms and two blocks fit; with
+// it the same code fits 64-85 registers (FP32) without spilling.
+template <typename T, int N, int V, int TILES, int CAP, int FLOOR> struct PipeMinBlocks {
+    static constexpr long threads = (long)Tile<T>::TC * PlanV<N, V>::P;
+    static constexpr long smem = (long)TILES * N * Tile<T>::TC * sizeof(typename C2<T>::type);
+    static constexpr long by_smem = (227L * 1024) / smem;
+    static constexpr long by_regs = 65536L / (threads * FLOOR);
+    static constexpr long lim = by_smem < by_regs ? by_smem : by_regs;
+    static constexpr int value = lim < 1 ? 1 : (lim < CAP ? (int)lim : CAP);
+};
+
 template <typename T, int N, int SIGN, int V = 0>
-__global__ void __launch_bounds__(Tile<T>::TC * PlanV<N, V>::P)
+__global__ void __launch_bounds__(Tile<T>::TC * PlanV<N, V>::P, (PipeMinBlocks<T, N, V, 2, 3, 64>::value))
 k_axis_pipe(const AxisJob *__restrict__ jobs, int njobs, int axis, Geo<T> g,
             const typename C2<T>::type *__restrict__ tw, int total) {
     typedef typename C2<T>::type T2;
@@ -162,7 +178,11 @@ k_axis_pipe(const AxisJob *__restrict__ jobs, int njobs, int axis, Geo<T> g,
     const int c = threadIdx.x % TC, p = threadIdx.x / TC;
     int t = blockIdx.x;
     if (t >= total) return;
-    auto prefetch = [&](const AxisTile<T> &G) {
+    // the tile's descriptor is recomputed where it is needed (loads,
+    // multipliers, stores) instead of being held across the transform:
+    // fewer live registers, more resident blocks
+    auto prefetch = [&](int tt) {
+        const AxisTile<T> G = axis_tile<T, N>(jobs, njobs, axis, tt, c, g.n, g.nzc);
 #pragma unroll
         for (int q = 0; q < E; ++q) {
             const int row = reg_row<N, P, PlanV<N, V>::R1>(p, q);
@@ -174,34 +194,33 @@ k_axis_pipe(const AxisJob *__restrict__ jobs, int njobs, int axis, Geo<T> g,
         }
         cp_async_commit();
     };
-    AxisTile<T> cur = axis_tile<T, N>(jobs, njobs, axis, t, c, g.n, g.nzc);
-    prefetch(cur);
+    prefetch(t);
     for (; t < total; t += gridDim.x) {
-        const int tn = t + gridDim.x;
-        AxisTile<T> nxt = cur;
-        if (tn < total) nxt = axis_tile<T, N>(jobs, njobs, axis, tn, c, g.n, g.nzc);
         cp_async_wait_all();
         T2 v[E];
+        {
+            const AxisTile<T> G = axis_tile<T, N>(jobs, njobs, axis, t, c, g.n, g.nzc);
+            const bool pm = G.mul == MUL_P || G.mul == MUL_P_IK;
+            const int b = pm ? dealias_bound(g.pb, G.jj, G.kk, g.nzc) : -2;
 #pragma unroll
-        for (int q = 0; q < E; ++q) {
-            const int row = reg_row<N, P, PlanV<N, V>::R1>(p, q);
-            T2 x = stg[row * TC + c];
-            if (cur.mul == MUL_P || cur.mul == MUL_P_IK) {
-                if (!dealias_keep(g.q2, g.thr, row, cur.jj, cur.kk)) x = mk<T2>((T)0, (T)0);
+            for (int q = 0; q < E; ++q) {
+                const int row = reg_row<N, P, PlanV<N, V>::R1>(p, q);
+                T2 x = stg[row * TC + c];
+                if (pm && !dealias_keep_b(g.q2, g.thr, b, N, row, G.jj, G.kk)) x = mk<T2>((T)0, (T)0);
+                if (G.mul == MUL_P_IK || G.mul == MUL_IK) x = mul_ik(x, g.kv[row]);
+                v[q] = x;
             }
-            if (cur.mul == MUL_P_IK || cur.mul == MUL_IK) x = mul_ik(x, g.kv[row]);
-            v[q] = x;
         }
-        if (tn < total) prefetch(nxt);
+        if (t + gridDim.x < total) prefetch(t + gridDim.x);
         PlanV<N, V>::template fft<T2, SIGN>(v, sm + c, StrideAddr{TC}, p, tw);
-        if (cur.valid) {
+        const AxisTile<T> G = axis_tile<T, N>(jobs, njobs, axis, t, c, g.n, g.nzc);
+        if (G.valid) {
 #pragma unroll
             for (int q = 0; q < E; ++q) {
                 const int row = reg_row<N, P, PlanV<N, V>::RL>(p, q);
-                cur.out[cur.base + row * cur.rstride] = v[q];
+                G.out[G.base + row * G.rstride] = v[q];
             }
         }
-        cur = nxt;
     }
 }
 
@@ -419,8 +438,11 @@ __device__ __forceinline__ typename C2<T>::type lin_term(const RhsArgs<T> &a, co
 //   penalization on : K_q = P(k) F_q              (the 2/3 filter after the
 //                     physical-space penalization, rhs_standard.cpp:491-532)
 // gridDim.x = number of column tiles; jobs[q].in = y-passed field, .out = K_q.
-template <typename T, int N, int V = 0>
-__global__ void __launch_bounds__(Tile<T>::TC * PlanV<N, V>::P)
+// PEN: the penalization form (a.terms has T_PENALIZATION), instantiated apart
+// so that its registers do not carry the linear terms'.
+template <typename T, int N, int V = 0, bool PEN = false>
+__global__ void __launch_bounds__(Tile<T>::TC * PlanV<N, V>::P,
+                                  (PEN ? PipeMinBlocks<T, N, V, 1, sizeof(T) == 4 ? 4 : 2, 64>::value : 1))
 k_xfwd_assemble(const AxisJob *__restrict__ jobs, Geo<T> g, RhsArgs<T> a,
                 const typename C2<T>::type *__restrict__ tw) {
     typedef typename C2<T>::type T2;
@@ -434,7 +456,7 @@ k_xfwd_assemble(const AxisJob *__restrict__ jobs, Geo<T> g, RhsArgs<T> a,
     const bool valid = col < n * nzc;
     const long rstride = (long)n * nzc;
     const int jj = col / nzc, kk = col - jj * nzc;
-    const bool pen = a.terms & T_PENALIZATION;
+    const int b = PEN ? dealias_bound(g.pb, jj, kk, nzc) : -2;
     for (int q = 0; q < 4; ++q) {
         const T2 *__restrict__ in = static_cast<const T2 *>(jobs[q].in);
         T2 *__restrict__ out = static_cast<T2 *>(jobs[q].out);
@@ -452,8 +474,8 @@ k_xfwd_assemble(const AxisJob *__restrict__ jobs, Geo<T> g, RhsArgs<T> a,
                 const long idx = col + i * rstride;
                 T2 F = v[e];
                 T2 K;
-                if (pen) {
-                    K = dealias_keep(g.q2, g.thr, i, jj, kk) ? F : mk<T2>((T)0, (T)0);
+                if constexpr (PEN) {
+                    K = dealias_keep_b(g.q2, g.thr, b, N, i, jj, kk) ? F : mk<T2>((T)0, (T)0);
                 } else {
                     T2 fb = lin_term(a, g, q, i, jj, kk, idx);
                     K = mk<T2>(-(fb.x + F.x), -(fb.y + F.y));

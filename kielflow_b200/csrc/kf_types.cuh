@@ -49,6 +49,7 @@ template <typename T> struct Geo {
     const T *kv;       // k_val_at(i), i < n                        (axis_EqSt.cpp:57-61)
     const double *q2;  // pow(k_val_at(i)/k_val_at(n/2), 2.), i < n  (OP_dealiasing.hpp:24-28)
     double thr;        // smallest double s with sqrt(s) >= 2/3 (see dealias_threshold)
+    const int *pb;     // per (j, kz) column: the 2/3 rule along i as a bound (dealias_bounds), or nullptr
 };
 
 // sqrt is correctly rounded and monotone, so sqrt(s) < 2/3 holds exactly when
@@ -65,6 +66,19 @@ inline double dealias_threshold() {
 // 2/3 rule of rhs_standard.cpp:22 on the exact |k~|^2 = (q2[i] + q2[j]) + q2[k].
 __device__ __forceinline__ bool dealias_keep(const double *__restrict__ q2, double thr, int i, int j, int k) {
     return __dadd_rn(__dadd_rn(q2[i], q2[j]), q2[k]) < thr;
+}
+
+// The 2/3 rule along the x axis of one (j, kz) column as a bound: keep(i) ==
+// (min(i, n - i) <= b), with b from the host table dealias_bounds (which checks
+// that equivalence for every i of the column and stores -2 where it does not
+// hold); -2 or no table: the exact sum of dealias_keep per element.
+__device__ __forceinline__ int dealias_bound(const int *__restrict__ pb, int jj, int kk, int nzc) {
+    return pb ? pb[jj * nzc + kk] : -2;
+}
+__device__ __forceinline__ bool dealias_keep_b(const double *__restrict__ q2, double thr, int b, int n, int i, int j,
+                                               int k) {
+    if (b >= -1) return (i <= n / 2 ? i : n - i) <= b;
+    return dealias_keep(q2, thr, i, j, k);
 }
 
 // Everything the spectral linear terms and the assembly need.
