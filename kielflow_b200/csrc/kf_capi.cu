@@ -1121,8 +1121,8 @@ template <typename T, int N> struct Impl {
         // C
         if (pen) {
             Launch L_(c, KC_LIN, (double)c->Nc * (9 * sizeof(T2) + 2 * sizeof(T)));
-            k_lin<T><<<nblk(c->Nc, 256), 256, 0, c->st>>>(rargs(c), geo(c), (T2 *)c->LIN[0], (T2 *)c->LIN[1],
-                                                         (T2 *)c->LIN[2], (T2 *)c->LIN[3]);
+            k_lin<T><<<mg_grid(NZC, N), mg_block(), 0, c->st>>>(rargs(c), geo(c), (T2 *)c->LIN[0], (T2 *)c->LIN[1],
+                                                               (T2 *)c->LIN[2], (T2 *)c->LIN[3]);
         }
         // D
         axis(c, c->jD_x, pen ? 10 : 6, 0, +1);

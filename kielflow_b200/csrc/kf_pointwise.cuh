@@ -66,22 +66,83 @@ __global__ void k_products(ProdArgs<T> a) {
     }
 }
 
-// rl_q = -lin_q in k-space (penalization path; one thread per half-spectrum element)
+// rl_q = -lin_q in k-space (penalization path).  Grid (ceil(nzc/32), n/8, n)
+// of 32 x 8 blocks over (kz, j, i): no index division.  The four outputs of
+// an element share its loads (state, phi^, tables); each is accumulated in the
+// order of lin_term (kf_passes.cuh), so the values are those of lin_term.
 template <typename T>
-__global__ void k_lin(RhsArgs<T> a, Geo<T> g, typename C2<T>::type *o0, typename C2<T>::type *o1,
-                      typename C2<T>::type *o2, typename C2<T>::type *o3) {
+__global__ void __launch_bounds__(256) k_lin(RhsArgs<T> a, Geo<T> g, typename C2<T>::type *o0,
+                                             typename C2<T>::type *o1, typename C2<T>::type *o2,
+                                             typename C2<T>::type *o3) {
     typedef typename C2<T>::type T2;
-    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long Nc = (long)g.n * g.n * g.nzc;
-    if (idx >= Nc) return;
-    const int k = (int)(idx % g.nzc);
-    const long r = idx / g.nzc;
-    const int j = (int)(r % g.n), i = (int)(r / g.n);
+    const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, i = blockIdx.z;
+    if (k >= g.nzc || j >= g.n) return;
+    const long idx = (long)k + (long)g.nzc * ((long)j + (long)i * g.n);
+    const int Tm = a.terms;
+    const bool P = dealias_keep(g.q2, g.thr, i, j, k);
+    const T kx = g.kv[i], ky = g.kv[j], kz = g.kv[k];
+    const T sv = a.SV[idx];
+    const T2 u[3] = {a.Y[0][idx], a.Y[1][idx], a.Y[2][idx]};
+    const T2 s = a.Y[3][idx];
+    const bool diss = Tm & T_DISSIPATION, svo = Tm & T_SVISCOSITY;
+    const bool pres = Tm & T_PRESSURE, eint = Tm & T_E_INT;
+    // F1 = PF phi^ + s^/theta, the E-force/pressure potential (rhs_standard.cpp:218-248)
+    T2 F1 = mk<T2>((T)0, (T)0);
+    if (pres || eint) {
+        if (eint) {
+            F1 = a.phihat[idx];
+            if (pres) { const T pf = a.PF[idx]; F1.x *= pf; F1.y *= pf; }
+        }
+        if (pres) {
+            F1.x += s.x / a.theta;
+            F1.y += s.y / a.theta;
+        }
+    }
     T2 *o[4] = {o0, o1, o2, o3};
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        T2 fb = lin_term(a, g, q, i, j, k, idx);
+    for (int q = 0; q < 3; ++q) {
+        const T cf = diss && svo ? (a.tau + sv) : diss ? a.tau : svo ? sv : (T)0;
+        T2 fb = mk<T2>(cf * u[q].x, cf * u[q].y);
+        if (Tm & T_DIFFUSION) {
+            const T k2 = kx * kx + ky * ky + kz * kz;
+            fb.x += a.D * k2 * u[q].x;
+            fb.y += a.D * k2 * u[q].y;
+        }
+        if (pres || eint) {
+            const T kc = q == 0 ? kx : q == 1 ? ky : kz;
+            const T2 d = mul_ik(F1, kc);
+            fb.x += d.x;
+            fb.y += d.y;
+        }
+        if ((Tm & T_E_EXT) && P) {
+            const T2 d = mul_ik(u[q], kx);
+            fb.x += a.M * d.x;
+            fb.y += a.M * d.y;
+        }
         o[q][idx] = mk<T2>(-fb.x, -fb.y);
+    }
+    {
+        const T cf = (Tm & T_SVISCOSITY) ? sv : (T)0;
+        T2 fb = mk<T2>(cf * s.x, cf * s.y);
+        if (Tm & T_DIFFUSION) {
+            const T k2 = kx * kx + ky * ky + kz * kz;
+            fb.x += a.D * k2 * s.x;
+            fb.y += a.D * k2 * s.y;
+        }
+        if ((Tm & T_E_EXT) && P) {
+            const T2 d = mul_ik(s, kx);
+            fb.x += a.M * d.x;
+            fb.y += a.M * d.y;
+        }
+        if ((Tm & T_CONTINUITY) && P) {
+            const T2 dx = mul_ik(u[0], kx);
+            const T2 dy = mul_ik(u[1], ky);
+            const T2 dz = mul_ik(u[2], kz);
+            fb.x += dx.x; fb.y += dx.y;
+            fb.x += dy.x; fb.y += dy.y;
+            fb.x += dz.x; fb.y += dz.y;
+        }
+        o[3][idx] = mk<T2>(-fb.x, -fb.y);
     }
 }
 
