@@ -47,6 +47,9 @@ def parse():
     ap.add_argument("--no-tune", action="store_true",
                     help="keep the default kernel variants (no kf_autotune; profiling runs)")
     ap.add_argument("--cpu-ref", default="", help=argparse.SUPPRESS)
+    ap.add_argument("--rbgs-rows", type=int, default=-1,
+                    help="force the smoother variant (kf_set_tuning rbgs_rows: 4, 8, 16, or 0 for the "
+                         "streaming sweep) after the autotuner; -1 keeps the autotuner's choice")
     ap.add_argument("--profile-range", action="store_true",
                     help="bracket the first arm's profile steps (launched kernel by kernel, the same "
                          "kernels as the timed graph replays) with cudaProfilerStart/Stop, for "
@@ -317,6 +320,9 @@ def run_kf(args):
         # radix plan and smoother shape, timed on this context
         tune = ctx.autotune() if not args.no_tune else {"fft_plan": 0, "rbgs_rows": 8,
                                                          "fft_radices": [[], []]}
+        if args.rbgs_rows >= 0:
+            ctx.set_tuning(tune["fft_plan"], args.rbgs_rows)
+            tune = dict(tune, rbgs_rows=args.rbgs_rows)
         ctx.rk4(dt, args.warmup)
         ctx.synchronize()
         barrier()

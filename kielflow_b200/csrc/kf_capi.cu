@@ -85,6 +85,7 @@ struct kf_ctx {
     int *d_sweeps = nullptr;
     unsigned long long *d_max = nullptr, *h_max = nullptr;
     int *d_err = nullptr, *h_err = nullptr;  // kernel error word (bit 0: a bounded copy wait gave up)
+    double l2_bytes = 0.;                    // the device's L2 cache (chunked sweeps)
     // RK4 time (Runge_kutta_O4::t_) and the phi history for extrapolated starts
     double t = 0., t_stage = 0.;
     double *phi_a = nullptr;
@@ -511,33 +512,68 @@ void smooth(kf_ctx *c, LevelBuf &L, double *phi, const double *rho, const double
     smooth_plain(c, L, phi, rho, cc, sweeps, cls);
 }
 
-// `sweeps` red-black sweeps as two half-sweep launches each (k_rbgs, or
-// k_rbgs_lin with the adjoint's e^phi)
+// Chunks of a red-black sweep on an n^3 level whose half-sweep reads
+// bytes_pp bytes per point: the smallest power of two G for which one chunk
+// (n/G consecutive i-planes) of those arrays fits in KF_CHUNK_L2 of the L2
+// cache (1 when the whole level does).
+#ifndef KF_CHUNK_L2
+#define KF_CHUNK_L2 0.5
+#endif
+int sweep_chunks(const kf_ctx *c, int n, double bytes_pp) {
+    const double lvl = bytes_pp * (double)n * n * n;
+    int G = 1;
+    while (G < n / 8 && lvl / G > KF_CHUNK_L2 * c->l2_bytes) G *= 2;
+    return G;
+}
+
+// `sweeps` red-black sweeps (k_rbgs, or k_rbgs_lin with the adjoint's e^phi).
+// A level larger than the L2 cache is swept in G chunks of P = n/G i-planes:
+//   red on planes [gP, gP + P), then black on [gP - 1, gP + P - 1) (from 1 for
+//   g = 0), for g = 0 ... G - 1, and last black on planes n - 1 and 0,
+// so the black half-sweep of a chunk reads the potential and the source the
+// red one has just brought into L2.  Each point reads exactly the values of a
+// red sweep over the level followed by a black one (a black point's red
+// neighbours are updated, its black ones not yet), so the potential is that of
+// two whole half-sweeps bit for bit.
 void smooth_plain(kf_ctx *c, LevelBuf &L, double *phi, const double *rho, const double *cc, int sweeps, int cls) {
     const int n = L.n;
-    const long N = (long)n * n * n;
     const int by = c->rbgs_by ? c->rbgs_by : 8;
     const double om = mg_omega(c->cfg);
-    const dim3 g((n / 2 + 31) / 32, (n + by - 1) / by, n), b(32, by);
-    for (int s = 0; s < sweeps; ++s)
-        for (int color = 0; color < 2; ++color) {
-            Launch L_(c, cls, 16. * N);
-            if (cc) {
-                if (by == 4)
-                    k_rbgs_lin<4><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color, om);
-                else if (by == 16)
-                    k_rbgs_lin<16><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color, om);
-                else
-                    k_rbgs_lin<8><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color, om);
-            } else {
-                if (by == 4)
-                    k_rbgs<4><<<g, b, 0, c->st>>>(phi, rho, L.lev(), color, om);
-                else if (by == 16)
-                    k_rbgs<16><<<g, b, 0, c->st>>>(phi, rho, L.lev(), color, om);
-                else
-                    k_rbgs<8><<<g, b, 0, c->st>>>(phi, rho, L.lev(), color, om);
-            }
+    const int G = sweep_chunks(c, n, cc ? 24. : 16.);
+    const int P = n / G;
+    auto half = [&](int color, int i0, int cnt) {
+        if (cnt <= 0) return;
+        Launch L_(c, cls, 16. * cnt * (double)n * n);
+        const dim3 g((n / 2 + 31) / 32, (n + by - 1) / by, cnt), b(32, by);
+        if (cc) {
+            if (by == 4)
+                k_rbgs_lin<4><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color, om, i0);
+            else if (by == 16)
+                k_rbgs_lin<16><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color, om, i0);
+            else
+                k_rbgs_lin<8><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color, om, i0);
+        } else {
+            if (by == 4)
+                k_rbgs<4><<<g, b, 0, c->st>>>(phi, rho, L.lev(), color, om, i0);
+            else if (by == 16)
+                k_rbgs<16><<<g, b, 0, c->st>>>(phi, rho, L.lev(), color, om, i0);
+            else
+                k_rbgs<8><<<g, b, 0, c->st>>>(phi, rho, L.lev(), color, om, i0);
         }
+    };
+    for (int s = 0; s < sweeps; ++s) {
+        if (G == 1) {
+            half(0, 0, n);
+            half(1, 0, n);
+            continue;
+        }
+        for (int gi = 0; gi < G; ++gi) {
+            half(0, gi * P, P);
+            const int lo = gi == 0 ? 1 : gi * P - 1, hi = gi * P + P - 1;
+            half(1, lo, hi - lo);
+        }
+        half(1, n - 1, 2);
+    }
 }
 
 void vcycle(kf_ctx *c, int l);
@@ -1530,6 +1566,12 @@ void build_levels(kf_ctx *c) {
     CK(cudaFuncSetAttribute(k_coarse_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     march_attrs();
     c->march_maps = encode_tiled() != nullptr;  // before the levels: L.t depends on it
+    {
+        int dev = 0, l2 = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev));
+        c->l2_bytes = (double)l2;
+    }
     c->lv.resize(nl);
     for (int l = 0; l < nl; ++l) {
         LevelBuf &L = c->lv[l];

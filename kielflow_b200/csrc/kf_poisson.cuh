@@ -249,13 +249,15 @@ __global__ void k_extrap(double *__restrict__ phi, double *__restrict__ phi_a, d
 }
 
 // Red-black Gauss-Seidel-Newton half sweep (colour (i+j+k)%2): one Newton
-// step per point; grid over (k/2, j, i), blocks of 32 x BY (the tile shape
-// kf_autotune chooses; the arithmetic does not depend on it).
+// step per point; grid over (k/2, j, planes i0 ... i0 + gridDim.z - 1 mod n),
+// blocks of 32 x BY (the tile shape kf_autotune chooses; the arithmetic does
+// not depend on it).
 template <int BY = 8>
 __global__ void __launch_bounds__(32 * BY) k_rbgs(double *__restrict__ phi, const double *__restrict__ rho, Lev L,
-                                                  int color, double om) {
+                                                  int color, double om, int i0 = 0) {
     const int n = L.n;
-    const int k2 = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * BY + threadIdx.y, i = blockIdx.z;
+    const int k2 = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
+    const int i = i0 + (int)blockIdx.z < n ? i0 + (int)blockIdx.z : i0 + (int)blockIdx.z - n;  // planes i0, i0 + 1, ... (mod n)
     if (2 * k2 >= n || j >= n) return;
     const int k = 2 * k2 + ((i + j + color) & 1);
     double A, D;
