@@ -18,6 +18,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/kielflow_b200.h"
 #include "kf_adjoint.cuh"
 #include "kf_graph.cuh"
@@ -161,6 +163,16 @@ struct kf_ctx {
 };
 
 namespace {
+
+// Host-side NVTX range (profiler timelines and ncu --nvtx filters): each RK4
+// stage, each Poisson solve, each replay of a captured step.  Header-only NVTX:
+// without a profiler attached the calls return at once.
+struct NvtxRange {
+    explicit NvtxRange(const char *s) { nvtxRangePushA(s); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 template <typename P> P *dalloc(kf_ctx *c, size_t bytes) {
     void *p = nullptr;
@@ -727,6 +739,7 @@ double read_max_slots(kf_ctx *c) {
 
 // Poisson solve on c->phi with source c->rho.  Returns KF_OK or KF_ERR_NOT_CONVERGED.
 int poisson(kf_ctx *c) {
+    NvtxRange nv("kf Poisson solve");
     const kf_config &cf = c->cfg;
     c->diag.solves++;
     LevelBuf &L0 = c->lv[0];
@@ -1903,7 +1916,9 @@ void rk4_step(kf_ctx *c, double dt, void *const *X, double *const *PH, double *c
     const double ts[4] = {t0, t0 + 0.5 * dt, t0 + 0.5 * dt, t0 + 1.0 * dt};
     const double cdt[4] = {0.5 * dt, 0.5 * dt, 1.0 * dt, dt / 6.};
     const int mode[4] = {0, 1, 1, 2};
+    static const char *const kStage[4] = {"kf RK4 stage 1", "kf RK4 stage 2", "kf RK4 stage 3", "kf RK4 stage 4"};
     for (int i = 0; i < 4; ++i) {
+        NvtxRange nv(kStage[i]);
         c->t_stage = ts[i];
         c->stage_idx = i;
         if (X) copy_state(c, X + 4 * i, c->Ys);
@@ -2008,6 +2023,7 @@ void graph_begin(kf_ctx *c, double dt) {
 }
 
 void graph_step(kf_ctx *c) {
+    NvtxRange nv("kf RK4 step (captured graph)");
     CK(cudaGraphLaunch(c->step_graph, c->st));
     c->launches += c->step_kernels;
 }
