@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -547,7 +548,13 @@ int sweep_chunks(const kf_ctx *c, int n, double bytes_pp) {
 // red sweep over the level followed by a black one (a black point's red
 // neighbours are updated, its black ones not yet), so the potential is that of
 // two whole half-sweeps bit for bit.
-void smooth_plain(kf_ctx *c, LevelBuf &L, double *phi, const double *rho, const double *cc, int sweeps, int cls) {
+//
+// after_black(lo, cnt), when given, runs after every black chunk and after the
+// last launch, with the planes whose potential just became final and whose
+// neighbours are final too: [lo, lo + cnt) (mod n); together they cover the
+// level once.  It runs on the last sweep only.
+void smooth_plain(kf_ctx *c, LevelBuf &L, double *phi, const double *rho, const double *cc, int sweeps, int cls,
+                  const std::function<void(int, int)> &after_black) {
     const int n = L.n;
     const int by = c->rbgs_by ? c->rbgs_by : 8;
     const double om = mg_omega(c->cfg);
@@ -574,18 +581,30 @@ void smooth_plain(kf_ctx *c, LevelBuf &L, double *phi, const double *rho, const 
         }
     };
     for (int s = 0; s < sweeps; ++s) {
+        const bool last = s == sweeps - 1 && after_black;
         if (G == 1) {
             half(0, 0, n);
             half(1, 0, n);
+            if (last) after_black(0, n);
             continue;
         }
+        int done = 2;  // planes [2, done) are handed over; planes 0, 1 and n - 1 come last
         for (int gi = 0; gi < G; ++gi) {
             half(0, gi * P, P);
             const int lo = gi == 0 ? 1 : gi * P - 1, hi = gi * P + P - 1;
             half(1, lo, hi - lo);
+            // final now: planes 1 .. hi - 1; with final neighbours: 2 .. hi - 2
+            if (last && hi - 1 > done) {
+                after_black(done, hi - 1 - done);
+                done = hi - 1;
+            }
         }
         half(1, n - 1, 2);
+        if (last) after_black(done, n - done + 2);  // planes done .. n - 1, 0, 1
     }
+}
+void smooth_plain(kf_ctx *c, LevelBuf &L, double *phi, const double *rho, const double *cc, int sweeps, int cls) {
+    smooth_plain(c, L, phi, rho, cc, sweeps, cls, std::function<void(int, int)>());
 }
 
 void vcycle(kf_ctx *c, int l);
@@ -618,6 +637,23 @@ void vcycle_head(kf_ctx *c, int l, bool with_max) {
         if (with_max) CK(cudaMemsetAsync(c->d_max, 0, 64 * sizeof(unsigned long long), c->st));
         march<MM_SWEEP_RES>(c, L, L.t, L.rho, L.phi, L.r, with_max ? c->d_max : nullptr,
                             l == 0 ? KC_MARCH_RES : KC_MG_COARSE);
+        return;
+    }
+    if (cf.mg_pre >= 1 && sweep_chunks(c, n, 16.) > 1) {
+        // chunked sweeps: the residual of each group of planes right after
+        // the black chunk that finishes them, while they are still in L2
+        if (with_max) CK(cudaMemsetAsync(c->d_max, 0, 64 * sizeof(unsigned long long), c->st));
+        smooth_plain(c, L, L.phi, L.rho, nullptr, cf.mg_pre, l == 0 ? KC_RBGS : KC_MG_COARSE, [&](int i0, int cnt) {
+            Launch L_(c, l == 0 ? KC_RESID : KC_MG_COARSE, 24. * cnt * (double)n * n);
+            dim3 g = mg_grid(n, n);
+            if (with_max) {
+                g.z = cnt < 16 ? cnt : 16;
+                k_residual<true, true><<<g, mg_block(), 0, c->st>>>(L.phi, L.rho, L.lev(), L.r, c->d_max, i0, cnt);
+            } else {
+                g.z = cnt;
+                k_residual<true><<<g, mg_block(), 0, c->st>>>(L.phi, L.rho, L.lev(), L.r, nullptr, i0, cnt);
+            }
+        });
         return;
     }
     smooth(c, L, L.phi, L.rho, nullptr, cf.mg_pre, l == 0 ? KC_RBGS : KC_MG_COARSE);
