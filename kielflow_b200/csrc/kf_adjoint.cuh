@@ -282,11 +282,9 @@ __global__ void __launch_bounds__(BS) k_dot_w(const double *__restrict__ w, cons
 
 template <int BY = 8>
 __global__ void __launch_bounds__(32 * BY) k_rbgs_lin(double *__restrict__ phi, const double *__restrict__ rho,
-                                                      const double *__restrict__ cl, Lev L, int color, double om,
-                                                      int i0 = 0) {
+                                                      const double *__restrict__ cl, Lev L, int color, double om) {
     const int n = L.n;
-    const int k2 = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
-    const int i = i0 + (int)blockIdx.z < n ? i0 + (int)blockIdx.z : i0 + (int)blockIdx.z - n;  // planes i0, ... (mod n)
+    const int k2 = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * BY + threadIdx.y, i = blockIdx.z;
     if (2 * k2 >= n || j >= n) return;
     const int k = 2 * k2 + ((i + j + color) & 1);
     double A, D;

@@ -15,7 +15,6 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
-#include <functional>
 #include <string>
 #include <vector>
 
@@ -88,7 +87,6 @@ struct kf_ctx {
     int *d_sweeps = nullptr;
     unsigned long long *d_max = nullptr, *h_max = nullptr;
     int *d_err = nullptr, *h_err = nullptr;  // kernel error word (bit 0: a bounded copy wait gave up)
-    double l2_bytes = 0.;                    // the device's L2 cache (chunked sweeps)
     // RK4 time (Runge_kutta_O4::t_) and the phi history for extrapolated starts
     double t = 0., t_stage = 0.;
     double *phi_a = nullptr;
@@ -525,86 +523,36 @@ void smooth(kf_ctx *c, LevelBuf &L, double *phi, const double *rho, const double
     smooth_plain(c, L, phi, rho, cc, sweeps, cls);
 }
 
-// Chunks of a red-black sweep on an n^3 level whose half-sweep reads
-// bytes_pp bytes per point: the smallest power of two G for which one chunk
-// (n/G consecutive i-planes) of those arrays fits in KF_CHUNK_L2 of the L2
-// cache (1 when the whole level does).
-#ifndef KF_CHUNK_L2
-#define KF_CHUNK_L2 0.5
-#endif
-int sweep_chunks(const kf_ctx *c, int n, double bytes_pp) {
-    const double lvl = bytes_pp * (double)n * n * n;
-    int G = 1;
-    while (G < n / 8 && lvl / G > KF_CHUNK_L2 * c->l2_bytes) G *= 2;
-    return G;
-}
-
-// `sweeps` red-black sweeps (k_rbgs, or k_rbgs_lin with the adjoint's e^phi).
-// A level larger than the L2 cache is swept in G chunks of P = n/G i-planes:
-//   red on planes [gP, gP + P), then black on [gP - 1, gP + P - 1) (from 1 for
-//   g = 0), for g = 0 ... G - 1, and last black on planes n - 1 and 0,
-// so the black half-sweep of a chunk reads the potential and the source the
-// red one has just brought into L2.  Each point reads exactly the values of a
-// red sweep over the level followed by a black one (a black point's red
-// neighbours are updated, its black ones not yet), so the potential is that of
-// two whole half-sweeps bit for bit.
-//
-// after_black(lo, cnt), when given, runs after every black chunk and after the
-// last launch, with the planes whose potential just became final and whose
-// neighbours are final too: [lo, lo + cnt) (mod n); together they cover the
-// level once.  It runs on the last sweep only.
-void smooth_plain(kf_ctx *c, LevelBuf &L, double *phi, const double *rho, const double *cc, int sweeps, int cls,
-                  const std::function<void(int, int)> &after_black) {
+// `sweeps` red-black sweeps as two half-sweep launches each (k_rbgs, or
+// k_rbgs_lin with the adjoint's e^phi).  (Sweeping a level larger than L2 in
+// chunks of i-planes, black one plane behind red so that the black half finds
+// its data in L2, gives the same potentials bit for bit but measured slower at
+// 256^3: 156 / 169 / 181 / 214 us per sweep for 1 / 2 / 4 / 8 chunks.)
+void smooth_plain(kf_ctx *c, LevelBuf &L, double *phi, const double *rho, const double *cc, int sweeps, int cls) {
     const int n = L.n;
+    const long N = (long)n * n * n;
     const int by = c->rbgs_by ? c->rbgs_by : 8;
     const double om = mg_omega(c->cfg);
-    const int G = sweep_chunks(c, n, cc ? 24. : 16.);
-    const int P = n / G;
-    auto half = [&](int color, int i0, int cnt) {
-        if (cnt <= 0) return;
-        Launch L_(c, cls, 16. * cnt * (double)n * n);
-        const dim3 g((n / 2 + 31) / 32, (n + by - 1) / by, cnt), b(32, by);
-        if (cc) {
-            if (by == 4)
-                k_rbgs_lin<4><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color, om, i0);
-            else if (by == 16)
-                k_rbgs_lin<16><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color, om, i0);
-            else
-                k_rbgs_lin<8><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color, om, i0);
-        } else {
-            if (by == 4)
-                k_rbgs<4><<<g, b, 0, c->st>>>(phi, rho, L.lev(), color, om, i0);
-            else if (by == 16)
-                k_rbgs<16><<<g, b, 0, c->st>>>(phi, rho, L.lev(), color, om, i0);
-            else
-                k_rbgs<8><<<g, b, 0, c->st>>>(phi, rho, L.lev(), color, om, i0);
-        }
-    };
-    for (int s = 0; s < sweeps; ++s) {
-        const bool last = s == sweeps - 1 && after_black;
-        if (G == 1) {
-            half(0, 0, n);
-            half(1, 0, n);
-            if (last) after_black(0, n);
-            continue;
-        }
-        int done = 2;  // planes [2, done) are handed over; planes 0, 1 and n - 1 come last
-        for (int gi = 0; gi < G; ++gi) {
-            half(0, gi * P, P);
-            const int lo = gi == 0 ? 1 : gi * P - 1, hi = gi * P + P - 1;
-            half(1, lo, hi - lo);
-            // final now: planes 1 .. hi - 1; with final neighbours: 2 .. hi - 2
-            if (last && hi - 1 > done) {
-                after_black(done, hi - 1 - done);
-                done = hi - 1;
+    const dim3 g((n / 2 + 31) / 32, (n + by - 1) / by, n), b(32, by);
+    for (int s = 0; s < sweeps; ++s)
+        for (int color = 0; color < 2; ++color) {
+            Launch L_(c, cls, 16. * N);
+            if (cc) {
+                if (by == 4)
+                    k_rbgs_lin<4><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color, om);
+                else if (by == 16)
+                    k_rbgs_lin<16><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color, om);
+                else
+                    k_rbgs_lin<8><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color, om);
+            } else {
+                if (by == 4)
+                    k_rbgs<4><<<g, b, 0, c->st>>>(phi, rho, L.lev(), color, om);
+                else if (by == 16)
+                    k_rbgs<16><<<g, b, 0, c->st>>>(phi, rho, L.lev(), color, om);
+                else
+                    k_rbgs<8><<<g, b, 0, c->st>>>(phi, rho, L.lev(), color, om);
             }
         }
-        half(1, n - 1, 2);
-        if (last) after_black(done, n - done + 2);  // planes done .. n - 1, 0, 1
-    }
-}
-void smooth_plain(kf_ctx *c, LevelBuf &L, double *phi, const double *rho, const double *cc, int sweeps, int cls) {
-    smooth_plain(c, L, phi, rho, cc, sweeps, cls, std::function<void(int, int)>());
 }
 
 void vcycle(kf_ctx *c, int l);
@@ -637,23 +585,6 @@ void vcycle_head(kf_ctx *c, int l, bool with_max) {
         if (with_max) CK(cudaMemsetAsync(c->d_max, 0, 64 * sizeof(unsigned long long), c->st));
         march<MM_SWEEP_RES>(c, L, L.t, L.rho, L.phi, L.r, with_max ? c->d_max : nullptr,
                             l == 0 ? KC_MARCH_RES : KC_MG_COARSE);
-        return;
-    }
-    if (cf.mg_pre >= 1 && sweep_chunks(c, n, 16.) > 1) {
-        // chunked sweeps: the residual of each group of planes right after
-        // the black chunk that finishes them, while they are still in L2
-        if (with_max) CK(cudaMemsetAsync(c->d_max, 0, 64 * sizeof(unsigned long long), c->st));
-        smooth_plain(c, L, L.phi, L.rho, nullptr, cf.mg_pre, l == 0 ? KC_RBGS : KC_MG_COARSE, [&](int i0, int cnt) {
-            Launch L_(c, l == 0 ? KC_RESID : KC_MG_COARSE, 24. * cnt * (double)n * n);
-            dim3 g = mg_grid(n, n);
-            if (with_max) {
-                g.z = cnt < 16 ? cnt : 16;
-                k_residual<true, true><<<g, mg_block(), 0, c->st>>>(L.phi, L.rho, L.lev(), L.r, c->d_max, i0, cnt);
-            } else {
-                g.z = cnt;
-                k_residual<true><<<g, mg_block(), 0, c->st>>>(L.phi, L.rho, L.lev(), L.r, nullptr, i0, cnt);
-            }
-        });
         return;
     }
     smooth(c, L, L.phi, L.rho, nullptr, cf.mg_pre, l == 0 ? KC_RBGS : KC_MG_COARSE);
@@ -1074,7 +1005,7 @@ template <typename T, int N> struct Impl {
             int dev = 0, sms = 0, per = 0;
             CK(cudaGetDevice(&dev));
             CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-            const size_t smem = 2 * (size_t)N * TC * sizeof(T2);
+            const size_t smem = axis_pipe_smem<T, N>(32);
             if (sign < 0)
                 CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_axis_pipe<T, N, -1, V>, TC * PV<V>, smem));
             else
@@ -1086,7 +1017,7 @@ template <typename T, int N> struct Impl {
     template <int V> static void axis_v(kf_ctx *c, int off, int njobs, int ax, int sign) {
         const int ntiles = ax == 0 ? (N * NZC + TC - 1) / TC : N * ((NZC + TC - 1) / TC);
         const int total = njobs * ntiles, grid = std::min(total, pipe_grid<V>(sign));
-        const size_t smem = 2 * (size_t)N * TC * sizeof(T2);
+        const size_t smem = axis_pipe_smem<T, N>(njobs);
         if (sign < 0)
             k_axis_pipe<T, N, -1, V><<<grid, TC * PV<V>, smem, c->st>>>(c->dj + off, njobs, ax, geo(c),
                                                                       (const T2 *)c->tw, total);
@@ -1121,8 +1052,7 @@ template <typename T, int N> struct Impl {
     static void zc2r(kf_ctx *c, int off, int njobs, double scale = -1.) {
         const int nrows = N * N;
         const int ntiles = (nrows + LZ - 1) / LZ;
-        const size_t smem = (size_t)(2 * LZ * NZC > LZ * PadLen<N>::value ? 2 * LZ * NZC : LZ * PadLen<N>::value) *
-                            sizeof(T2);
+        const size_t smem = ZSmem<T, N, true>::bytes;
         Launch L_(c, KC_Z_C2R, z_bytes(c, off, njobs, true));
         const T sc = (T)(scale < 0. ? 1. / ((double)N * N * N) : scale);
         if (c->fftv)
@@ -1135,7 +1065,7 @@ template <typename T, int N> struct Impl {
     static void zr2c(kf_ctx *c, int off, int njobs) {
         const int nrows = N * N;
         const int ntiles = (nrows + LZ - 1) / LZ;
-        const size_t smem = (size_t)(LZ * PadLen<N>::value) * sizeof(T2);
+        const size_t smem = ZSmem<T, N, false>::bytes;
         Launch L_(c, KC_Z_R2C, z_bytes(c, off, njobs, false));
         if (c->fftv)
             k_z_r2c<T, N, 1><<<njobs * ntiles, LZ * PV<1>, smem, c->st>>>(c->dz + off, njobs, nrows, (const T2 *)c->tw);
@@ -1615,12 +1545,6 @@ void build_levels(kf_ctx *c) {
     CK(cudaFuncSetAttribute(k_coarse_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     march_attrs();
     c->march_maps = encode_tiled() != nullptr;  // before the levels: L.t depends on it
-    {
-        int dev = 0, l2 = 0;
-        CK(cudaGetDevice(&dev));
-        CK(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev));
-        c->l2_bytes = (double)l2;
-    }
     c->lv.resize(nl);
     for (int l = 0; l < nl; ++l) {
         LevelBuf &L = c->lv[l];

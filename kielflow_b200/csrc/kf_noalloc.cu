@@ -105,7 +105,7 @@ cudaError_t run(const double *in, double *out, unsigned char *scratch, cudaStrea
     constexpr int NZC = N / 2 + 1, LZ = ZTile<double>::LZ, P = Plan<N>::P, TC = Tile<double>::TC;
     const Geo<double> g{N, NZC, nullptr, nullptr, 0.};  // no multipliers: the axis tables are not read
     const int nrows = N * N;
-    k_z_r2c<double, N><<<(nrows + LZ - 1) / LZ, LZ * P, (size_t)LZ * PadLen<N>::value * sizeof(double2), st>>>(
+    k_z_r2c<double, N><<<(nrows + LZ - 1) / LZ, LZ * P, ZSmem<double, N, false>::bytes, st>>>(
         zj, 1, nrows, tw);
     const size_t smem = (size_t)N * TC * sizeof(double2);
     k_axis_pass<double, N, -1><<<N * ((NZC + TC - 1) / TC), TC * P, smem, st>>>(aj, 1, 1, g, tw);

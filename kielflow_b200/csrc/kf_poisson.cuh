@@ -174,24 +174,20 @@ __global__ void __launch_bounds__(BS) k_reduce_final(const double *__restrict__ 
 inline dim3 mg_grid(int nx, int n) { return dim3((nx + 31) / 32, (n + 7) / 8, n); }
 inline dim3 mg_block() { return dim3(32, 8, 1); }
 
-// Pointwise residual r = f(phi) = lap_h phi + rho - e^phi on the planes i0 ...
-// i0 + cnt - 1 (mod n; cnt < 0: the whole level); with MAX also max |r|, so
-// that the convergence test of a cycle needs no pass of its own: each block
-// then covers the planes i0 + blockIdx.z, i0 + blockIdx.z + gridDim.z, ...
-// (launched with gridDim.z <= 16), takes the block maximum and makes one atomic
-// max on the IEEE bit pattern into one of 64 slots.
+// Pointwise residual r = f(phi) = lap_h phi + rho - e^phi on the whole level;
+// with MAX also max |r|, so that the convergence test of a cycle needs no pass
+// of its own: each block then covers the i-planes blockIdx.z, blockIdx.z +
+// gridDim.z, ... (launched with gridDim.z <= 16), takes the block
+// maximum and makes one atomic max on the IEEE bit pattern into one of 64 slots.
 template <bool FAST, bool MAX = false>
 __global__ void __launch_bounds__(256) k_residual(const double *__restrict__ phi, const double *__restrict__ rho,
                                                   Lev L, double *__restrict__ r,
-                                                  unsigned long long *__restrict__ slots = nullptr, int i0 = 0,
-                                                  int cnt = -1) {
+                                                  unsigned long long *__restrict__ slots = nullptr) {
     const int n = L.n;
     const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y;
-    if (cnt < 0) cnt = n;  // planes i0 ... i0 + cnt - 1 (mod n)
     double af = 0.;
     if (k < n && j < n) {
-        for (int ii = blockIdx.z; ii < cnt; ii += (MAX ? gridDim.z : cnt)) {
-            const int i = i0 + ii < n ? i0 + ii : i0 + ii - n;
+        for (int i = blockIdx.z; i < n; i += (MAX ? gridDim.z : n)) {
             double A, D;
             coeffs_t<FAST>(phi, rho, L, i, j, k, A, D);
             const long id = lidx(i, j, k, n);
@@ -253,15 +249,13 @@ __global__ void k_extrap(double *__restrict__ phi, double *__restrict__ phi_a, d
 }
 
 // Red-black Gauss-Seidel-Newton half sweep (colour (i+j+k)%2): one Newton
-// step per point; grid over (k/2, j, planes i0 ... i0 + gridDim.z - 1 mod n),
-// blocks of 32 x BY (the tile shape kf_autotune chooses; the arithmetic does
-// not depend on it).
+// step per point; grid over (k/2, j, i), blocks of 32 x BY (the tile shape
+// kf_autotune chooses; the arithmetic does not depend on it).
 template <int BY = 8>
 __global__ void __launch_bounds__(32 * BY) k_rbgs(double *__restrict__ phi, const double *__restrict__ rho, Lev L,
-                                                  int color, double om, int i0 = 0) {
+                                                  int color, double om) {
     const int n = L.n;
-    const int k2 = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
-    const int i = i0 + (int)blockIdx.z < n ? i0 + (int)blockIdx.z : i0 + (int)blockIdx.z - n;  // planes i0, i0 + 1, ... (mod n)
+    const int k2 = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * BY + threadIdx.y, i = blockIdx.z;
     if (2 * k2 >= n || j >= n) return;
     const int k = 2 * k2 + ((i + j + color) & 1);
     double A, D;
