@@ -528,16 +528,30 @@ void smooth(kf_ctx *c, LevelBuf &L, double *phi, const double *rho, const double
 // chunks of i-planes, black one plane behind red so that the black half finds
 // its data in L2, gives the same potentials bit for bit but measured slower at
 // 256^3: 156 / 169 / 181 / 214 us per sweep for 1 / 2 / 4 / 8 chunks.)
+// Levels on which the column forms of the half sweep and the residual run
+// (whole warps along k, columns of COL_PI planes).
+constexpr int COL_PI = 8;
+bool col_level(int n) { return n >= 64 && n % 64 == 0 && n % COL_PI == 0; }
+
 void smooth_plain(kf_ctx *c, LevelBuf &L, double *phi, const double *rho, const double *cc, int sweeps, int cls) {
     const int n = L.n;
     const long N = (long)n * n * n;
     const int by = c->rbgs_by ? c->rbgs_by : 8;
     const double om = mg_omega(c->cfg);
     const dim3 g((n / 2 + 31) / 32, (n + by - 1) / by, n), b(32, by);
+    const dim3 gc(n / 64, n / by, n / COL_PI);
+    const bool col = !cc && col_level(n);
     for (int s = 0; s < sweeps; ++s)
         for (int color = 0; color < 2; ++color) {
             Launch L_(c, cls, 16. * N);
-            if (cc) {
+            if (col) {
+                if (by == 4)
+                    k_rbgs_col<4, COL_PI><<<gc, b, 0, c->st>>>(phi, rho, L.lev(), color, om);
+                else if (by == 16)
+                    k_rbgs_col<16, COL_PI><<<gc, b, 0, c->st>>>(phi, rho, L.lev(), color, om);
+                else
+                    k_rbgs_col<8, COL_PI><<<gc, b, 0, c->st>>>(phi, rho, L.lev(), color, om);
+            } else if (cc) {
                 if (by == 4)
                     k_rbgs_lin<4><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color, om);
                 else if (by == 16)
@@ -590,7 +604,13 @@ void vcycle_head(kf_ctx *c, int l, bool with_max) {
     smooth(c, L, L.phi, L.rho, nullptr, cf.mg_pre, l == 0 ? KC_RBGS : KC_MG_COARSE);
     if (with_max) CK(cudaMemsetAsync(c->d_max, 0, 64 * sizeof(unsigned long long), c->st));
     Launch L_(c, l == 0 ? KC_RESID : KC_MG_COARSE, 24. * N);
-    if (with_max) {
+    if (col_level(n)) {
+        const dim3 gc(n / 64, n / 8, n / COL_PI);
+        if (with_max)
+            k_residual_col<8, COL_PI, true><<<gc, mg_block(), 0, c->st>>>(L.phi, L.rho, L.lev(), L.r, c->d_max);
+        else
+            k_residual_col<8, COL_PI, false><<<gc, mg_block(), 0, c->st>>>(L.phi, L.rho, L.lev(), L.r, nullptr);
+    } else if (with_max) {
         dim3 g = mg_grid(n, n);
         g.z = n < 16 ? n : 16;  // each block strides over n/16 i-planes (ncu, 256^3: 158 us; 64 groups 169 us)
         k_residual<true, true><<<g, mg_block(), 0, c->st>>>(L.phi, L.rho, L.lev(), L.r, c->d_max);

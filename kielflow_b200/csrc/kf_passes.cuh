@@ -166,16 +166,17 @@ template <typename T, int N, int V, int TILES, int CAP, int FLOOR> struct PipeMi
     static constexpr int value = lim < 1 ? 1 : (lim < CAP ? (int)lim : CAP);
 };
 
-// Shared memory of a k_axis_pipe launch with njobs jobs: exchange and staging
-// tiles, the twiddle table, the axis k values and the job descriptors.
-template <typename T, int N> inline size_t axis_pipe_smem(int njobs) {
-    typedef typename C2<T>::type T2;
-    return 2 * (size_t)N * Tile<T>::TC * sizeof(T2) + (size_t)N * (sizeof(T2) + sizeof(T)) +
-           (size_t)njobs * sizeof(AxisJob) + 16;
+// Shared memory of a k_axis_pipe launch: exchange and staging tiles.  (Held
+// to fewer registers for three resident blocks, or with its twiddles, k values
+// and job descriptors staged in shared memory, the pass measured no faster:
+// 12.5 and 13.8 ms against 12.4 ms for 48 launches; it is bound by the latency
+// of its loads, not by occupancy.)
+template <typename T, int N> inline size_t axis_pipe_smem(int) {
+    return 2 * (size_t)N * Tile<T>::TC * sizeof(typename C2<T>::type);
 }
 
 template <typename T, int N, int SIGN, int V = 0>
-__global__ void __launch_bounds__(Tile<T>::TC * PlanV<N, V>::P, (PipeMinBlocks<T, N, V, 2, 3, 64>::value))
+__global__ void __launch_bounds__(Tile<T>::TC * PlanV<N, V>::P)
 k_axis_pipe(const AxisJob *__restrict__ jobs, int njobs, int axis, Geo<T> g,
             const typename C2<T>::type *__restrict__ tw, int total) {
     typedef typename C2<T>::type T2;
@@ -183,24 +184,10 @@ k_axis_pipe(const AxisJob *__restrict__ jobs, int njobs, int axis, Geo<T> g,
     extern __shared__ __align__(16) unsigned char kf_smem[];
     T2 *sm = reinterpret_cast<T2 *>(kf_smem);  // exchange [N][TC]
     T2 *stg = sm + N * TC;                      // staging  [N][TC]
-    T2 *stw = stg + N * TC;                     // twiddles W_N^m [N]
-    T *skv = reinterpret_cast<T *>(stw + N);    // k_val_at [N]
-    AxisJob *sjob = reinterpret_cast<AxisJob *>(
-        (reinterpret_cast<uintptr_t>(skv + N) + 15) & ~(uintptr_t)15);  // job descriptors [njobs]
     const int c = threadIdx.x % TC, p = threadIdx.x / TC;
     int t = blockIdx.x;
     if (t >= total) return;
-    // the tables every tile reads, once per (persistent) block: the loads of
-    // the loop then wait on shared memory, not on L1/L2
-    for (int i = threadIdx.x; i < N; i += blockDim.x) {
-        stw[i] = tw[i];
-        skv[i] = g.kv ? g.kv[i] : (T)0;
-    }
-    for (int i = threadIdx.x; i < njobs; i += blockDim.x) sjob[i] = jobs[i];
-    __syncthreads();
-    const SharedTw<T2> stwp{stw};
-    auto prefetch = [&](int tt) {
-        const AxisTile<T> G = axis_tile<T, N>(sjob, njobs, axis, tt, c, g.n, g.nzc);
+    auto prefetch = [&](const AxisTile<T> &G) {
 #pragma unroll
         for (int q = 0; q < E; ++q) {
             const int row = reg_row<N, P, PlanV<N, V>::R1>(p, q);
@@ -212,26 +199,26 @@ k_axis_pipe(const AxisJob *__restrict__ jobs, int njobs, int axis, Geo<T> g,
         }
         cp_async_commit();
     };
-    AxisTile<T> cur = axis_tile<T, N>(sjob, njobs, axis, t, c, g.n, g.nzc);
-    prefetch(t);
+    AxisTile<T> cur = axis_tile<T, N>(jobs, njobs, axis, t, c, g.n, g.nzc);
+    prefetch(cur);
     for (; t < total; t += gridDim.x) {
+        const int tn = t + gridDim.x;
+        AxisTile<T> nxt = cur;
+        if (tn < total) nxt = axis_tile<T, N>(jobs, njobs, axis, tn, c, g.n, g.nzc);
         cp_async_wait_all();
         T2 v[E];
-        {
-            const bool pm = cur.mul == MUL_P || cur.mul == MUL_P_IK;
-            const int b = pm ? dealias_bound(g.pb, cur.jj, cur.kk, g.nzc) : -2;
 #pragma unroll
-            for (int q = 0; q < E; ++q) {
-                const int row = reg_row<N, P, PlanV<N, V>::R1>(p, q);
-                T2 x = stg[row * TC + c];
-                if (pm && !dealias_keep_b(g.q2, g.thr, b, N, row, cur.jj, cur.kk)) x = mk<T2>((T)0, (T)0);
-                if (cur.mul == MUL_P_IK || cur.mul == MUL_IK) x = mul_ik(x, skv[row]);
-                v[q] = x;
+        for (int q = 0; q < E; ++q) {
+            const int row = reg_row<N, P, PlanV<N, V>::R1>(p, q);
+            T2 x = stg[row * TC + c];
+            if (cur.mul == MUL_P || cur.mul == MUL_P_IK) {
+                if (!dealias_keep(g.q2, g.thr, row, cur.jj, cur.kk)) x = mk<T2>((T)0, (T)0);
             }
+            if (cur.mul == MUL_P_IK || cur.mul == MUL_IK) x = mul_ik(x, g.kv[row]);
+            v[q] = x;
         }
-        const int tn = t + gridDim.x;
-        if (tn < total) prefetch(tn);
-        PlanV<N, V>::template fft<T2, SIGN>(v, sm + c, StrideAddr{TC}, p, stwp);
+        if (tn < total) prefetch(nxt);
+        PlanV<N, V>::template fft<T2, SIGN>(v, sm + c, StrideAddr{TC}, p, tw);
         if (cur.valid) {
 #pragma unroll
             for (int q = 0; q < E; ++q) {
@@ -239,7 +226,7 @@ k_axis_pipe(const AxisJob *__restrict__ jobs, int njobs, int axis, Geo<T> g,
                 cur.out[cur.base + row * cur.rstride] = v[q];
             }
         }
-        if (tn < total) cur = axis_tile<T, N>(sjob, njobs, axis, tn, c, g.n, g.nzc);
+        cur = nxt;
     }
 }
 
@@ -251,14 +238,13 @@ k_axis_pipe(const AxisJob *__restrict__ jobs, int njobs, int axis, Geo<T> g,
 // `scale` (the 1/N of OP_iFFT.cpp:59-61).
 template <typename T> struct ZTile { static constexpr int LZ = 8; };
 
-// Elements (T2) of a z pass's line buffers, and its shared memory with the
-// twiddle table and the axis k values staged after them (read by every
-// element's multiplier and every radix stage).
+// Shared memory of a z pass: its line buffers (the c2r staging of two half
+// spectra per line pair, reused by the transform).
 template <typename T, int N, bool C2R> struct ZSmem {
     typedef typename C2<T>::type T2;
     static constexpr int LZ = ZTile<T>::LZ, NZC = N / 2 + 1, LS = PadLen<N>::value;
     static constexpr int lines = C2R ? (2 * LZ * NZC > LZ * LS ? 2 * LZ * NZC : LZ * LS) : LZ * LS;
-    static constexpr size_t bytes = (size_t)lines * sizeof(T2) + (size_t)N * (sizeof(T2) + sizeof(T));
+    static constexpr size_t bytes = (size_t)lines * sizeof(T2);
 };
 
 template <typename T, int N, int V = 0>
@@ -271,12 +257,6 @@ k_z_c2r(const ZJob *__restrict__ jobs, int njobs, int nrows, Geo<T> g,
     extern __shared__ __align__(16) unsigned char kf_smem[];
     T2 *half = reinterpret_cast<T2 *>(kf_smem);  // [2][LZ][NZC], staging of the half spectra
     T2 *xch = half;                              // [LZ][LS], reused by the transform once staged
-    T2 *stw = half + ZSmem<T, N, true>::lines;   // twiddles [N]
-    T *skv = reinterpret_cast<T *>(stw + N);     // k_val_at [N]
-    for (int i = threadIdx.x; i < N; i += blockDim.x) {
-        stw[i] = tw[i];
-        skv[i] = g.kv ? g.kv[i] : (T)0;
-    }
     const int job = blockIdx.x % njobs, tile = blockIdx.x / njobs;
     const ZJob J = jobs[job];
     const int r0 = tile * LZ;
@@ -305,7 +285,7 @@ k_z_c2r(const ZJob *__restrict__ jobs, int njobs, int nrows, Geo<T> g,
     // imaginary parts of the kz = 0 and kz = n/2 bins dropped
     auto staged = [&](const T2 *h, int kk, int mul) {
         T2 x = h[kk];
-        if (mul == MUL_IK) x = mul_ik(x, skv[kk]);
+        if (mul == MUL_IK) x = mul_ik(x, g.kv[kk]);
         if (mul == MUL_HALF && kk > 0 && 2 * kk < N) x = mk<T2>((T)0.5 * x.x, (T)0.5 * x.y);
         if (kk == 0 || 2 * kk == N) x.y = (T)0;
         return x;
@@ -327,7 +307,7 @@ k_z_c2r(const ZJob *__restrict__ jobs, int njobs, int nrows, Geo<T> g,
         v[q] = mk<T2>(a.x - b.y, a.y + b.x);  // A + iB
     }
     __syncthreads();  // staging consumed: the exchange buffer may overwrite it
-    PlanV<N, V>::template fft<T2, +1>(v, xch + l * LS, PadAddr{}, p, SharedTw<T2>{stw});
+    PlanV<N, V>::template fft<T2, +1>(v, xch + l * LS, PadAddr{}, p, tw);
     const int r = r0 + l;
     if (r < nrows) {
         T *oA = static_cast<T *>(J.outA) + (long)r * N;
@@ -351,9 +331,6 @@ k_z_r2c(const ZJob *__restrict__ jobs, int njobs, int nrows,
     constexpr int LS = PadLen<N>::value;
     extern __shared__ __align__(16) unsigned char kf_smem[];
     T2 *xch = reinterpret_cast<T2 *>(kf_smem);  // [LZ][LS], padded lines
-    T2 *stw = xch + ZSmem<T, N, false>::lines;   // twiddles [N]
-    for (int i = threadIdx.x; i < N; i += blockDim.x) stw[i] = tw[i];
-    __syncthreads();
     const int job = blockIdx.x % njobs, tile = blockIdx.x / njobs;
     const ZJob J = jobs[job];
     const int r0 = tile * LZ;
@@ -374,7 +351,7 @@ k_z_r2c(const ZJob *__restrict__ jobs, int njobs, int nrows,
     }
     T2 *line = xch + l * LS;
     const PadAddr pa;
-    PlanV<N, V>::template fft<T2, -1>(v, line, pa, p, SharedTw<T2>{stw});
+    PlanV<N, V>::template fft<T2, -1>(v, line, pa, p, tw);
     __syncthreads();
 #pragma unroll
     for (int q = 0; q < E; ++q) line[pa(reg_row<N, P, PlanV<N, V>::RL>(p, q))] = v[q];
