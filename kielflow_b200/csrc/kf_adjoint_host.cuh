@@ -251,7 +251,11 @@ void avcycle(kf_ctx *c, int l) {
     smooth(c, L, A.psi, A.b, A.cc, cf.mg_pre, KC_ADJ_MG);
     {
         Launch L_(c, KC_ADJ_MG, 32. * N);
-        k_residual_lin<<<mg_grid(n, n), mg_block(), 0, c->st>>>(A.psi, A.b, A.cc, L.lev(), A.r);
+        if (col_level(n))
+            k_residual_col<8, COL_PI, false, true><<<dim3(n / 64, n / 8, n / COL_PI), mg_block(), 0, c->st>>>(
+                A.psi, A.b, L.lev(), A.r, nullptr, A.cc);
+        else
+            k_residual_lin<<<mg_grid(n, n), mg_block(), 0, c->st>>>(A.psi, A.b, A.cc, L.lev(), A.r);
     }
     LevelBuf &Lc = c->lv[l + 1];
     const ALev C = alev(c, l + 1);
@@ -317,7 +321,11 @@ double adj_resmax(kf_ctx *c) {
         Launch L_(c, KC_ADJ_MG, 24. * c->N);
         dim3 g = mg_grid(L.n, L.n);
         g.z = L.n < 16 ? L.n : 16;
-        k_resmax_lin<<<g, mg_block(), 0, c->st>>>(a.rhob, a.phibar, a.c0, L.lev(), c->d_max);
+        if (col_level(L.n))
+            k_residual_col<8, COL_PI, true, true, false><<<dim3(L.n / 64, L.n / 8, L.n / COL_PI), mg_block(), 0, c->st>>>(
+                a.rhob, a.phibar, L.lev(), nullptr, c->d_max, a.c0);
+        else
+            k_resmax_lin<<<g, mg_block(), 0, c->st>>>(a.rhob, a.phibar, a.c0, L.lev(), c->d_max);
     }
     CK(cudaGetLastError());
     return read_max64(c);

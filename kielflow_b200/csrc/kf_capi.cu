@@ -348,6 +348,14 @@ int red_blocks(long N) {
     return (int)(nb < 1184 ? nb : 1184);
 }
 
+// Levels on which the column form of the residual runs (whole warps along k,
+// columns of COL_PI planes).  At 256^3 (one B200): 99.6 us against 155.9 us for
+// k_residual<1, 1>; the column form of the half sweep measured slower (201-225
+// us per sweep against 150 us: its per-thread chain of Newton steps is
+// latency-bound), so the half sweep stays one point per thread.
+constexpr int COL_PI = 16;
+bool col_level(int n) { return n >= 64 && n % 64 == 0 && n % COL_PI == 0; }
+
 // The kernel error word: queued for reading before a synchronisation
 // (kerr_fetch) and checked after it (kerr_check, which clears it)
 void kerr_fetch(kf_ctx *c) {
@@ -368,7 +376,10 @@ double max_residual(kf_ctx *c, const LevelBuf &L, const double *phi, const doubl
         Launch L_(c, KC_RESID, 16. * N);
         dim3 g = mg_grid(L.n, L.n);
         g.z = L.n < 16 ? L.n : 16;  // each block strides over the i-planes
-        if (fast)
+        if (fast && col_level(L.n))
+            k_residual_col<8, COL_PI, true, false, false>
+                <<<dim3(L.n / 64, L.n / 8, L.n / COL_PI), mg_block(), 0, c->st>>>(phi, rho, L.lev(), nullptr, c->d_max);
+        else if (fast)
             k_resmax<true><<<g, mg_block(), 0, c->st>>>(phi, rho, L.lev(), c->d_max);
         else
             k_resmax<false><<<g, mg_block(), 0, c->st>>>(phi, rho, L.lev(), c->d_max);
@@ -528,10 +539,6 @@ void smooth(kf_ctx *c, LevelBuf &L, double *phi, const double *rho, const double
 // chunks of i-planes, black one plane behind red so that the black half finds
 // its data in L2, gives the same potentials bit for bit but measured slower at
 // 256^3: 156 / 169 / 181 / 214 us per sweep for 1 / 2 / 4 / 8 chunks.)
-// Levels on which the column forms of the half sweep and the residual run
-// (whole warps along k, columns of COL_PI planes).
-constexpr int COL_PI = 8;
-bool col_level(int n) { return n >= 64 && n % 64 == 0 && n % COL_PI == 0; }
 
 void smooth_plain(kf_ctx *c, LevelBuf &L, double *phi, const double *rho, const double *cc, int sweeps, int cls) {
     const int n = L.n;
@@ -539,19 +546,10 @@ void smooth_plain(kf_ctx *c, LevelBuf &L, double *phi, const double *rho, const 
     const int by = c->rbgs_by ? c->rbgs_by : 8;
     const double om = mg_omega(c->cfg);
     const dim3 g((n / 2 + 31) / 32, (n + by - 1) / by, n), b(32, by);
-    const dim3 gc(n / 64, n / by, n / COL_PI);
-    const bool col = !cc && col_level(n);
     for (int s = 0; s < sweeps; ++s)
         for (int color = 0; color < 2; ++color) {
             Launch L_(c, cls, 16. * N);
-            if (col) {
-                if (by == 4)
-                    k_rbgs_col<4, COL_PI><<<gc, b, 0, c->st>>>(phi, rho, L.lev(), color, om);
-                else if (by == 16)
-                    k_rbgs_col<16, COL_PI><<<gc, b, 0, c->st>>>(phi, rho, L.lev(), color, om);
-                else
-                    k_rbgs_col<8, COL_PI><<<gc, b, 0, c->st>>>(phi, rho, L.lev(), color, om);
-            } else if (cc) {
+            if (cc) {
                 if (by == 4)
                     k_rbgs_lin<4><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color, om);
                 else if (by == 16)
@@ -932,7 +930,12 @@ void poisson_captured(kf_ctx *c) {
         Launch L_(c, KC_RESID, 16. * c->N);
         dim3 g = mg_grid(L0.n, L0.n);
         g.z = L0.n < 16 ? L0.n : 16;
-        k_resmax<true><<<g, mg_block(), 0, st>>>(c->phi, c->rho, L0.lev(), c->d_max);
+        if (col_level(L0.n))
+            k_residual_col<8, COL_PI, true, false, false>
+                <<<dim3(L0.n / 64, L0.n / 8, L0.n / COL_PI), mg_block(), 0, st>>>(c->phi, c->rho, L0.lev(), nullptr,
+                                                                                  c->d_max);
+        else
+            k_resmax<true><<<g, mg_block(), 0, st>>>(c->phi, c->rho, L0.lev(), c->d_max);
     };
     cudaStreamCaptureStatus cs;
     cudaGraph_t g = nullptr;

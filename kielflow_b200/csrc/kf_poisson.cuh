@@ -264,74 +264,32 @@ __global__ void __launch_bounds__(32 * BY) k_rbgs(double *__restrict__ phi, cons
     phi[q] = newton_step(phi[q], A, D, om);
 }
 
-// ------------------------------------------------------------ column forms
-// The half sweep and the residual above are bound by L1 throughput (about 17
-// loads per point: 7 potentials, rho, 9 axis-table entries, most strided by
-// the colouring).  In the column forms a thread owns the k-pair (2 k2,
-// 2 k2 + 1) of row j and marches the planes i0 ... i0 + PI - 1 of a column:
-// each plane's pair is one 16-byte load, kept in registers as the i-neighbour
-// of the next and previous plane; the k-neighbours outside the pair come from
-// the neighbouring lanes by warp shuffle (the warp's two edge lanes load
-// theirs); the k tables are read once per column.  The arithmetic and its
-// order are those of point_coeffs_fast, so the results are bit-identical.
-// Requires n/2 a multiple of 32 (whole warps along k), BY | n and PI | n.
+// ------------------------------------------------------------ column form
+// k_residual is bound by L1 throughput (about 17 loads per point: 7
+// potentials, rho, 9 axis-table entries, most strided).  In the column form a
+// thread owns the k-pair (2 k2, 2 k2 + 1) of row j and marches the planes
+// i0 ... i0 + PI - 1 of a column: each plane's pair is one 16-byte load, kept
+// in registers as the i-neighbour of the next and previous plane; the
+// k-neighbours outside the pair come from the neighbouring lanes by warp
+// shuffle (the warp's two edge lanes load theirs); the k tables are read once
+// per column.  The arithmetic and its order are those of point_coeffs_fast,
+// so the results are bit-identical.  Requires n/2 a multiple of 32 (whole
+// warps along k), BY | n and PI | n.
 __device__ __forceinline__ double2 ld_pair(const double *p, int i, int j, int ka, int n) {
     return *reinterpret_cast<const double2 *>(p + lidx(i, j, ka, n));
 }
 
-// One half sweep of colour `color`: at plane i the thread updates k = 2 k2 +
-// ((i + j + color) & 1).  The i-neighbours of that point are the other
-// element of the pairs of planes i -+ 1, which no thread of this half sweep
-// writes, so the pairs loaded once stay valid from plane to plane.
-template <int BY, int PI>
-__global__ void __launch_bounds__(32 * BY) k_rbgs_col(double *__restrict__ phi, const double *__restrict__ rho, Lev L,
-                                                      int color, double om) {
-    const int n = L.n;
-    const int lane = threadIdx.x;
-    const int k2 = blockIdx.x * 32 + lane, j = blockIdx.y * BY + threadIdx.y, i0 = blockIdx.z * PI;
-    const int jp = j + 1 == n ? 0 : j + 1, jm = j == 0 ? n - 1 : j - 1;
-    const int ka = 2 * k2, kb = ka + 1;
-    const int kl = ka == 0 ? n - 1 : ka - 1, kr = kb + 1 == n ? 0 : kb + 1;
-    const double dda = L.dd[ka], ipa = L.ip[ka], ima = L.im[ka];
-    const double ddb = L.dd[kb], ipb = L.ip[kb], imb = L.im[kb];
-    const double ddj = L.dd[j], ipj = L.ip[j], imj = L.im[j];
-    double2 pm = ld_pair(phi, wrapi(i0 - 1, n), j, ka, n), pc = ld_pair(phi, i0, j, ka, n);
-#pragma unroll 2
-    for (int ii = 0; ii < PI; ++ii) {
-        const int i = i0 + ii;
-        const double2 pn = ld_pair(phi, i + 1 == n ? 0 : i + 1, j, ka, n);
-        const int par = (i + j + color) & 1;
-        double fromR = __shfl_down_sync(0xffffffffu, pc.x, 1);  // phi(kb + 1) from lane + 1
-        double fromL = __shfl_up_sync(0xffffffffu, pc.y, 1);    // phi(ka - 1) from lane - 1
-        if (lane == 31 && par == 1) fromR = phi[lidx(i, j, kr, n)];
-        if (lane == 0 && par == 0) fromL = phi[lidx(i, j, kl, n)];
-        const int k = par ? kb : ka;
-        const long q = lidx(i, j, k, n);
-        const double x = par ? pc.y : pc.x;
-        const double xkp = par ? fromR : pc.y, xkm = par ? pc.x : fromL;
-        const double xip = par ? pn.y : pn.x, xim = par ? pm.y : pm.x;
-        const double xjp = phi[lidx(i, jp, k, n)], xjm = phi[lidx(i, jm, k, n)];
-        double A = __dmul_rn(xip, L.ip[i]);
-        A = __dadd_rn(A, __dmul_rn(xim, L.im[i]));
-        A = __dadd_rn(A, __dmul_rn(xjp, ipj));
-        A = __dadd_rn(A, __dmul_rn(xjm, imj));
-        A = __dadd_rn(A, __dmul_rn(xkp, par ? ipb : ipa));
-        A = __dadd_rn(A, __dmul_rn(xkm, par ? imb : ima));
-        A = __dadd_rn(A, rho[q]);
-        const double D = __dadd_rn(__dadd_rn(L.dd[i], ddj), par ? ddb : dda);
-        phi[q] = newton_step(x, A, D, om);
-        pm = pc;
-        pc = pn;
-    }
-}
-
 // The residual r = f(phi) of both points of the pair at every plane of the
 // column (16-byte loads of the pairs of rows j, j -+ 1 and of rho, one 16-byte
-// store); with MAX also max |r| as k_residual<FAST, true>.
-template <int BY, int PI, bool MAX>
+// store): the pointwise f of k_residual<true>; with MAX also max |r| as
+// k_residual<true, true>; without STORE only the maximum (k_resmax<true>).
+// LIN: the adjoint's linear residual A - (D + cl) psi (k_residual_lin,
+// k_resmax_lin).
+template <int BY, int PI, bool MAX, bool LIN = false, bool STORE = true>
 __global__ void __launch_bounds__(32 * BY) k_residual_col(const double *__restrict__ phi, const double *__restrict__ rho,
                                                           Lev L, double *__restrict__ r,
-                                                          unsigned long long *__restrict__ slots) {
+                                                          unsigned long long *__restrict__ slots,
+                                                          const double *__restrict__ cl = nullptr) {
     const int n = L.n;
     const int lane = threadIdx.x;
     const int k2 = blockIdx.x * 32 + lane, j = blockIdx.y * BY + threadIdx.y, i0 = blockIdx.z * PI;
@@ -369,8 +327,16 @@ __global__ void __launch_bounds__(32 * BY) k_residual_col(const double *__restri
         Ab = __dadd_rn(Ab, __dmul_rn(pc.x, imb));
         Ab = __dadd_rn(Ab, rr.y);
         const double Da = __dadd_rn(__dadd_rn(ddi, ddj), dda), Db = __dadd_rn(__dadd_rn(ddi, ddj), ddb);
-        const double fa = f_point(Aa, Da, pc.x), fb = f_point(Ab, Db, pc.y);
-        *reinterpret_cast<double2 *>(r + lidx(i, j, ka, n)) = make_double2(fa, fb);
+        double fa, fb;
+        if constexpr (LIN) {
+            const double2 cp = ld_pair(cl, i, j, ka, n);
+            fa = __dsub_rn(Aa, __dmul_rn(__dadd_rn(Da, cp.x), pc.x));
+            fb = __dsub_rn(Ab, __dmul_rn(__dadd_rn(Db, cp.y), pc.y));
+        } else {
+            fa = f_point(Aa, Da, pc.x);
+            fb = f_point(Ab, Db, pc.y);
+        }
+        if (STORE) *reinterpret_cast<double2 *>(r + lidx(i, j, ka, n)) = make_double2(fa, fb);
         if (MAX) af = nmax(af, nmax(fabs(fa), fabs(fb)));
         pm = pc;
         pc = pn;
