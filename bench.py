@@ -50,6 +50,9 @@ def parse():
     ap.add_argument("--rbgs-rows", type=int, default=-1,
                     help="force the smoother variant (kf_set_tuning rbgs_rows: 4, 8, 16, or 0 for the "
                          "streaming sweep) after the autotuner; -1 keeps the autotuner's choice")
+    ap.add_argument("--coarse-block", type=int, default=1, choices=[0, 1],
+                    help="kf_set_coarse_block: 1 (the default) runs the V-cycle's levels of at most "
+                         "16^3 points in one shared-memory block, 0 level by level")
     ap.add_argument("--profile-range", action="store_true",
                     help="bracket the first arm's profile steps (launched kernel by kernel, the same "
                          "kernels as the timed graph replays) with cudaProfilerStart/Stop, for "
@@ -323,6 +326,7 @@ def run_kf(args):
         if args.rbgs_rows >= 0:
             ctx.set_tuning(tune["fft_plan"], args.rbgs_rows)
             tune = dict(tune, rbgs_rows=args.rbgs_rows)
+        ctx.set_coarse_block(args.coarse_block == 1)
         ctx.rk4(dt, args.warmup)
         ctx.synchronize()
         barrier()
@@ -469,7 +473,8 @@ def run_kf(args):
         "data": "synthetic (seeded noise, Gaussian dust; seed = rank)",
         "config": workload_config(w, args.workload, ws),
         "tuning": {"fft_radices": tune32["fft_radices"][tune32["fft_plan"]], "rbgs_rows": tune32["rbgs_rows"],
-                   "rbgs_rows_meaning": "0: streaming TMA-staged sweep (k_rbgs_march)"},
+                   "rbgs_rows_meaning": "0: streaming TMA-staged sweep (k_rbgs_march)",
+                   "coarse_block": args.coarse_block},
         "gpu_launches": launches,
         "roofline": roofline,
         "cpu_baseline": cpu,

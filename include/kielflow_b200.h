@@ -280,6 +280,14 @@ int kf_autotune(kf_ctx *ctx, int reps, kf_tune_out *out);
  * applied to every instance of a sweep).  KF_ERR_ARG for other values. */
 int kf_set_tuning(kf_ctx *ctx, int fft_plan, int rbgs_rows);
 
+/* Levels of at most 16^3 points below the finest, in FAS V-cycles that reach
+ * a level below them (the 16^3 and 8^3 levels of the 6-level 256^3 cycle):
+ * on = 1 (the default) runs them, with the correction they return, as one
+ * block with the levels in shared memory (one launch instead of 16 kernels
+ * that each last about their launch latency); on = 0 level by level.  The
+ * potentials are the same bit for bit.  KF_ERR_ARG for other values. */
+int kf_set_coarse_block(kf_ctx *ctx, int on);
+
 /* interface_poisson_solver::solve (interface_poisson_solver.hpp:18): phi_io is
  * the initial guess and the result, rho is read only; host arrays, n^3 doubles. */
 int kf_poisson_solve(kf_ctx *ctx, double *phi_io, const double *rho);

@@ -16,7 +16,7 @@ SRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libkf.so")
 SOURCES = ["kf_capi.cu", "kf_noalloc.cu", "kf_io.cpp"]
 HEADERS = ["kf_fft.cuh", "kf_types.cuh", "kf_passes.cuh", "kf_pointwise.cuh", "kf_poisson.cuh", "kf_adjoint.cuh",
-           "kf_adjoint_host.cuh", "kf_graph.cuh", "kf_driver.cuh", "kf_io.hpp", "kf_stretch.cuh"]
+           "kf_adjoint_host.cuh", "kf_graph.cuh", "kf_driver.cuh", "kf_io.hpp", "kf_stretch.cuh", "kf_march.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-shared"]
 

@@ -139,6 +139,10 @@ struct kf_ctx {
     int fftv = 0;     // radix-plan variant of the transform kernels (kf_autotune)
     int rbgs_by = 8;  // smoother variant (kf_autotune): k_rbgs rows per block, or 0 for k_rbgs_march
     bool march_maps = false;  // the driver's tensor-map encoder is available
+    bool coarse_block = true;  // levels <= 16^3 of a V-cycle in one k_coarse_cycle block (kf_set_coarse_block)
+    int cc_level = -1;         // entry level of k_coarse_cycle, or -1 (cc_setup)
+    CoarseCycle ccyc{};
+    size_t cc_smem = 0;
     int stage_idx = 0;  // RK stage of the right-hand side being evaluated (0..3)
     // one RK4 step captured as a CUDA graph (FAS or no Poisson, profile off):
     // time / warm-start history and solve statistics live on the device
@@ -538,7 +542,11 @@ void smooth(kf_ctx *c, LevelBuf &L, double *phi, const double *rho, const double
 // k_rbgs_lin with the adjoint's e^phi).  (Sweeping a level larger than L2 in
 // chunks of i-planes, black one plane behind red so that the black half finds
 // its data in L2, gives the same potentials bit for bit but measured slower at
-// 256^3: 156 / 169 / 181 / 214 us per sweep for 1 / 2 / 4 / 8 chunks.)
+// 256^3: 156 / 169 / 181 / 214 us per sweep for 1 / 2 / 4 / 8 chunks.  So did
+// threads that update one (j, k) on 2 or 4 planes two apart, sharing the axis
+// tables and the planes between their points: 20.4 / 20.2 ms against 18.9 ms
+// for 240 half sweeps; L1 use fell from 89 to 62 %, but occupancy halved and
+// the DRAM throughput, 4.5 TB/s on 1.33x the algorithmic bytes, stayed.)
 
 void smooth_plain(kf_ctx *c, LevelBuf &L, double *phi, const double *rho, const double *cc, int sweeps, int cls) {
     const int n = L.n;
@@ -630,14 +638,21 @@ void vcycle_tail(kf_ctx *c, int l) {
         Launch L_(c, l == 0 ? KC_TRANSFER : KC_MG_COARSE, 8. * N + 32. * Nc3);
         k_restrict<<<mg_grid(Lc.n, Lc.n), mg_block(), 0, c->st>>>(L.r, L.phi, n, Lc.r, Lc.phi, Lc.phi0);
     }
-    {
-        Launch L_(c, l == 0 ? KC_TRANSFER : KC_MG_COARSE, 24. * Nc3);
-        k_fas_rhs<<<mg_grid(Lc.n, Lc.n), mg_block(), 0, c->st>>>(Lc.phi, Lc.r, Lc.lev(), Lc.rho);
-    }
-    vcycle(c, l + 1);
-    {
-        Launch L_(c, l == 0 ? KC_TRANSFER : KC_MG_COARSE, 24. * Nc3);
-        k_correction<<<mg_grid(Lc.n, Lc.n), mg_block(), 0, c->st>>>(Lc.phi, Lc.phi0, Lc.n);
+    if (l + 1 == c->cc_level) {
+        // the levels from l + 1 down in one block: FAS right-hand side, cycle, correction
+        Launch L_(c, KC_COARSE, 40. * Nc3);
+        k_coarse_cycle<<<1, 1024, c->cc_smem, c->st>>>(Lc.phi, Lc.phi0, Lc.r, c->ccyc, cf.mg_pre, cf.mg_post,
+                                                       cf.coarse_tol, 1000, mg_omega(cf), c->d_sweeps);
+    } else {
+        {
+            Launch L_(c, l == 0 ? KC_TRANSFER : KC_MG_COARSE, 24. * Nc3);
+            k_fas_rhs<<<mg_grid(Lc.n, Lc.n), mg_block(), 0, c->st>>>(Lc.phi, Lc.r, Lc.lev(), Lc.rho);
+        }
+        vcycle(c, l + 1);
+        {
+            Launch L_(c, l == 0 ? KC_TRANSFER : KC_MG_COARSE, 24. * Nc3);
+            k_correction<<<mg_grid(Lc.n, Lc.n), mg_block(), 0, c->st>>>(Lc.phi, Lc.phi0, Lc.n);
+        }
     }
     {
         Launch L_(c, l == 0 ? KC_TRANSFER : KC_MG_COARSE, 16. * N + 8. * Nc3);
@@ -1554,6 +1569,8 @@ void build_tables(kf_ctx *c) {
     }
 }
 
+void cc_setup(kf_ctx *c);
+
 void build_levels(kf_ctx *c) {
     const kf_config &cf = c->cfg;
     int nl = 1;
@@ -1616,6 +1633,36 @@ void build_levels(kf_ctx *c) {
             L.phi0 = dalloc<double>(c, bytes);
         }
     }
+    CK(cudaFuncSetAttribute(k_coarse_cycle, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    cc_setup(c);
+}
+
+// The entry level of k_coarse_cycle: the first level below the finest with
+// n <= 16 that has at least one level below it, when the levels from it down
+// fit the kernel (KF_CC_LEVELS, 200 KB of shared memory); -1 otherwise or
+// with the block switched off.
+void cc_setup(kf_ctx *c) {
+    c->cc_level = -1;
+    const int nl = (int)c->lv.size();
+    if (!c->coarse_block || c->cfg.poisson_mode != KF_PS_FAS) return;
+    int lb = 1;
+    while (lb < nl && c->lv[lb].n > 16) ++lb;
+    if (lb >= nl - 1 || nl - lb > KF_CC_LEVELS) return;
+    CoarseCycle C{};
+    C.nl = nl - lb;
+    for (int m = 0; m < C.nl; ++m) {
+        const LevelBuf &L = c->lv[lb + m];
+        C.n[m] = L.n;
+        C.dd[m] = L.dd;
+        C.ip[m] = L.ip;
+        C.im[m] = L.im;
+        C.gam[m] = L.gam;
+    }
+    const size_t b = coarse_cycle_smem(C);
+    if (b > 200 * 1024) return;
+    c->ccyc = C;
+    c->cc_smem = b;
+    c->cc_level = lb;
 }
 
 void build_jobs(kf_ctx *c) {
@@ -2383,6 +2430,17 @@ int kf_set_tuning(kf_ctx *c, int fft_plan, int rbgs_rows) {
         c->fftv = fft_plan;
         c->rbgs_by = rbgs_rows;
         if (changed) drop_graphs(c);
+    });
+}
+
+int kf_set_coarse_block(kf_ctx *c, int on) {
+    return guarded(c, [&] {
+        if (on != 0 && on != 1) throw KfError{KF_ERR_ARG, "kf_set_coarse_block: on is 0 or 1"};
+        if (c->capturing) throw KfError{KF_ERR_ARG, "kf_set_coarse_block during a capture"};
+        if (c->coarse_block == (on == 1)) return;
+        c->coarse_block = on == 1;
+        cc_setup(c);
+        drop_graphs(c);
     });
 }
 

@@ -71,13 +71,14 @@ k_axis_pass(const AxisJob *__restrict__ jobs, int njobs, int axis, Geo<T> g,
         base = (long)plane * n * nzc + kk;
         rstride = nzc;
     }
+    const int pbnd = valid && (J.mul == MUL_P || J.mul == MUL_P_IK) ? dealias_bound(g.pb, jj, kk, g.nzc) : -2;
     T2 v[E];
 #pragma unroll
     for (int q = 0; q < E; ++q) {
         const int row = reg_row<N, P, Plan<N>::R1>(p, q);
         T2 x = valid ? in[base + row * rstride] : mk<T2>((T)0, (T)0);
         if (J.mul == MUL_P || J.mul == MUL_P_IK) {
-            if (!dealias_keep(g.q2, g.thr, row, jj, kk)) x = mk<T2>((T)0, (T)0);
+            if (!dealias_keep_b(g.q2, g.thr, pbnd, g.n, row, jj, kk)) x = mk<T2>((T)0, (T)0);
         }
         if (J.mul == MUL_P_IK || J.mul == MUL_IK) x = mul_ik(x, g.kv[row]);
         v[q] = x;
@@ -110,6 +111,9 @@ __device__ __forceinline__ void cp_async_copy(void *smem, const double2 *g) {
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+template <int PENDING> __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(PENDING) : "memory");
+}
 
 template <typename T> struct AxisTile {
     typedef typename C2<T>::type T2;
@@ -166,13 +170,22 @@ template <typename T, int N, int V, int TILES, int CAP, int FLOOR> struct PipeMi
     static constexpr int value = lim < 1 ? 1 : (lim < CAP ? (int)lim : CAP);
 };
 
-// Shared memory of a k_axis_pipe launch: exchange and staging tiles.  (Held
-// to fewer registers for three resident blocks, or with its twiddles, k values
-// and job descriptors staged in shared memory, the pass measured no faster:
-// 12.5 and 13.8 ms against 12.4 ms for 48 launches; it is bound by the latency
-// of its loads, not by occupancy.)
+// Staging slots per k_axis_pipe block: the tile being transformed was loaded
+// into one slot while the next KF_PIPE_DEPTH - 1 tiles load into the others.
+// (Two slots, 96 KB per block at 256^3, measured slower: 13.5 against 12.2 ms
+// for the 48 inverse launches of a 20-step run; the shared memory they take
+// from the L1 cache is what the twiddle and table loads hit.)
+#ifndef KF_PIPE_DEPTH
+#define KF_PIPE_DEPTH 1
+#endif
+
+// Shared memory of a k_axis_pipe launch: the exchange tile and KF_PIPE_DEPTH
+// staging tiles.  (Held to fewer registers for three resident blocks, or with
+// its twiddles, k values and job descriptors staged in shared memory, the
+// one-slot pass measured no faster: 12.5 and 13.8 ms against 12.4 ms for 48
+// launches.)
 template <typename T, int N> inline size_t axis_pipe_smem(int) {
-    return 2 * (size_t)N * Tile<T>::TC * sizeof(typename C2<T>::type);
+    return (1 + KF_PIPE_DEPTH) * (size_t)N * Tile<T>::TC * sizeof(typename C2<T>::type);
 }
 
 template <typename T, int N, int SIGN, int V = 0>
@@ -181,43 +194,55 @@ k_axis_pipe(const AxisJob *__restrict__ jobs, int njobs, int axis, Geo<T> g,
             const typename C2<T>::type *__restrict__ tw, int total) {
     typedef typename C2<T>::type T2;
     constexpr int TC = Tile<T>::TC, P = PlanV<N, V>::P, E = N / P;
+    constexpr int D = KF_PIPE_DEPTH;
     extern __shared__ __align__(16) unsigned char kf_smem[];
     T2 *sm = reinterpret_cast<T2 *>(kf_smem);  // exchange [N][TC]
-    T2 *stg = sm + N * TC;                      // staging  [N][TC]
+    T2 *stg0 = sm + N * TC;                     // staging  [D][N][TC]
     const int c = threadIdx.x % TC, p = threadIdx.x / TC;
     int t = blockIdx.x;
     if (t >= total) return;
-    auto prefetch = [&](const AxisTile<T> &G) {
+    // Each thread stages exactly the elements it reads back, so the slots need
+    // no barrier.  One commit group per tile (empty past the end), so that
+    // cp.async.wait_group D - 1 always leaves the current tile complete.
+    auto prefetch = [&](int tt, int slot) {
+        if (tt < total) {
+            const AxisTile<T> G = axis_tile<T, N>(jobs, njobs, axis, tt, c, g.n, g.nzc);
+            T2 *st = stg0 + slot * (N * TC);
 #pragma unroll
-        for (int q = 0; q < E; ++q) {
-            const int row = reg_row<N, P, PlanV<N, V>::R1>(p, q);
-            T2 *dst = stg + row * TC + c;
-            if (G.valid)
-                cp_async_copy(dst, G.in + G.base + row * G.rstride);
-            else
-                *dst = mk<T2>((T)0, (T)0);
+            for (int q = 0; q < E; ++q) {
+                const int row = reg_row<N, P, PlanV<N, V>::R1>(p, q);
+                T2 *dst = st + row * TC + c;
+                if (G.valid)
+                    cp_async_copy(dst, G.in + G.base + row * G.rstride);
+                else
+                    *dst = mk<T2>((T)0, (T)0);
+            }
         }
         cp_async_commit();
     };
-    AxisTile<T> cur = axis_tile<T, N>(jobs, njobs, axis, t, c, g.n, g.nzc);
-    prefetch(cur);
-    for (; t < total; t += gridDim.x) {
-        const int tn = t + gridDim.x;
-        AxisTile<T> nxt = cur;
-        if (tn < total) nxt = axis_tile<T, N>(jobs, njobs, axis, tn, c, g.n, g.nzc);
-        cp_async_wait_all();
+#pragma unroll
+    for (int d = 0; d < D; ++d) prefetch(t + d * (int)gridDim.x, d);
+    for (int it = 0; t < total; t += gridDim.x, ++it) {
+        const int slot = it % D;
+        const AxisTile<T> cur = axis_tile<T, N>(jobs, njobs, axis, t, c, g.n, g.nzc);
+        // the 2/3 rule of this column as an index bound (one table read per tile)
+        const int pbnd = cur.valid && (cur.mul == MUL_P || cur.mul == MUL_P_IK)
+                             ? dealias_bound(g.pb, cur.jj, cur.kk, g.nzc)
+                             : -2;
+        cp_async_wait<D - 1>();
+        const T2 *stg = stg0 + slot * (N * TC);
         T2 v[E];
 #pragma unroll
         for (int q = 0; q < E; ++q) {
             const int row = reg_row<N, P, PlanV<N, V>::R1>(p, q);
             T2 x = stg[row * TC + c];
             if (cur.mul == MUL_P || cur.mul == MUL_P_IK) {
-                if (!dealias_keep(g.q2, g.thr, row, cur.jj, cur.kk)) x = mk<T2>((T)0, (T)0);
+                if (!dealias_keep_b(g.q2, g.thr, pbnd, g.n, row, cur.jj, cur.kk)) x = mk<T2>((T)0, (T)0);
             }
             if (cur.mul == MUL_P_IK || cur.mul == MUL_IK) x = mul_ik(x, g.kv[row]);
             v[q] = x;
         }
-        if (tn < total) prefetch(nxt);
+        prefetch(t + D * (int)gridDim.x, slot);
         PlanV<N, V>::template fft<T2, SIGN>(v, sm + c, StrideAddr{TC}, p, tw);
         if (cur.valid) {
 #pragma unroll
@@ -226,7 +251,6 @@ k_axis_pipe(const AxisJob *__restrict__ jobs, int njobs, int axis, Geo<T> g,
                 cur.out[cur.base + row * cur.rstride] = v[q];
             }
         }
-        cur = nxt;
     }
 }
 
@@ -379,12 +403,13 @@ k_z_r2c(const ZJob *__restrict__ jobs, int njobs, int nrows,
 //        (rhs_standard.cpp:119-140, 218-248, 279-295)
 //   s  : SV s^ [+ D|k|^2 s^] + M i k_x P s^ + i k.P u^
 //        (rhs_standard.cpp:135-139, 304-319)
+// b: the column's 2/3-rule bound (dealias_bound), or -2 for the exact test.
 template <typename T>
 __device__ __forceinline__ typename C2<T>::type lin_term(const RhsArgs<T> &a, const Geo<T> &g, int q,
-                                                         int i, int j, int k, long idx) {
+                                                         int i, int j, int k, long idx, int b) {
     typedef typename C2<T>::type T2;
     const int Tm = a.terms;
-    const bool P = dealias_keep(g.q2, g.thr, i, j, k);
+    const bool P = dealias_keep_b(g.q2, g.thr, b, g.n, i, j, k);
     const T kx = g.kv[i], ky = g.kv[j], kz = g.kv[k];
     const T sv = a.SV[idx];
     T2 fb;
@@ -471,7 +496,7 @@ k_xfwd_assemble(const AxisJob *__restrict__ jobs, Geo<T> g, RhsArgs<T> a,
     const bool valid = col < n * nzc;
     const long rstride = (long)n * nzc;
     const int jj = col / nzc, kk = col - jj * nzc;
-    const int b = PEN ? dealias_bound(g.pb, jj, kk, nzc) : -2;
+    const int b = valid ? dealias_bound(g.pb, jj, kk, nzc) : -2;
     for (int q = 0; q < 4; ++q) {
         const T2 *__restrict__ in = static_cast<const T2 *>(jobs[q].in);
         T2 *__restrict__ out = static_cast<T2 *>(jobs[q].out);
@@ -492,7 +517,7 @@ k_xfwd_assemble(const AxisJob *__restrict__ jobs, Geo<T> g, RhsArgs<T> a,
                 if constexpr (PEN) {
                     K = dealias_keep_b(g.q2, g.thr, b, N, i, jj, kk) ? F : mk<T2>((T)0, (T)0);
                 } else {
-                    T2 fb = lin_term(a, g, q, i, jj, kk, idx);
+                    T2 fb = lin_term(a, g, q, i, jj, kk, idx, b);
                     K = mk<T2>(-(fb.x + F.x), -(fb.y + F.y));
                 }
                 out[idx] = K;

@@ -355,11 +355,71 @@ __global__ void __launch_bounds__(32 * BY) k_residual_col(const double *__restri
     }
 }
 
-// Coarsest-level solve in one block: the level (phi, rho and the axis
-// tables) is staged in shared memory, red-black sweeps run until
-// max |f| <= max(tol, 1e-4 max |f| at entry) (checked before every sweep, as
-// the host loop of the oracle), then phi is written back.  Dynamic shared
-// memory: 16 n^3 + 24 n bytes.
+// Block-wide max of m (NaN-propagating) over up to 1024 threads; sh: 32 doubles.
+__device__ __forceinline__ double block_nmax(double m, double *sh) {
+    for (int o = 16; o > 0; o >>= 1) m = nmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double t = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.;
+        for (int o = 16; o > 0; o >>= 1) t = nmax(t, __shfl_xor_sync(0xffffffffu, t, o));
+        if (threadIdx.x == 0) sh[0] = t;
+    }
+    __syncthreads();
+    const double res = sh[0];
+    __syncthreads();
+    return res;
+}
+
+// One red-black half sweep (k_rbgs's point update) of a level the block holds.
+__device__ __forceinline__ void block_half_sweep(double *sp, const double *sr, const Lev &Ls, int color,
+                                                 double om) {
+    const int n = Ls.n;
+    const int M = n * n * n / 2, nh = n / 2;
+    for (int id = threadIdx.x; id < M; id += blockDim.x) {
+        const int k2 = id % nh;
+        const int r = id / nh;
+        const int j = r % n, i = r / n;
+        const int k = 2 * k2 + ((i + j + color) & 1);
+        double A, D;
+        point_coeffs_fast(sp, sr, Ls, i, j, k, A, D);
+        const int q = (int)lidx(i, j, k, n);
+        sp[q] = newton_step(sp[q], A, D, om);
+    }
+    __syncthreads();
+}
+
+// Coarsest-level relaxation of a level the block holds: red-black sweeps until
+// max |f| <= max(tol, 1e-4 max |f| at entry), checked before every sweep (as
+// the host loop of the oracle); returns the number of sweeps.
+__device__ __forceinline__ int block_coarse_relax(double *sp, const double *sr, const Lev &Ls, double tol,
+                                                  int max_sweeps, double om, double *sh) {
+    const int n = Ls.n;
+    const int N = n * n * n;
+    int s = 0;
+    double r0 = 0.;
+    for (;; ++s) {
+        double m = 0.;
+        for (int id = threadIdx.x; id < N; id += blockDim.x) {
+            const int k = id % n;
+            const int r = id / n;
+            const int j = r % n, i = r / n;
+            double A, D;
+            point_coeffs_fast(sp, sr, Ls, i, j, k, A, D);
+            m = nmax(m, fabs(f_point(A, D, sp[id])));
+        }
+        const double res = block_nmax(m, sh);
+        if (s == 0) r0 = res;
+        if (!(res > fmax(tol, 1e-4 * r0)) || s >= max_sweeps) break;  // converged, NaN or capped
+        block_half_sweep(sp, sr, Ls, 0, om);
+        block_half_sweep(sp, sr, Ls, 1, om);
+    }
+    return s;
+}
+
+// Coarsest-level solve in one block: the level (phi, rho and the axis tables)
+// is staged in shared memory, block_coarse_relax runs, then phi is written
+// back.  Dynamic shared memory: 16 n^3 + 24 n bytes.
 __global__ void __launch_bounds__(1024) k_coarse_solve(double *__restrict__ phi, const double *__restrict__ rho,
                                                        Lev L, double tol, int max_sweeps,
                                                        int *__restrict__ sweeps_out, double om) {
@@ -379,46 +439,7 @@ __global__ void __launch_bounds__(1024) k_coarse_solve(double *__restrict__ phi,
     }
     __syncthreads();
     const Lev Ls{n, sd, nullptr, nullptr, si, sm_};
-    int s = 0;
-    double r0 = 0.;
-    for (;; ++s) {
-        double m = 0.;
-        for (int id = threadIdx.x; id < N; id += blockDim.x) {
-            const int k = id % n;
-            const int r = id / n;
-            const int j = r % n, i = r / n;
-            double A, D;
-            point_coeffs_fast(sp, sr, Ls, i, j, k, A, D);
-            m = nmax(m, fabs(f_point(A, D, sp[id])));
-        }
-        for (int o = 16; o > 0; o >>= 1) m = nmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-        if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = m;
-        __syncthreads();
-        if (threadIdx.x < 32) {
-            double t = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.;
-            for (int o = 16; o > 0; o >>= 1) t = nmax(t, __shfl_xor_sync(0xffffffffu, t, o));
-            if (threadIdx.x == 0) sh[0] = t;
-        }
-        __syncthreads();
-        const double res = sh[0];
-        __syncthreads();
-        if (s == 0) r0 = res;
-        if (!(res > fmax(tol, 1e-4 * r0)) || s >= max_sweeps) break;  // converged, NaN or capped
-        for (int color = 0; color < 2; ++color) {
-            const int M = N / 2, nh = n / 2;
-            for (int id = threadIdx.x; id < M; id += blockDim.x) {
-                const int k2 = id % nh;
-                const int r = id / nh;
-                const int j = r % n, i = r / n;
-                const int k = 2 * k2 + ((i + j + color) & 1);
-                double A, D;
-                point_coeffs_fast(sp, sr, Ls, i, j, k, A, D);
-                const int q = (int)lidx(i, j, k, n);
-                sp[q] = newton_step(sp[q], A, D, om);
-            }
-            __syncthreads();
-        }
-    }
+    const int s = block_coarse_relax(sp, sr, Ls, tol, max_sweeps, om, sh);
     for (int id = threadIdx.x; id < N; id += blockDim.x) phi[id] = sp[id];
     if (threadIdx.x == 0) *sweeps_out = s;
 }
@@ -432,15 +453,8 @@ __global__ void __launch_bounds__(256) k_correction(const double *__restrict__ p
     phic0[q] = __dsub_rn(phic[q], phic0[q]);
 }
 
-// Full-weighting restriction of r (fine n) and injection of phi:
-// rc = FW(r), phic = phic0 = phi[2i,2j,2k]  (field_interpolation.cpp:233-259 for phi)
-__global__ void __launch_bounds__(256) k_restrict(const double *__restrict__ r, const double *__restrict__ phi, int nf,
-                                                  double *__restrict__ rc, double *__restrict__ phic,
-                                                  double *__restrict__ phic0) {
-    const int nc = nf / 2;
-    const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, i = blockIdx.z;
-    if (k >= nc || j >= nc) return;
-    const long id = lidx(i, j, k, nc);
+// Full-weighting restriction of r (fine nf) at the coarse point (i, j, k)
+__device__ __forceinline__ double fw_point(const double *__restrict__ r, int nf, int i, int j, int k) {
     const double w[3] = {0.25, 0.5, 0.25};
     double s = 0.;
     for (int a = -1; a <= 1; ++a) {
@@ -457,23 +471,40 @@ __global__ void __launch_bounds__(256) k_restrict(const double *__restrict__ r, 
         }
         s = __dadd_rn(s, __dmul_rn(w[a + 1], sy));
     }
-    rc[id] = s;
+    return s;
+}
+
+// Full-weighting restriction of r (fine n) and injection of phi:
+// rc = FW(r), phic = phic0 = phi[2i,2j,2k]  (field_interpolation.cpp:233-259 for phi)
+__global__ void __launch_bounds__(256) k_restrict(const double *__restrict__ r, const double *__restrict__ phi, int nf,
+                                                  double *__restrict__ rc, double *__restrict__ phic,
+                                                  double *__restrict__ phic0) {
+    const int nc = nf / 2;
+    const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, i = blockIdx.z;
+    if (k >= nc || j >= nc) return;
+    const long id = lidx(i, j, k, nc);
+    rc[id] = fw_point(r, nf, i, j, k);
     const double p = phi[lidx(2 * i, 2 * j, 2 * k, nf)];
     phic[id] = p;
     phic0[id] = p;
 }
 
-// rho_c = N_c(phi_c) + r_c with N(phi) = -lap_h phi + e^phi
+// rho_c = N_c(phi_c) + r_c with N(phi) = -lap_h phi + e^phi, at one point
+__device__ __forceinline__ double fas_rho_point(const double *__restrict__ phic, double rc, const Lev &L, int i, int j,
+                                                int k) {
+    double A, D;
+    point_coeffs_fast(phic, nullptr, L, i, j, k, A, D);
+    const double Nc = __dsub_rn(0., f_point(A, D, phic[lidx(i, j, k, L.n)]));
+    return __dadd_rn(Nc, rc);
+}
+
 __global__ void __launch_bounds__(256) k_fas_rhs(const double *__restrict__ phic, const double *__restrict__ rc, Lev L,
                                                  double *__restrict__ rhoc) {
     const int n = L.n;
     const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, i = blockIdx.z;
     if (k >= n || j >= n) return;
     const long id = lidx(i, j, k, n);
-    double A, D;
-    point_coeffs_fast(phic, nullptr, L, i, j, k, A, D);
-    const double Nc = __dsub_rn(0., f_point(A, D, phic[id]));
-    rhoc[id] = __dadd_rn(Nc, rc[id]);
+    rhoc[id] = fas_rho_point(phic, rc[id], L, i, j, k);
 }
 
 // Trilinear prolongation of e = phic - phic0 in the z, y, x pass order of
@@ -496,16 +527,12 @@ __device__ __forceinline__ double py(const double *pc, const double *pc0, const 
     return __dadd_rn(__dmul_rn(1. - g, pz(pc, pc0, gam, nf, i, j - 1, k)),
                      __dmul_rn(g, pz(pc, pc0, gam, nf, i, (j + 1) % nf, k)));
 }
-// One thread per coarse cell (I, J, K): the 8 fine points (2I+a, 2J+b, 2K+c)
-// from the 8 corner values, with OP_hto2h's z, y, x passes and gammas (the
-// same operations per fine point as interpolating the whole field pass by pass).
-__global__ void __launch_bounds__(256) k_prolong_add(double *__restrict__ phi, const double *__restrict__ e,
-                                                     const double *__restrict__ unused,
-                                                     const double *__restrict__ gam, int nf) {
-    (void)unused;
+// The coarse cell (I, J, K): the 8 fine points (2I+a, 2J+b, 2K+c) from the 8
+// corner values, with OP_hto2h's z, y, x passes and gammas (the same
+// operations per fine point as interpolating the whole field pass by pass).
+__device__ __forceinline__ void prolong_cell(double *__restrict__ phi, const double *__restrict__ e,
+                                             const double *__restrict__ gam, int nf, int I, int J, int K) {
     const int nc = nf / 2;
-    const int K = blockIdx.x * 32 + threadIdx.x, J = blockIdx.y * 8 + threadIdx.y, I = blockIdx.z;
-    if (K >= nc || J >= nc) return;
     const int I1 = I + 1 == nc ? 0 : I + 1, J1 = J + 1 == nc ? 0 : J + 1, K1 = K + 1 == nc ? 0 : K + 1;
     // corner values e[I+di][J+dj][K+dk]
     double c[2][2][2];
@@ -548,6 +575,145 @@ __global__ void __launch_bounds__(256) k_prolong_add(double *__restrict__ phi, c
                 const long q = lidx(2 * I + a, 2 * J + b, 2 * K + cc, nf);
                 phi[q] = __dadd_rn(phi[q], v);
             }
+}
+
+// phi += P e, one thread per coarse cell
+__global__ void __launch_bounds__(256) k_prolong_add(double *__restrict__ phi, const double *__restrict__ e,
+                                                     const double *__restrict__ unused,
+                                                     const double *__restrict__ gam, int nf) {
+    (void)unused;
+    const int nc = nf / 2;
+    const int K = blockIdx.x * 32 + threadIdx.x, J = blockIdx.y * 8 + threadIdx.y, I = blockIdx.z;
+    if (K >= nc || J >= nc) return;
+    prolong_cell(phi, e, gam, nf, I, J, K);
+}
+
+// ------------------------------------------------------------ coarse levels in one block
+// Levels of at most 16^3 points hold at most 4096 points: the kernels of one
+// V-cycle there (half-sweeps, residual, restriction, FAS right-hand side,
+// coarsest solve, correction, prolongation: 14 launches from the 16^3 level
+// down to 8^3) each run for about the time of their launch.  k_coarse_cycle
+// runs all of it in one block with every level in shared memory, from the
+// entry level's injected potential and restricted residual (k_restrict) to
+// its correction e = phi - phi0 (left in phi0 for k_prolong_add), with the
+// per-point arithmetic of the level-by-level kernels, so the potentials are
+// the same bit for bit.
+constexpr int KF_CC_LEVELS = 4;
+
+struct CoarseCycle {
+    int nl;  // levels held: 0 = the entry level, nl - 1 = the coarsest (2 <= nl <= KF_CC_LEVELS)
+    int n[KF_CC_LEVELS];
+    const double *dd[KF_CC_LEVELS], *ip[KF_CC_LEVELS], *im[KF_CC_LEVELS];
+    const double *gam[KF_CC_LEVELS];  // fine-axis gammas of level m (prolongation from m + 1)
+};
+
+// Shared memory of k_coarse_cycle: per level phi, rho, r, phi0 (n^3 each) and
+// four axis tables (n each).
+inline size_t coarse_cycle_smem(const CoarseCycle &C) {
+    size_t b = 0;
+    for (int m = 0; m < C.nl; ++m) b += 8 * (4 * (size_t)C.n[m] * C.n[m] * C.n[m] + 4 * (size_t)C.n[m]);
+    return b;
+}
+
+// Level m of the shared-memory layout of k_coarse_cycle.
+struct CcLevel {
+    double *P, *R, *F, *P0;  // phi, rho, r, phi0
+    Lev L;                   // n and the tables dd, ip, im (in shared memory)
+    double *G;               // gammas (in shared memory)
+};
+__device__ __forceinline__ CcLevel cc_level(const CoarseCycle &C, double *sm, int m) {
+    for (int l = 0; l < m; ++l) sm += 4 * (C.n[l] * C.n[l] * C.n[l] + C.n[l]);
+    const int n = C.n[m], N = n * n * n;
+    double *t = sm + 4 * N;
+    return CcLevel{sm, sm + N, sm + 2 * N, sm + 3 * N, Lev{n, t, nullptr, nullptr, t + n, t + 2 * n}, t + 3 * n};
+}
+
+__global__ void __launch_bounds__(1024) k_coarse_cycle(double *__restrict__ phi, double *__restrict__ phi0,
+                                                       const double *__restrict__ r, CoarseCycle C, int pre,
+                                                       int post, double tol, int max_sweeps, double om,
+                                                       int *__restrict__ sweeps_out) {
+    extern __shared__ __align__(16) double cc_sm[];
+    __shared__ double sh[32];
+    for (int m = 0; m < C.nl; ++m) {
+        const CcLevel V = cc_level(C, cc_sm, m);
+        double *dd = const_cast<double *>(V.L.dd), *ip = const_cast<double *>(V.L.ip);
+        double *im = const_cast<double *>(V.L.im);
+        for (int t = threadIdx.x; t < V.L.n; t += blockDim.x) {
+            dd[t] = C.dd[m][t];
+            ip[t] = C.ip[m][t];
+            im[t] = C.im[m][t];
+            V.G[t] = C.gam[m] ? C.gam[m][t] : 0.;
+        }
+    }
+    {
+        const CcLevel V = cc_level(C, cc_sm, 0);
+        const int N = C.n[0] * C.n[0] * C.n[0];
+        for (int id = threadIdx.x; id < N; id += blockDim.x) {
+            V.P[id] = phi[id];
+            V.R[id] = r[id];
+        }
+    }
+    __syncthreads();
+    // the entry level's FAS right-hand side (k_fas_rhs) in place of its r;
+    // on the levels below, the restriction leaves r in R the same way
+    for (int m = 0; m < C.nl; ++m) {
+        const CcLevel V = cc_level(C, cc_sm, m);
+        const int n = V.L.n, N = n * n * n;
+        for (int id = threadIdx.x; id < N; id += blockDim.x) {
+            const int k = id % n, j = (id / n) % n, i = id / (n * n);
+            V.R[id] = fas_rho_point(V.P, V.R[id], V.L, i, j, k);
+        }
+        __syncthreads();
+        if (m + 1 == C.nl) break;
+        // pre-smoothing, residual (k_residual<true>), restriction and injection (k_restrict)
+        for (int s = 0; s < pre; ++s) {
+            block_half_sweep(V.P, V.R, V.L, 0, om);
+            block_half_sweep(V.P, V.R, V.L, 1, om);
+        }
+        for (int id = threadIdx.x; id < N; id += blockDim.x) {
+            const int k = id % n, j = (id / n) % n, i = id / (n * n);
+            double A, D;
+            point_coeffs_fast(V.P, V.R, V.L, i, j, k, A, D);
+            V.F[id] = f_point(A, D, V.P[id]);
+        }
+        __syncthreads();
+        const CcLevel W = cc_level(C, cc_sm, m + 1);
+        const int nc = n / 2, Ncc = nc * nc * nc;
+        for (int id = threadIdx.x; id < Ncc; id += blockDim.x) {
+            const int k = id % nc, j = (id / nc) % nc, i = id / (nc * nc);
+            W.R[id] = fw_point(V.F, n, i, j, k);
+            const double p = V.P[lidx(2 * i, 2 * j, 2 * k, n)];
+            W.P[id] = p;
+            W.P0[id] = p;
+        }
+        __syncthreads();
+    }
+    const CcLevel Vc = cc_level(C, cc_sm, C.nl - 1);
+    const int s = block_coarse_relax(Vc.P, Vc.R, Vc.L, tol, max_sweeps, om, sh);
+    for (int m = C.nl - 2; m >= 0; --m) {
+        // correction (k_correction), prolongation (k_prolong_add), post-smoothing
+        const CcLevel V = cc_level(C, cc_sm, m), W = cc_level(C, cc_sm, m + 1);
+        const int n = V.L.n, nc = n / 2, Ncc = nc * nc * nc;
+        for (int id = threadIdx.x; id < Ncc; id += blockDim.x) W.P0[id] = __dsub_rn(W.P[id], W.P0[id]);
+        __syncthreads();
+        for (int id = threadIdx.x; id < Ncc; id += blockDim.x) {
+            const int K = id % nc, J = (id / nc) % nc, I = id / (nc * nc);
+            prolong_cell(V.P, W.P0, V.G, n, I, J, K);
+        }
+        __syncthreads();
+        for (int t = 0; t < post; ++t) {
+            block_half_sweep(V.P, V.R, V.L, 0, om);
+            block_half_sweep(V.P, V.R, V.L, 1, om);
+        }
+    }
+    const CcLevel V0 = cc_level(C, cc_sm, 0);
+    const int N = C.n[0] * C.n[0] * C.n[0];
+    for (int id = threadIdx.x; id < N; id += blockDim.x) {
+        const double p = V0.P[id];
+        phi[id] = p;
+        phi0[id] = __dsub_rn(p, phi0[id]);
+    }
+    if (threadIdx.x == 0 && sweeps_out) *sweeps_out = s;
 }
 
 // Strided injection (OP_2htoh_lvl0 / OP_4htoh / OP_8htoh)

@@ -124,6 +124,9 @@ def test_rk4_jacobi32_config0_100_steps():
     errs = state_rel(g, r)
     assert max(errs) < TOL64, errs
     assert rel(gphi, o.get_phi()) < TOL64
+    # the same window in FP32 bulk against this FP64 oracle run
+    e = fp32_vs_fp64_errors(w, 32, steps, ref=(r, o.get_phi()))
+    assert max(e.values()) < TOL32, e
 
 
 def test_rk4_fas128_config1_20_steps():
@@ -153,6 +156,9 @@ def test_rk4_fas128_config1_20_steps():
     assert rel(np.exp(bind.c2r(g[3])), np.exp(bind.c2r(r[3]))) < TOL64
     assert rel(gphi, o.get_phi()) < TOL64
     assert gd.total_iterations == o.stats().total_iterations
+    # the same window in FP32 bulk against this FP64 oracle run
+    e = fp32_vs_fp64_errors(w, n, steps, ref=(r, o.get_phi()))
+    assert max(e.values()) < TOL32, e
 
 
 @pytest.mark.parametrize("n,steps", [(64, 3), (128, 1)])
@@ -177,31 +183,35 @@ def test_rk4_fas_vs_oracle(n, steps):
     assert rel(gphi, o.get_phi()) < TOL64
 
 
-def fp32_vs_fp64_errors(w, n, steps):
+def fp32_vs_fp64_errors(w, n, steps, ref=None):
     """FP32-bulk GPU run against the FP64 oracle (residual 1e-10) of the same
     inputs: relative max-norm errors of n = e^s, of the total velocity
-    M e_x + u' (three components together) and of phi."""
+    M e_x + u' (three components together) and of phi.  `ref` = (state, phi)
+    of an FP64 oracle run of these inputs already made."""
     st, nd, mask, dt = C.make_inputs(w, n=n)
-    cfg32 = C.config_for(w, n=n)
+    cfg32 = C.config_for(w, n=n, precision=kf.KF_FP32_BULK)
     cfg64 = C.config_for(w, n=n, precision=kf.KF_FP64)
-    assert cfg32.precision == kf.KF_FP32_BULK and cfg64.res_tol == 1e-10
+    assert cfg64.res_tol == 1e-10 and cfg32.res_tol == C.fp32_res_tol(w["Q"], w["sigma"])
     with kf.Context(cfg32) as ctx:
         ctx.set_state(*st)
         ctx.set_sources(nd, mask)
         ctx.rk4(dt, steps)
         g = ctx.get_state()
         gphi = ctx.get_phi()
-    o = oracle_for(cfg64)
-    o.set_state(st)
-    o.set_sources(nd, mask)
-    o.rk4(dt, steps)
-    r = o.get_state()
+        assert ctx.diag().not_converged == 0
+    if ref is None:
+        o = oracle_for(cfg64)
+        o.set_state(st)
+        o.set_sources(nd, mask)
+        o.rk4(dt, steps)
+        ref = (o.get_state(), o.get_phi())
+    r, ophi = ref
     ug = np.stack([bind.c2r(x) for x in g[:3]])
     ur = np.stack([bind.c2r(x) for x in r[:3]])
     ug[0] += w["M"]
     ur[0] += w["M"]
     return {"n": rel(np.exp(bind.c2r(g[3])), np.exp(bind.c2r(r[3]))), "u": rel(ug, ur),
-            "phi": rel(gphi, o.get_phi())}
+            "phi": rel(gphi, ophi)}
 
 
 def test_fp32_bulk_vs_fp64_oracle():

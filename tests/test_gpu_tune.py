@@ -117,6 +117,50 @@ def test_rk4_streaming_smoother_bit_identical(prec):
     assert np.array_equal(p8, p0) and c8 == c0
 
 
+@pytest.mark.parametrize("n,levels,prec", [(64, 4, kf.KF_FP64), (256, 6, kf.KF_FP32_BULK)])
+def test_coarse_block_bit_identical(n, levels, prec):
+    """Captured FAS steps whose cycle reaches 8^3 (64-32-16-8, and the 6-level
+    256^3 cycle): the 16^3 and 8^3 levels in one shared-memory block give the
+    state, potential and V-cycle counts of the level-by-level kernels."""
+    steps = 2 if n == 64 else 1
+    w = C.WORKLOADS["fas128"] if n == 64 else C.WORKLOADS["fp32bulk256"]
+    st, nd, mask, dt = C.make_inputs(w, n=n)
+    cfg = C.config_for(w, n=n, precision=prec, mg_levels=levels)
+    res = {}
+    for on in (False, True):
+        with kf.Context(cfg) as ctx:
+            ctx.set_coarse_block(on)
+            ctx.set_state(*st)
+            ctx.set_sources(nd, mask)
+            ctx.rk4(dt, steps)
+            d = ctx.diag()
+            res[on] = (ctx.get_state(), ctx.get_phi(), d.total_iterations, d.not_converged)
+    (sa, pa, ca, na), (sb, pb, cb, nb) = res[False], res[True]
+    assert all(np.array_equal(a, b) for a, b in zip(sa, sb))
+    assert np.array_equal(pa, pb) and ca == cb and na == nb == 0
+
+
+def test_coarse_block_vs_oracle():
+    """The 4-level cycle at 64^3 (coarsest 8^3, levels 16 and 8 in the
+    block) against the oracle: 3 FP64 steps at 1e-12, equal V-cycle count."""
+    n, steps = 64, 3
+    w = C.WORKLOADS["fas128"]
+    st, nd, mask, dt = C.make_inputs(w, n=n)
+    cfg = C.config_for(w, n=n, mg_levels=4)
+    with kf.Context(cfg) as ctx:
+        ctx.set_state(*st)
+        ctx.set_sources(nd, mask)
+        ctx.rk4(dt, steps)
+        g, gphi, it = ctx.get_state(), ctx.get_phi(), ctx.diag().total_iterations
+    o = oracle_for(cfg)
+    o.set_state(st)
+    o.set_sources(nd, mask)
+    o.rk4(dt, steps)
+    assert max(state_rel(g, o.get_state())) < TOL64
+    assert rel(gphi, o.get_phi()) < TOL64
+    assert it == o.stats().total_iterations
+
+
 def test_autotune_keeps_state_and_steps():
     """kf_autotune on a 64^3 FP32-bulk context between captured steps: state,
     potential and time unchanged; the following steps equal those of a context
@@ -154,3 +198,4 @@ def test_set_tuning_rejects_other_values():
         for args in ((2, 8), (0, 6), (-1, 16)):
             with pytest.raises(kf.KfError):
                 ctx.set_tuning(*args)
+        assert ctx.L.kf_set_coarse_block(ctx.h, 2) == -1  # KF_ERR_ARG
