@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--coarse-block", type=int, default=1, choices=[0, 1],
                     help="kf_set_coarse_block: 1 (the default) runs the V-cycle's levels of at most "
                          "16^3 points in one shared-memory block, 0 level by level")
+    ap.add_argument("--overlap", type=int, default=1, choices=[0, 1],
+                    help="kf_set_overlap: 1 (the default) runs the u', s transforms of each stage beside "
+                         "its Poisson solve, 0 after it")
     ap.add_argument("--profile-range", action="store_true",
                     help="bracket the first arm's profile steps (launched kernel by kernel, the same "
                          "kernels as the timed graph replays) with cudaProfilerStart/Stop, for "
@@ -327,6 +330,7 @@ def run_kf(args):
             ctx.set_tuning(tune["fft_plan"], args.rbgs_rows)
             tune = dict(tune, rbgs_rows=args.rbgs_rows)
         ctx.set_coarse_block(args.coarse_block == 1)
+        ctx.set_overlap(args.overlap == 1)
         ctx.rk4(dt, args.warmup)
         ctx.synchronize()
         barrier()
@@ -474,7 +478,7 @@ def run_kf(args):
         "config": workload_config(w, args.workload, ws),
         "tuning": {"fft_radices": tune32["fft_radices"][tune32["fft_plan"]], "rbgs_rows": tune32["rbgs_rows"],
                    "rbgs_rows_meaning": "0: streaming TMA-staged sweep (k_rbgs_march)",
-                   "coarse_block": args.coarse_block},
+                   "coarse_block": args.coarse_block, "overlap": args.overlap},
         "gpu_launches": launches,
         "roofline": roofline,
         "cpu_baseline": cpu,

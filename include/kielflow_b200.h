@@ -288,6 +288,13 @@ int kf_set_tuning(kf_ctx *ctx, int fft_plan, int rbgs_rows);
  * potentials are the same bit for bit.  KF_ERR_ARG for other values. */
 int kf_set_coarse_block(kf_ctx *ctx, int on);
 
+/* In the captured step (kf_rk4_steps, kf_step_host, kf_batch_rk4_steps), the
+ * transforms of u' and s that feed the products do not depend on phi: on = 1
+ * (the default) runs them on a second stream of the context beside each
+ * stage's Poisson solve, on = 0 after it.  Same kernels and inputs, so the
+ * same results bit for bit.  KF_ERR_ARG for other values. */
+int kf_set_overlap(kf_ctx *ctx, int on);
+
 /* interface_poisson_solver::solve (interface_poisson_solver.hpp:18): phi_io is
  * the initial guess and the result, rho is read only; host arrays, n^3 doubles. */
 int kf_poisson_solve(kf_ctx *ctx, double *phi_io, const double *rho);

@@ -137,7 +137,7 @@ EXPORTS = [
     "kf_profile_enable", "kf_profile_read", "kf_profile_class_name", "kf_fft_r2c_noalloc", "kf_adjoint_run",
     "kf_batch_rk4_steps", "kf_set_state_linear", "kf_get_output", "kf_run", "kf_save", "kf_load",
     "kf_file_info_read", "kf_frontend_state", "kf_step_host", "kf_autotune", "kf_set_tuning",
-    "kf_set_coarse_block",
+    "kf_set_coarse_block", "kf_set_overlap",
 ]
 KCLASSES = 19
 
@@ -193,6 +193,7 @@ def load_library():
     L.kf_autotune.argtypes = [vp, ctypes.c_int, ctypes.POINTER(TuneOut)]
     L.kf_set_tuning.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     L.kf_set_coarse_block.argtypes = [vp, ctypes.c_int]
+    L.kf_set_overlap.argtypes = [vp, ctypes.c_int]
     L.kf_adjoint_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, _D,
                                  ctypes.POINTER(GradOut), _D, _D]
     _lib = L
@@ -360,6 +361,12 @@ class Context:
         (when a level lies below them) as one shared-memory block (True, the
         default) or level by level (False); bit-identical potentials."""
         self._check(self.L.kf_set_coarse_block(self.h, 1 if on else 0))
+
+    def set_overlap(self, on: bool):
+        """kf_set_overlap: in the captured step, run the u' and s transforms
+        beside the Poisson solve on a second stream (True, the default) or
+        after it (False); bit-identical results."""
+        self._check(self.L.kf_set_overlap(self.h, 1 if on else 0))
 
     def rk4(self, dt: float, nsteps: int = 1):
         self._check(self.L.kf_rk4_steps(self.h, nsteps, dt))

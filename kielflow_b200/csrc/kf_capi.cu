@@ -54,6 +54,7 @@ struct LevelBuf {
 
 constexpr int RBS = 256;  // reduction block size
 
+
 struct AdjState;  // discrete-adjoint buffers (allocated by the first kf_adjoint_run)
 struct OutState;  // output buffers of kf_run / kf_get_output (allocated on first use)
 
@@ -148,6 +149,11 @@ struct kf_ctx {
     // time / warm-start history and solve statistics live on the device
     bool capturing = false;
     cudaStream_t st_body = nullptr;  // stream on which conditional bodies are captured
+    // round D's transforms of u' and s, which do not depend on phi, run in a
+    // captured step on st_side beside the Poisson solve (kf_set_overlap)
+    bool overlap_d = true;
+    cudaStream_t st_side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     DevTime *dtime = nullptr;
     DevPois *dpois = nullptr;
     DevPois hpois{};  // last values read back
@@ -1126,7 +1132,42 @@ template <typename T, int N> struct Impl {
 
     // rounds A (P s, d_x s, d_y s and s_d = c2r(P s)), the Poisson solve and
     // B (phi^ = r2c(phi)), shared by both right-hand sides
-    static void rounds_AB(kf_ctx *c) {
+    // Round D's jobs on u' and s (the first 6 x, 9 y and 8 z jobs of its
+    // lists): every input is the stage state or round A's output.
+    static void round_D_us(kf_ctx *c) {
+        axis(c, c->jD_x, 6, 0, +1);
+        axis(c, c->jD_y, 9, 1, +1);
+        zc2r(c, c->zD, 8);
+    }
+
+    // In a captured step, fork round_D_us onto st_side after round A; rhs
+    // joins it before the products.  The branch writes CX[2..7], CY[3..11]
+    // and R[1..15], which nothing between the fork and the join touches (the
+    // Poisson solve, round B in CX[8] / CY[12], k_lin, round D's LIN part).
+    // (Measured at 256^3 FP32 bulk: +1 to +2.4 % per step; the Poisson chain
+    // at a higher stream priority than the branch was slower than equal
+    // priorities, and the branch's transform passes on half the persistent
+    // grid were no faster.)
+    static bool fork_D(kf_ctx *c) {
+        if (!(c->capturing && c->overlap_d)) return false;
+        CK(cudaEventRecord(c->ev_fork, c->st));
+        CK(cudaStreamWaitEvent(c->st_side, c->ev_fork, 0));
+        if (c->capture_wait_u && c->stage_idx == 0)
+            CK(cudaStreamWaitEvent(c->st_side, c->ev_u, cudaEventWaitExternal));
+        cudaStream_t main = c->st;
+        c->st = c->st_side;
+        try {
+            round_D_us(c);
+        } catch (...) {
+            c->st = main;
+            throw;
+        }
+        c->st = main;
+        CK(cudaEventRecord(c->ev_join, c->st_side));
+        return true;
+    }
+
+    static bool rounds_AB(kf_ctx *c, bool fork = false) {
         const int Tm = c->cfg.terms;
         const bool pen = Tm & T_PENALIZATION;
         const bool pois = (Tm & T_POISSON) && (Tm & T_E_INT);
@@ -1134,6 +1175,7 @@ template <typename T, int N> struct Impl {
         axis(c, c->jA_x, 2, 0, +1);
         axis(c, c->jA_y, 3, 1, +1);
         if (pois || pen) zc2r(c, c->zA, 1);
+        const bool forked = fork && fork_D(c);
         if (pois && !c->phi_given) {
             {
                 Launch L_(c, KC_RHO, (double)c->N * (sizeof(T) + 16));
@@ -1164,23 +1206,33 @@ template <typename T, int N> struct Impl {
             axis(c, c->jB_y, 1, 1, -1);
             axis(c, c->jB_x, 1, 0, -1);
         }
+        return forked;
     }
 
     // one right-hand-side evaluation: Ys -> K
     static void rhs(kf_ctx *c) {
         const int Tm = c->cfg.terms;
         const bool pen = Tm & T_PENALIZATION;
-        rounds_AB(c);
+        const bool forked = rounds_AB(c, true);
         // C
         if (pen) {
             Launch L_(c, KC_LIN, (double)c->Nc * (9 * sizeof(T2) + 2 * sizeof(T)));
             k_lin<T><<<mg_grid(NZC, N), mg_block(), 0, c->st>>>(rargs(c), geo(c), (T2 *)c->LIN[0], (T2 *)c->LIN[1],
                                                                (T2 *)c->LIN[2], (T2 *)c->LIN[3]);
         }
-        // D
-        axis(c, c->jD_x, pen ? 10 : 6, 0, +1);
-        axis(c, c->jD_y, pen ? 13 : 9, 1, +1);
-        zc2r(c, c->zD, pen ? 10 : 8);
+        // D: the u', s part (unless forked) and the linear terms' part
+        if (!forked) {
+            axis(c, c->jD_x, pen ? 10 : 6, 0, +1);
+            axis(c, c->jD_y, pen ? 13 : 9, 1, +1);
+            zc2r(c, c->zD, pen ? 10 : 8);
+        } else {
+            if (pen) {
+                axis(c, c->jD_x + 6, 4, 0, +1);
+                axis(c, c->jD_y + 9, 4, 1, +1);
+                zc2r(c, c->zD + 8, 2);
+            }
+            CK(cudaStreamWaitEvent(c->st, c->ev_join, 0));
+        }
         // E
         ProdArgs<T> pa;
         for (int q = 0; q < 3; ++q) {
@@ -1571,6 +1623,7 @@ void build_tables(kf_ctx *c) {
 
 void cc_setup(kf_ctx *c);
 
+
 void build_levels(kf_ctx *c) {
     const kf_config &cf = c->cfg;
     int nl = 1;
@@ -1685,11 +1738,11 @@ void build_jobs(kf_ctx *c) {
     zj(CY[0], MUL_NONE, nullptr, 0, R[0], nullptr);
     // B
     c->zB = (int)Z.size();
-    zj(c->phiT, 0, nullptr, 0, CX[2], nullptr);
+    zj(c->phiT, 0, nullptr, 0, CX[8], nullptr);  // CX[8], CY[12]: not written by round D's u', s part
     c->jB_y = (int)J.size();
-    aj(CX[2], CY[3], MUL_NONE);
+    aj(CX[8], CY[12], MUL_NONE);
     c->jB_x = (int)J.size();
-    aj(CY[3], c->phihat, MUL_NONE);
+    aj(CY[12], c->phihat, MUL_NONE);
     // D
     c->jD_x = (int)J.size();
     for (int q = 0; q < 3; ++q) {
@@ -1847,6 +1900,9 @@ void create(kf_ctx *c) {
     CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
     c->own_stream = true;
     CK(cudaStreamCreateWithFlags(&c->st_body, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&c->st_side, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
     const size_t cb = c->cs * c->Nc, rb = c->es * c->N;
     for (int q = 0; q < 4; ++q) {
         c->Y[q] = dalloc<void>(c, cb);
@@ -2299,6 +2355,9 @@ int kf_ctx_destroy(kf_ctx *c) {
     if (c->ev_u) cudaEventDestroy(c->ev_u);
     if (c->st_copy) cudaStreamDestroy(c->st_copy);
     if (c->st_body) cudaStreamDestroy(c->st_body);
+    if (c->st_side) cudaStreamDestroy(c->st_side);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
     adj_release(c);
     out_release(c);
     for (void *p : c->allocs) cudaFree(p);
@@ -2440,6 +2499,16 @@ int kf_set_coarse_block(kf_ctx *c, int on) {
         if (c->coarse_block == (on == 1)) return;
         c->coarse_block = on == 1;
         cc_setup(c);
+        drop_graphs(c);
+    });
+}
+
+int kf_set_overlap(kf_ctx *c, int on) {
+    return guarded(c, [&] {
+        if (on != 0 && on != 1) throw KfError{KF_ERR_ARG, "kf_set_overlap: on is 0 or 1"};
+        if (c->capturing) throw KfError{KF_ERR_ARG, "kf_set_overlap during a capture"};
+        if (c->overlap_d == (on == 1)) return;
+        c->overlap_d = on == 1;
         drop_graphs(c);
     });
 }

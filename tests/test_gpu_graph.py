@@ -84,3 +84,30 @@ def test_step_host_matches_set_step_get(name, nsteps):
     for a, b in zip(out[0][0], out[1][0]):
         assert np.array_equal(a, b)
     assert np.array_equal(out[0][1], out[1][1])
+
+
+@pytest.mark.parametrize("name,n,host_call", [("fp32bulk256", 256, False), ("fas128", 64, True),
+                                              ("fp32bulk256", 32, True)])
+def test_overlap_on_off_identical(name, n, host_call):
+    """The u', s transforms forked beside the Poisson solve (kf_set_overlap 1)
+    against the same step with them after it (0): identical states and
+    potentials, through kf_rk4_steps and through kf_step_host (whose stage 1
+    also waits for the upload of u')."""
+    w = C.WORKLOADS[name]
+    st, nd, mask, dt = C.make_inputs(w, n)
+    out = []
+    for on in (True, False):
+        with kf.Context(C.config_for(w, n)) as ctx:
+            ctx.set_overlap(on)
+            ctx.set_sources(nd, mask)
+            if host_call:
+                arrays = [np.ascontiguousarray(x).copy() for x in st]
+                ctx.step_host(arrays, dt, 2)
+            else:
+                ctx.set_state(*st)
+                ctx.rk4(dt, 1)
+                arrays = ctx.get_state()
+            out.append((arrays, ctx.get_phi()))
+    for a, b in zip(out[0][0], out[1][0]):
+        assert np.array_equal(a, b)
+    assert np.array_equal(out[0][1], out[1][1])
