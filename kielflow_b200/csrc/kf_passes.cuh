@@ -124,13 +124,13 @@ template <typename T> struct AxisTile {
     bool valid;
 };
 
+// Tile `tile` of job `job` (global tile index tile * njobs + job), column c.
 template <typename T, int N>
-__device__ __forceinline__ AxisTile<T> axis_tile(const AxisJob *__restrict__ jobs, int njobs, int axis, int t,
-                                                 int c, int n, int nzc) {
+__device__ __forceinline__ AxisTile<T> axis_tile(const AxisJob *__restrict__ jobs, int job, int tile, int axis,
+                                                 int c) {
     typedef typename C2<T>::type T2;
-    constexpr int TC = Tile<T>::TC;
+    constexpr int TC = Tile<T>::TC, n = N, nzc = N / 2 + 1;
     AxisTile<T> G;
-    const int job = t % njobs, tile = t / njobs;
     const AxisJob J = jobs[job];
     G.in = static_cast<const T2 *>(J.in);
     G.out = static_cast<T2 *>(J.out);
@@ -145,7 +145,7 @@ __device__ __forceinline__ AxisTile<T> axis_tile(const AxisJob *__restrict__ job
         G.jj = col / nzc;
         G.kk = col - G.jj * nzc;
     } else {
-        const int tpp = (nzc + TC - 1) / TC;
+        constexpr int tpp = (nzc + TC - 1) / TC;
         const int plane = tile / tpp;
         G.kk = (tile - plane * tpp) * TC + c;
         G.valid = G.kk < nzc;
@@ -201,12 +201,26 @@ k_axis_pipe(const AxisJob *__restrict__ jobs, int njobs, int axis, Geo<T> g,
     const int c = threadIdx.x % TC, p = threadIdx.x / TC;
     int t = blockIdx.x;
     if (t >= total) return;
+    // (job, tile) of global tile t = tile * njobs + job, advanced by the grid
+    // stride without a division per tile: for the tile being transformed (c*)
+    // and for the next one to stage (p*)
+    const int GS = gridDim.x, Gq = GS / njobs, Gr = GS - Gq * njobs;
+    auto adv = [&](int &j, int &tl) {
+        j += Gr;
+        tl += Gq;
+        if (j >= njobs) {
+            j -= njobs;
+            ++tl;
+        }
+    };
+    int cj = t % njobs, ct = t / njobs;
+    int pj = cj, pt = ct, ptt = t;
     // Each thread stages exactly the elements it reads back, so the slots need
     // no barrier.  One commit group per tile (empty past the end), so that
     // cp.async.wait_group D - 1 always leaves the current tile complete.
-    auto prefetch = [&](int tt, int slot) {
-        if (tt < total) {
-            const AxisTile<T> G = axis_tile<T, N>(jobs, njobs, axis, tt, c, g.n, g.nzc);
+    auto prefetch = [&](int slot) {
+        if (ptt < total) {
+            const AxisTile<T> G = axis_tile<T, N>(jobs, pj, pt, axis, c);
             T2 *st = stg0 + slot * (N * TC);
 #pragma unroll
             for (int q = 0; q < E; ++q) {
@@ -219,12 +233,15 @@ k_axis_pipe(const AxisJob *__restrict__ jobs, int njobs, int axis, Geo<T> g,
             }
         }
         cp_async_commit();
+        ptt += GS;
+        adv(pj, pt);
     };
 #pragma unroll
-    for (int d = 0; d < D; ++d) prefetch(t + d * (int)gridDim.x, d);
-    for (int it = 0; t < total; t += gridDim.x, ++it) {
+    for (int d = 0; d < D; ++d) prefetch(d);
+    for (int it = 0; t < total; t += GS, ++it) {
         const int slot = it % D;
-        const AxisTile<T> cur = axis_tile<T, N>(jobs, njobs, axis, t, c, g.n, g.nzc);
+        const AxisTile<T> cur = axis_tile<T, N>(jobs, cj, ct, axis, c);
+        adv(cj, ct);
         // the 2/3 rule of this column as an index bound (one table read per tile)
         const int pbnd = cur.valid && (cur.mul == MUL_P || cur.mul == MUL_P_IK)
                              ? dealias_bound(g.pb, cur.jj, cur.kk, g.nzc)
@@ -242,7 +259,7 @@ k_axis_pipe(const AxisJob *__restrict__ jobs, int njobs, int axis, Geo<T> g,
             if (cur.mul == MUL_P_IK || cur.mul == MUL_IK) x = mul_ik(x, g.kv[row]);
             v[q] = x;
         }
-        prefetch(t + D * (int)gridDim.x, slot);
+        prefetch(slot);
         PlanV<N, V>::template fft<T2, SIGN>(v, sm + c, StrideAddr{TC}, p, tw);
         if (cur.valid) {
 #pragma unroll
@@ -260,7 +277,12 @@ k_axis_pipe(const AxisJob *__restrict__ jobs, int njobs, int axis, Geo<T> g,
 // the kz = 0 and kz = n/2 bins are dropped, as a c2r transform does), packed
 // as A + iB, transformed backwards and written as two real rows scaled by
 // `scale` (the 1/N of OP_iFFT.cpp:59-61).
-template <typename T> struct ZTile { static constexpr int LZ = 8; };
+// Line pairs per z-pass block (4 and 16 measured no faster than 8 at 256^3:
+// the c2r launches took 7.36 and 8.01 ms against 7.33 ms over 20 steps).
+#ifndef KF_ZLZ
+#define KF_ZLZ 8
+#endif
+template <typename T> struct ZTile { static constexpr int LZ = KF_ZLZ; };
 
 // Shared memory of a z pass: its line buffers (the c2r staging of two half
 // spectra per line pair, reused by the transform).
