@@ -200,7 +200,7 @@ enum KCls { KC_AXIS_INV, KC_AXIS_FWD, KC_Z_C2R, KC_Z_R2C, KC_XASM, KC_PROD, KC_L
 const char *const kKClsName[KC_N] = {"k_axis_pass(inverse)", "k_axis_pass(forward)", "k_z_c2r", "k_z_r2c",
                                      "k_xfwd_assemble", "k_products", "k_lin", "k_rho", "k_rk", "k_jacobi",
                                      "k_rbgs", "k_residual", "k_restrict/k_fas_rhs/k_prolong/k_inject",
-                                     "k_coarse_solve", "k_reduce_final", "conversion/diagnostics",
+                                     "k_coarse_solve/k_coarse_cycle", "k_reduce_final", "conversion/diagnostics",
                                      "adjoint pointwise (k_prod_vjp/k_vjp_assemble/k_adj_stage/...)",
                                      "adjoint Poisson (linear multigrid)",
                                      "FAS levels below the finest (k_rbgs/k_residual/transfers)",

@@ -251,6 +251,9 @@ __global__ void k_extrap(double *__restrict__ phi, double *__restrict__ phi_a, d
 // Red-black Gauss-Seidel-Newton half sweep (colour (i+j+k)%2): one Newton
 // step per point; grid over (k/2, j, i), blocks of 32 x BY (the tile shape
 // kf_autotune chooses; the arithmetic does not depend on it).
+// The point's index and its six periodic neighbours' are one 32-bit base and
+// wrapped offsets (n^3 < 2^31 for every supported n <= 256): the loads, the
+// sum and its order are point_coeffs_fast's, with fewer integer instructions.
 template <int BY = 8>
 __global__ void __launch_bounds__(32 * BY) k_rbgs(double *__restrict__ phi, const double *__restrict__ rho, Lev L,
                                                   int color, double om) {
@@ -258,9 +261,19 @@ __global__ void __launch_bounds__(32 * BY) k_rbgs(double *__restrict__ phi, cons
     const int k2 = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * BY + threadIdx.y, i = blockIdx.z;
     if (2 * k2 >= n || j >= n) return;
     const int k = 2 * k2 + ((i + j + color) & 1);
-    double A, D;
-    point_coeffs_fast(phi, rho, L, i, j, k, A, D);
-    const long q = lidx(i, j, k, n);
+    const int nn = n * n;
+    const int q = (i * n + j) * n + k;
+    const int oip = i == n - 1 ? -(n - 1) * nn : nn, oim = i == 0 ? (n - 1) * nn : -nn;
+    const int ojp = j == n - 1 ? -(n - 1) * n : n, ojm = j == 0 ? (n - 1) * n : -n;
+    const int okp = k == n - 1 ? -(n - 1) : 1, okm = k == 0 ? n - 1 : -1;
+    const double D = __dadd_rn(__dadd_rn(L.dd[i], L.dd[j]), L.dd[k]);
+    double A = __dmul_rn(phi[q + oip], L.ip[i]);
+    A = __dadd_rn(A, __dmul_rn(phi[q + oim], L.im[i]));
+    A = __dadd_rn(A, __dmul_rn(phi[q + ojp], L.ip[j]));
+    A = __dadd_rn(A, __dmul_rn(phi[q + ojm], L.im[j]));
+    A = __dadd_rn(A, __dmul_rn(phi[q + okp], L.ip[k]));
+    A = __dadd_rn(A, __dmul_rn(phi[q + okm], L.im[k]));
+    A = __dadd_rn(A, rho[q]);
     phi[q] = newton_step(phi[q], A, D, om);
 }
 
@@ -275,9 +288,12 @@ __global__ void __launch_bounds__(32 * BY) k_rbgs(double *__restrict__ phi, cons
 // per column.  The arithmetic and its order are those of point_coeffs_fast,
 // so the results are bit-identical.  Requires n/2 a multiple of 32 (whole
 // warps along k), BY | n and PI | n.
-__device__ __forceinline__ double2 ld_pair(const double *p, int i, int j, int ka, int n) {
-    return *reinterpret_cast<const double2 *>(p + lidx(i, j, ka, n));
-}
+// Resident blocks per SM asked of the register allocator for k_residual_col
+// (measured at 256^3, 36 launches: 1 -> 120 registers, 4.09 ms; 4 -> 64
+// registers with a 40-byte spill, 3.42 ms).
+#ifndef KF_RESCOL_MINB
+#define KF_RESCOL_MINB 4
+#endif
 
 // The residual r = f(phi) of both points of the pair at every plane of the
 // column (16-byte loads of the pairs of rows j, j -+ 1 and of rho, one 16-byte
@@ -286,7 +302,7 @@ __device__ __forceinline__ double2 ld_pair(const double *p, int i, int j, int ka
 // LIN: the adjoint's linear residual A - (D + cl) psi (k_residual_lin,
 // k_resmax_lin).
 template <int BY, int PI, bool MAX, bool LIN = false, bool STORE = true>
-__global__ void __launch_bounds__(32 * BY) k_residual_col(const double *__restrict__ phi, const double *__restrict__ rho,
+__global__ void __launch_bounds__(32 * BY, KF_RESCOL_MINB) k_residual_col(const double *__restrict__ phi, const double *__restrict__ rho,
                                                           Lev L, double *__restrict__ r,
                                                           unsigned long long *__restrict__ slots,
                                                           const double *__restrict__ cl = nullptr) {
@@ -299,18 +315,25 @@ __global__ void __launch_bounds__(32 * BY) k_residual_col(const double *__restri
     const double dda = L.dd[ka], ipa = L.ip[ka], ima = L.im[ka];
     const double ddb = L.dd[kb], ipb = L.ip[kb], imb = L.im[kb];
     const double ddj = L.dd[j], ipj = L.ip[j], imj = L.im[j];
-    double2 pm = ld_pair(phi, wrapi(i0 - 1, n), j, ka, n), pc = ld_pair(phi, i0, j, ka, n);
+    // 32-bit element indices (n^3 < 2^31 for every supported n): q = the
+    // pair at (i, j, ka); the j, k and next-plane neighbours as offsets
+    const int nn = n * n, ojp = (jp - j) * n, ojm = (jm - j) * n, okl = kl - ka, okr = kr - ka;
+    int q = (i0 * n + j) * n + ka;
+    double2 pm = *reinterpret_cast<const double2 *>(phi + ((wrapi(i0 - 1, n) * n + j) * n + ka));
+    double2 pc = *reinterpret_cast<const double2 *>(phi + q);
     double af = 0.;
 #pragma unroll 2
     for (int ii = 0; ii < PI; ++ii) {
         const int i = i0 + ii;
-        const double2 pn = ld_pair(phi, i + 1 == n ? 0 : i + 1, j, ka, n);
-        const double2 pjp = ld_pair(phi, i, jp, ka, n), pjm = ld_pair(phi, i, jm, ka, n);
-        const double2 rr = ld_pair(rho, i, j, ka, n);
+        const int qn = i + 1 == n ? q - (n - 1) * nn : q + nn;
+        const double2 pn = *reinterpret_cast<const double2 *>(phi + qn);
+        const double2 pjp = *reinterpret_cast<const double2 *>(phi + q + ojp);
+        const double2 pjm = *reinterpret_cast<const double2 *>(phi + q + ojm);
+        const double2 rr = *reinterpret_cast<const double2 *>(rho + q);
         double fromR = __shfl_down_sync(0xffffffffu, pc.x, 1);
         double fromL = __shfl_up_sync(0xffffffffu, pc.y, 1);
-        if (lane == 31) fromR = phi[lidx(i, j, kr, n)];
-        if (lane == 0) fromL = phi[lidx(i, j, kl, n)];
+        if (lane == 31) fromR = phi[q + okr];
+        if (lane == 0) fromL = phi[q + okl];
         const double ipi = L.ip[i], imi = L.im[i], ddi = L.dd[i];
         double Aa = __dmul_rn(pn.x, ipi);
         Aa = __dadd_rn(Aa, __dmul_rn(pm.x, imi));
@@ -329,17 +352,18 @@ __global__ void __launch_bounds__(32 * BY) k_residual_col(const double *__restri
         const double Da = __dadd_rn(__dadd_rn(ddi, ddj), dda), Db = __dadd_rn(__dadd_rn(ddi, ddj), ddb);
         double fa, fb;
         if constexpr (LIN) {
-            const double2 cp = ld_pair(cl, i, j, ka, n);
+            const double2 cp = *reinterpret_cast<const double2 *>(cl + q);
             fa = __dsub_rn(Aa, __dmul_rn(__dadd_rn(Da, cp.x), pc.x));
             fb = __dsub_rn(Ab, __dmul_rn(__dadd_rn(Db, cp.y), pc.y));
         } else {
             fa = f_point(Aa, Da, pc.x);
             fb = f_point(Ab, Db, pc.y);
         }
-        if (STORE) *reinterpret_cast<double2 *>(r + lidx(i, j, ka, n)) = make_double2(fa, fb);
+        if (STORE) *reinterpret_cast<double2 *>(r + q) = make_double2(fa, fb);
         if (MAX) af = nmax(af, nmax(fabs(fa), fabs(fb)));
         pm = pc;
         pc = pn;
+        q = qn;
     }
     if constexpr (MAX) {
         __shared__ double sh[BY];
