@@ -119,7 +119,7 @@ template <typename T> struct AxisTile {
     typedef typename C2<T>::type T2;
     const T2 *in;
     T2 *out;
-    long base, rstride;
+    int base, rstride;  // element indices: n * n * (n/2 + 1) < 2^31 for every supported n
     int jj, kk, mul;
     bool valid;
 };
@@ -141,7 +141,7 @@ __device__ __forceinline__ AxisTile<T> axis_tile(const AxisJob *__restrict__ job
         const int col = tile * TC + c;
         G.valid = col < n * nzc;
         G.base = col;
-        G.rstride = (long)n * nzc;
+        G.rstride = n * nzc;
         G.jj = col / nzc;
         G.kk = col - G.jj * nzc;
     } else {
@@ -149,7 +149,7 @@ __device__ __forceinline__ AxisTile<T> axis_tile(const AxisJob *__restrict__ job
         const int plane = tile / tpp;
         G.kk = (tile - plane * tpp) * TC + c;
         G.valid = G.kk < nzc;
-        G.base = (long)plane * n * nzc + G.kk;
+        G.base = plane * n * nzc + G.kk;
         G.rstride = nzc;
     }
     return G;
@@ -309,17 +309,22 @@ k_z_c2r(const ZJob *__restrict__ jobs, int njobs, int nrows, Geo<T> g,
     const T2 *inA = static_cast<const T2 *>(J.inA);
     const T2 *inB = static_cast<const T2 *>(J.inB);
     // raw half spectra -> shared memory with asynchronous copies (all of a
-    // thread's loads in flight at once); the multipliers are applied below
-    for (int idx = threadIdx.x; idx < 2 * LZ * NZC; idx += blockDim.x) {
-        const int which = idx / (LZ * NZC);
-        const int rem = idx - which * LZ * NZC;
-        const int l = rem / NZC, k = rem - l * NZC;
-        const int r = r0 + l;
-        const T2 *src = which ? inB : inA;
-        if (src && r < nrows)
-            cp_async_copy(half + idx, src + (long)r * NZC + k);
-        else
-            half[idx] = mk<T2>((T)0, (T)0);
+    // thread's loads in flight at once); the multipliers are applied below.
+    // The tile's LZ rows of a half spectrum are one contiguous run of
+    // LZ * NZC elements from row r0.
+    const int lim = (nrows - r0) * NZC;  // elements of the run inside the field
+    const long off = (long)r0 * NZC;
+    for (int e = threadIdx.x; e < LZ * NZC; e += blockDim.x) {
+        if (e < lim) {
+            cp_async_copy(half + e, inA + off + e);
+            if (inB)
+                cp_async_copy(half + LZ * NZC + e, inB + off + e);
+            else
+                half[LZ * NZC + e] = mk<T2>((T)0, (T)0);
+        } else {
+            half[e] = mk<T2>((T)0, (T)0);
+            half[LZ * NZC + e] = mk<T2>((T)0, (T)0);
+        }
     }
     cp_async_commit();
     cp_async_wait_all();
@@ -402,19 +407,18 @@ k_z_r2c(const ZJob *__restrict__ jobs, int njobs, int nrows,
 #pragma unroll
     for (int q = 0; q < E; ++q) line[pa(reg_row<N, P, PlanV<N, V>::RL>(p, q))] = v[q];
     __syncthreads();
-    for (int idx = threadIdx.x; idx < LZ * NZC; idx += blockDim.x) {
+    // the tile's LZ output rows of a half spectrum are one contiguous run of
+    // LZ * NZC elements from row r0
+    const int lim = (nrows - r0) * NZC;
+    T2 *oA = static_cast<T2 *>(J.outA) + (long)r0 * NZC;
+    T2 *oB = J.outB ? static_cast<T2 *>(J.outB) + (long)r0 * NZC : nullptr;
+    for (int idx = threadIdx.x; idx < LZ * NZC && idx < lim; idx += blockDim.x) {
         const int ll = idx / NZC, k = idx - ll * NZC;
-        const int rr = r0 + ll;
-        if (rr >= nrows) continue;
         const T2 zk = xch[ll * LS + pa(k)];
-        const T2 zm = xch[ll * LS + pa((N - k) % N)];
+        const T2 zm = xch[ll * LS + pa(k == 0 ? 0 : N - k)];
         const T cr = zm.x, ci = -zm.y;  // conj(Z[N-k])
-        T2 *oA = static_cast<T2 *>(J.outA) + (long)rr * NZC;
-        oA[k] = mk<T2>((T)0.5 * (zk.x + cr), (T)0.5 * (zk.y + ci));
-        if (J.outB) {
-            T2 *oB = static_cast<T2 *>(J.outB) + (long)rr * NZC;
-            oB[k] = mk<T2>((T)0.5 * (zk.y - ci), (T)-0.5 * (zk.x - cr));
-        }
+        oA[idx] = mk<T2>((T)0.5 * (zk.x + cr), (T)0.5 * (zk.y + ci));
+        if (oB) oB[idx] = mk<T2>((T)0.5 * (zk.y - ci), (T)-0.5 * (zk.x - cr));
     }
 }
 
