@@ -188,8 +188,21 @@ template <typename T, int N> inline size_t axis_pipe_smem(int) {
     return (1 + KF_PIPE_DEPTH) * (size_t)N * Tile<T>::TC * sizeof(typename C2<T>::type);
 }
 
+// Resident blocks per SM asked of the register allocator for k_axis_pipe
+// (0: no request; 3 fits the FP32 256-point pass in 80 registers without
+// spilling: its 48 inverse launches of 20 steps took 12.0-12.1 ms against
+// 13.7 ms with 125 registers and 2 blocks), and for the FP32 k_z_c2r (12
+// blocks, 40 registers with spills: 8.0 against 7.5 ms; not used).
+#ifndef KF_PIPE_MINB
+#define KF_PIPE_MINB 3
+#endif
+#ifndef KF_ZC2R_MINB
+#define KF_ZC2R_MINB 0
+#endif
+
 template <typename T, int N, int SIGN, int V = 0>
-__global__ void __launch_bounds__(Tile<T>::TC * PlanV<N, V>::P)
+__global__ void __launch_bounds__(Tile<T>::TC * PlanV<N, V>::P,
+                                  (KF_PIPE_MINB ? PipeMinBlocks<T, N, V, 1 + KF_PIPE_DEPTH, (KF_PIPE_MINB > 0 ? KF_PIPE_MINB : 1), 64>::value : 1))
 k_axis_pipe(const AxisJob *__restrict__ jobs, int njobs, int axis, Geo<T> g,
             const typename C2<T>::type *__restrict__ tw, int total) {
     typedef typename C2<T>::type T2;
@@ -294,7 +307,7 @@ template <typename T, int N, bool C2R> struct ZSmem {
 };
 
 template <typename T, int N, int V = 0>
-__global__ void __launch_bounds__(ZTile<T>::LZ * PlanV<N, V>::P)
+__global__ void __launch_bounds__(ZTile<T>::LZ * PlanV<N, V>::P, (sizeof(T) == 4 && KF_ZC2R_MINB > 0 ? KF_ZC2R_MINB : 1))
 k_z_c2r(const ZJob *__restrict__ jobs, int njobs, int nrows, Geo<T> g,
         const typename C2<T>::type *__restrict__ tw, T scale) {
     typedef typename C2<T>::type T2;
