@@ -16,6 +16,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <memory>
 #include <vector>
 
 #include <nvtx3/nvToolsExt.h>
@@ -49,10 +50,17 @@ struct LevelBuf {
     double *dd = nullptr, *dp = nullptr, *dm = nullptr, *ip = nullptr, *im = nullptr, *gam = nullptr;
     double *phi = nullptr, *rho = nullptr, *r = nullptr, *phi0 = nullptr;
     double *t = nullptr;  // second potential of the streaming smoother (k_rbgs_march), n >= MT_TK
+    std::shared_ptr<AxTab> tab;  // host copy of dd, ip, im for k_rbgs_t (n <= KF_TAB_N)
     Lev lev() const { return Lev{n, dd, dp, dm, ip, im}; }
 };
 
 constexpr int RBS = 256;  // reduction block size
+
+// Half sweeps with the i and j axis tables passed as a kernel parameter
+// (k_rbgs_t; 0: k_rbgs reads them from global memory).
+#ifndef KF_RBGS_TAB
+#define KF_RBGS_TAB 1
+#endif
 
 
 struct AdjState;  // discrete-adjoint buffers (allocated by the first kf_adjoint_run)
@@ -570,6 +578,13 @@ void smooth_plain(kf_ctx *c, LevelBuf &L, double *phi, const double *rho, const 
                     k_rbgs_lin<16><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color, om);
                 else
                     k_rbgs_lin<8><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color, om);
+            } else if (L.tab) {
+                if (by == 4)
+                    k_rbgs_t<4><<<g, b, 0, c->st>>>(phi, rho, L.lev(), color, om, *L.tab);
+                else if (by == 16)
+                    k_rbgs_t<16><<<g, b, 0, c->st>>>(phi, rho, L.lev(), color, om, *L.tab);
+                else
+                    k_rbgs_t<8><<<g, b, 0, c->st>>>(phi, rho, L.lev(), color, om, *L.tab);
             } else {
                 if (by == 4)
                     k_rbgs<4><<<g, b, 0, c->st>>>(phi, rho, L.lev(), color, om);
@@ -1670,6 +1685,14 @@ void build_levels(kf_ctx *c) {
         CK(cudaMemcpy(L.dp, dp.data(), 8 * n, cudaMemcpyHostToDevice));
         CK(cudaMemcpy(L.dm, dm.data(), 8 * n, cudaMemcpyHostToDevice));
         CK(cudaMemcpy(L.gam, gam.data(), 8 * n, cudaMemcpyHostToDevice));
+        if (KF_RBGS_TAB && n <= KF_TAB_N) {
+            L.tab = std::make_shared<AxTab>();
+            for (int m = 0; m < n; ++m) {
+                L.tab->dd[m] = dd[m];
+                L.tab->ip[m] = ip[m];
+                L.tab->im[m] = im[m];
+            }
+        }
         const size_t bytes = sizeof(double) * (size_t)n * n * n;
         L.r = dalloc<double>(c, bytes);
         if (cf.poisson_mode == KF_PS_FAS && march_level(L) && c->march_maps) {

@@ -251,6 +251,14 @@ __global__ void k_extrap(double *__restrict__ phi, double *__restrict__ phi_a, d
 // Red-black Gauss-Seidel-Newton half sweep (colour (i+j+k)%2): one Newton
 // step per point; grid over (k/2, j, i), blocks of 32 x BY (the tile shape
 // kf_autotune chooses; the arithmetic does not depend on it).
+// The axis tables of a level of at most 256 points per axis, passed by value
+// as a kernel parameter: entries read with a warp-uniform index (the i and j
+// of a half-sweep warp) come from the constant bank instead of L1.
+constexpr int KF_TAB_N = 256;
+struct AxTab {
+    double dd[KF_TAB_N], ip[KF_TAB_N], im[KF_TAB_N];
+};
+
 // The point's index and its six periodic neighbours' are one 32-bit base and
 // wrapped offsets (n^3 < 2^31 for every supported n <= 256): the loads, the
 // sum and its order are point_coeffs_fast's, with fewer integer instructions.
@@ -277,6 +285,30 @@ __global__ void __launch_bounds__(32 * BY) k_rbgs(double *__restrict__ phi, cons
     phi[q] = newton_step(phi[q], A, D, om);
 }
 
+// The same half sweep with the i and j tables from the constant bank (AxTab).
+template <int BY = 8>
+__global__ void __launch_bounds__(32 * BY) k_rbgs_t(double *__restrict__ phi, const double *__restrict__ rho, Lev L,
+                                                    int color, double om, const __grid_constant__ AxTab T) {
+    const int n = L.n;
+    const int k2 = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * BY + threadIdx.y, i = blockIdx.z;
+    if (2 * k2 >= n || j >= n) return;
+    const int k = 2 * k2 + ((i + j + color) & 1);
+    const int nn = n * n;
+    const int q = (i * n + j) * n + k;
+    const int oip = i == n - 1 ? -(n - 1) * nn : nn, oim = i == 0 ? (n - 1) * nn : -nn;
+    const int ojp = j == n - 1 ? -(n - 1) * n : n, ojm = j == 0 ? (n - 1) * n : -n;
+    const int okp = k == n - 1 ? -(n - 1) : 1, okm = k == 0 ? n - 1 : -1;
+    const double D = __dadd_rn(__dadd_rn(T.dd[i], T.dd[j]), L.dd[k]);
+    double A = __dmul_rn(phi[q + oip], T.ip[i]);
+    A = __dadd_rn(A, __dmul_rn(phi[q + oim], T.im[i]));
+    A = __dadd_rn(A, __dmul_rn(phi[q + ojp], T.ip[j]));
+    A = __dadd_rn(A, __dmul_rn(phi[q + ojm], T.im[j]));
+    A = __dadd_rn(A, __dmul_rn(phi[q + okp], L.ip[k]));
+    A = __dadd_rn(A, __dmul_rn(phi[q + okm], L.im[k]));
+    A = __dadd_rn(A, rho[q]);
+    phi[q] = newton_step(phi[q], A, D, om);
+}
+
 // ------------------------------------------------------------ column form
 // k_residual is bound by L1 throughput (about 17 loads per point: 7
 // potentials, rho, 9 axis-table entries, most strided).  In the column form a
@@ -289,8 +321,8 @@ __global__ void __launch_bounds__(32 * BY) k_rbgs(double *__restrict__ phi, cons
 // so the results are bit-identical.  Requires n/2 a multiple of 32 (whole
 // warps along k), BY | n and PI | n.
 // Resident blocks per SM asked of the register allocator for k_residual_col
-// (measured at 256^3, 36 launches: 1 -> 120 registers, 4.09 ms; 4 -> 64
-// registers with a 40-byte spill, 3.42 ms).
+// (measured at 256^3, 36 launches: 1 -> 120 registers, 4.09 ms; 3 -> 80
+// registers, 3.62 ms; 4 -> 64 registers with a 40-byte spill, 3.40 ms).
 #ifndef KF_RESCOL_MINB
 #define KF_RESCOL_MINB 4
 #endif
