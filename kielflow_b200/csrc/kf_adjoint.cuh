@@ -294,6 +294,34 @@ __global__ void __launch_bounds__(32 * BY) k_rbgs_lin(double *__restrict__ phi, 
     phi[q] = om == 1. ? y : __dadd_rn(phi[q], __dmul_rn(om, __dsub_rn(y, phi[q])));
 }
 
+// The same linear half sweep indexed as k_rbgs_t: one 32-bit index with
+// wrapped neighbour offsets, the i and j axis tables from the constant bank;
+// the loads, the sum and its order are point_coeffs_fast's.
+template <int BY = 8>
+__global__ void __launch_bounds__(32 * BY) k_rbgs_lin_t(double *__restrict__ phi, const double *__restrict__ rho,
+                                                        const double *__restrict__ cl, Lev L, int color, double om,
+                                                        const __grid_constant__ AxTab T) {
+    const int n = L.n;
+    const int k2 = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * BY + threadIdx.y, i = blockIdx.z;
+    if (2 * k2 >= n || j >= n) return;
+    const int k = 2 * k2 + ((i + j + color) & 1);
+    const int nn = n * n;
+    const int q = (i * n + j) * n + k;
+    const int oip = i == n - 1 ? -(n - 1) * nn : nn, oim = i == 0 ? (n - 1) * nn : -nn;
+    const int ojp = j == n - 1 ? -(n - 1) * n : n, ojm = j == 0 ? (n - 1) * n : -n;
+    const int okp = k == n - 1 ? -(n - 1) : 1, okm = k == 0 ? n - 1 : -1;
+    const double D = __dadd_rn(__dadd_rn(T.dd[i], T.dd[j]), L.dd[k]);
+    double A = __dmul_rn(phi[q + oip], T.ip[i]);
+    A = __dadd_rn(A, __dmul_rn(phi[q + oim], T.im[i]));
+    A = __dadd_rn(A, __dmul_rn(phi[q + ojp], T.ip[j]));
+    A = __dadd_rn(A, __dmul_rn(phi[q + ojm], T.im[j]));
+    A = __dadd_rn(A, __dmul_rn(phi[q + okp], L.ip[k]));
+    A = __dadd_rn(A, __dmul_rn(phi[q + okm], L.im[k]));
+    if (rho) A = __dadd_rn(A, rho[q]);
+    const double y = A / __dadd_rn(D, cl[q]);
+    phi[q] = om == 1. ? y : __dadd_rn(phi[q], __dmul_rn(om, __dsub_rn(y, phi[q])));
+}
+
 __global__ void __launch_bounds__(256) k_residual_lin(const double *__restrict__ phi, const double *__restrict__ rho,
                                                       const double *__restrict__ cl, Lev L, double *__restrict__ r) {
     const int n = L.n;

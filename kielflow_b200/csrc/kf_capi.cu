@@ -571,7 +571,14 @@ void smooth_plain(kf_ctx *c, LevelBuf &L, double *phi, const double *rho, const 
     for (int s = 0; s < sweeps; ++s)
         for (int color = 0; color < 2; ++color) {
             Launch L_(c, cls, 16. * N);
-            if (cc) {
+            if (cc && L.tab) {
+                if (by == 4)
+                    k_rbgs_lin_t<4><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color, om, *L.tab);
+                else if (by == 16)
+                    k_rbgs_lin_t<16><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color, om, *L.tab);
+                else
+                    k_rbgs_lin_t<8><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color, om, *L.tab);
+            } else if (cc) {
                 if (by == 4)
                     k_rbgs_lin<4><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color, om);
                 else if (by == 16)
