@@ -56,6 +56,11 @@ struct LevelBuf {
 
 constexpr int RBS = 256;  // reduction block size
 
+// Colour-split copy of the finest rho for the half sweeps (0: they read rho).
+#ifndef KF_RHO_CS
+#define KF_RHO_CS 1
+#endif
+
 // Half sweeps with the i and j axis tables passed as a kernel parameter
 // (k_rbgs_t; 0: k_rbgs reads them from global memory).
 #ifndef KF_RBGS_TAB
@@ -83,6 +88,7 @@ struct kf_ctx {
     void *Y[4] = {}, *Ys[4] = {}, *ACC[4] = {}, *K[4] = {};
     void *CX[12] = {}, *CY[16] = {}, *R[24] = {}, *phihat = nullptr, *LIN[4] = {};
     double *phi = nullptr, *rho = nullptr, *nd = nullptr;
+    double *rho_cs = nullptr;  // colour-split copy of rho for the finest half sweeps (rho_split)
     void *H = nullptr, *phiT = nullptr;
     void *kv = nullptr, *SV = nullptr, *PF = nullptr, *tw = nullptr;
     double *q2 = nullptr;
@@ -585,6 +591,14 @@ void smooth_plain(kf_ctx *c, LevelBuf &L, double *phi, const double *rho, const 
                     k_rbgs_lin<16><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color, om);
                 else
                     k_rbgs_lin<8><<<g, b, 0, c->st>>>(phi, rho, cc, L.lev(), color, om);
+            } else if (L.tab && rho == c->rho && c->rho_cs) {
+                // the finest level reads the colour-split copy (rho_split at the solve's start)
+                if (by == 4)
+                    k_rbgs_t<4, true><<<g, b, 0, c->st>>>(phi, c->rho_cs, L.lev(), color, om, *L.tab);
+                else if (by == 16)
+                    k_rbgs_t<16, true><<<g, b, 0, c->st>>>(phi, c->rho_cs, L.lev(), color, om, *L.tab);
+                else
+                    k_rbgs_t<8, true><<<g, b, 0, c->st>>>(phi, c->rho_cs, L.lev(), color, om, *L.tab);
             } else if (L.tab) {
                 if (by == 4)
                     k_rbgs_t<4><<<g, b, 0, c->st>>>(phi, rho, L.lev(), color, om, *L.tab);
@@ -765,6 +779,16 @@ double read_max_slots(kf_ctx *c) {
     return r;
 }
 
+// The colour-split copy of c->rho that the finest half sweeps read: made at
+// the start of every FAS solve, so it follows whatever wrote c->rho.
+void rho_split(kf_ctx *c) {
+    if (!c->rho_cs) return;
+    const int n = c->n;
+    Launch L_(c, KC_RHO, 16. * c->N);
+    k_rho_split<<<mg_grid(n / 2, n), mg_block(), 0, c->st>>>(c->rho, c->rho_cs, n);
+    CK(cudaGetLastError());
+}
+
 // Poisson solve on c->phi with source c->rho.  Returns KF_OK or KF_ERR_NOT_CONVERGED.
 int poisson(kf_ctx *c) {
     NvtxRange nv("kf Poisson solve");
@@ -814,6 +838,7 @@ int poisson(kf_ctx *c) {
     } else if (!(cf.res_tol > 0.)) {
         // fixed number of V-cycles: the result is a smooth function of rho
         // and of the initial guess (no data-dependent stopping)
+        rho_split(c);
         for (int cyc = 0; cyc < cf.max_cycles; ++cyc) run_vcycle(c);
         const double r = max_residual(c, L0, c->phi, c->rho, true);
         c->diag.last_iterations = cf.max_cycles;
@@ -824,6 +849,7 @@ int poisson(kf_ctx *c) {
     } else if (c->lv.size() > 1) {
         // test after each cycle's pre-smoothing on the residual the cycle
         // computes anyway; the rest of the cycle only when it fails
+        rho_split(c);
         double r = 0.;
         int cyc = 0;
         for (;;) {
@@ -844,6 +870,7 @@ int poisson(kf_ctx *c) {
             rc = 1;
         }
     } else {
+        rho_split(c);
         double r = max_residual(c, L0, c->phi, c->rho, true);
         int cyc = 0;
         while (r > cf.res_tol && cyc < cf.max_cycles) {
@@ -898,6 +925,7 @@ void poisson_captured(kf_ctx *c) {
     }
     LevelBuf &L0 = c->lv[0];
     const bool fixed = !(cf.res_tol > 0.);
+    rho_split(c);
     c->head_kernels = 0;
     if (!fixed && c->lv.size() > 1) {
         // WHILE { head of the cycle (pre-smoothing, residual with its max);
@@ -1949,6 +1977,8 @@ void create(kf_ctx *c) {
     c->phihat = dalloc<void>(c, cb);
     c->phi = dalloc<double>(c, 8 * c->N);
     c->rho = dalloc<double>(c, 8 * c->N);
+    if (KF_RHO_CS && c->cfg.poisson_mode == KF_PS_FAS && c->n >= 64 && c->n <= KF_TAB_N)
+        c->rho_cs = dalloc<double>(c, 8 * c->N);
     c->nd = dalloc<double>(c, 8 * c->N);
     c->H = dalloc<void>(c, rb);
     c->phiT = c->fp32 ? dalloc<void>(c, rb) : (void *)c->phi;
@@ -2316,6 +2346,7 @@ void autotune(kf_ctx *c, int reps, kf_tune_out *o) {
         CK(cudaMalloc(&tmp, 8 * (size_t)c->N));
         try {
             CK(cudaMemcpyAsync(tmp, c->phi, 8 * (size_t)c->N, cudaMemcpyDeviceToDevice, c->st));
+            rho_split(c);  // the finest half sweeps read the colour-split copy
             int best = -1;
             for (int k = 0; k < 4; ++k) {
                 c->rbgs_by = rows[k];

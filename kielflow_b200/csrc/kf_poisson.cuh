@@ -285,8 +285,23 @@ __global__ void __launch_bounds__(32 * BY) k_rbgs(double *__restrict__ phi, cons
     phi[q] = newton_step(phi[q], A, D, om);
 }
 
-// The same half sweep with the i and j tables from the constant bank (AxTab).
-template <int BY = 8>
+// rho split by colour (the finest level's copy for the half sweeps): the
+// point of colour c at k = 2 k2 + ((i + j + c) & 1) is element
+// c n^3/2 + (i n + j) n/2 + k2, so a half sweep reads only its own colour's
+// rho, contiguously (the natural layout makes it read every sector of rho).
+__global__ void __launch_bounds__(256) k_rho_split(const double *__restrict__ rho, double *__restrict__ rcs, int n) {
+    const int k2 = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 8 + threadIdx.y, i = blockIdx.z;
+    if (2 * k2 >= n || j >= n) return;
+    const int row = (i * n + j) * (n / 2) + k2, half = n * n * (n / 2);
+    const double2 v = *reinterpret_cast<const double2 *>(rho + 2 * row);
+    const int c0 = (i + j) & 1;  // colour of k = 2 k2
+    rcs[c0 * half + row] = v.x;
+    rcs[(c0 ^ 1) * half + row] = v.y;
+}
+
+// The same half sweep with the i and j tables from the constant bank (AxTab);
+// CS: rho is the colour-split copy (k_rho_split), the sum and its order unchanged.
+template <int BY = 8, bool CS = false>
 __global__ void __launch_bounds__(32 * BY) k_rbgs_t(double *__restrict__ phi, const double *__restrict__ rho, Lev L,
                                                     int color, double om, const __grid_constant__ AxTab T) {
     const int n = L.n;
@@ -305,7 +320,10 @@ __global__ void __launch_bounds__(32 * BY) k_rbgs_t(double *__restrict__ phi, co
     A = __dadd_rn(A, __dmul_rn(phi[q + ojm], T.im[j]));
     A = __dadd_rn(A, __dmul_rn(phi[q + okp], L.ip[k]));
     A = __dadd_rn(A, __dmul_rn(phi[q + okm], L.im[k]));
-    A = __dadd_rn(A, rho[q]);
+    if constexpr (CS)
+        A = __dadd_rn(A, rho[color * (nn * (n / 2)) + (i * n + j) * (n / 2) + k2]);
+    else
+        A = __dadd_rn(A, rho[q]);
     phi[q] = newton_step(phi[q], A, D, om);
 }
 
